@@ -1,0 +1,134 @@
+/*
+ * shgemm_b200 -- C ABI of the B200 (sm_100a) SHGEMM library.
+ *
+ * Plain C types only (pointers, sizes, ints), so any FFI can bind it. Every
+ * entry point returns an int status (SHGEMM_STATUS_*). Matrices are
+ * column-major with BLAS op semantics; all matrix pointers are device memory
+ * owned by the caller; alpha/beta point to host floats read at call time; work
+ * is enqueued asynchronously on the handle's CUDA stream.
+ *
+ * Each entry point names the reference interface it replaces
+ * (enp1s0/shgemm, paths relative to that project).
+ */
+#ifndef SHGEMM_B200_H_
+#define SHGEMM_B200_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct shgemm_b200_handle* shgemm_b200_handle_t;
+
+/* operation_t (include/shgemm/shgemm.hpp:36-39) */
+enum { SHGEMM_OP_N = 0, SHGEMM_OP_T = 1 };
+/* tc_t (include/shgemm/shgemm.hpp:41-44) */
+enum { SHGEMM_TC_FP16 = 0, SHGEMM_TC_TF32 = 1 };
+/* detail::kernel_level (include/shgemm/shgemm.hpp:30-34) */
+enum { SHGEMM_LEVEL_P0 = 0, SHGEMM_LEVEL_P1 = 1, SHGEMM_LEVEL_AUTO = -1 };
+
+enum {
+    SHGEMM_STATUS_OK = 0,
+    SHGEMM_STATUS_INVALID_VALUE = 1,
+    SHGEMM_STATUS_NOT_SUPPORTED = 2,
+    SHGEMM_STATUS_ALLOC_FAILED = 3,
+    SHGEMM_STATUS_LAUNCH_FAILED = 4,
+    SHGEMM_STATUS_TIMEOUT = 5,
+    SHGEMM_STATUS_CUDA_ERROR = 6
+};
+
+/* Tunables for shgemm_b200_set_config (no reference counterpart; the
+ * reference fixes these at compile time in its tile tables, src/shgemm.cu:429-488). */
+enum {
+    SHGEMM_CFG_CHUNK_K = 1,       /* k elements per hi-accumulator drain (multiple of 64; default 256) */
+    SHGEMM_CFG_SPLIT_K = 2,       /* 0 = automatic, 1 = never split, s > 1 = force s slices */
+    SHGEMM_CFG_WAIT_LIMIT_MS = 3, /* bound on every in-kernel wait (default 2000 ms) */
+    SHGEMM_CFG_GROUP_M = 4        /* tile rasterisation group along m (default 8) */
+};
+
+/* mtk::shgemm::create (include/shgemm/shgemm.hpp:94; src/shgemm.cu:401-490).
+ * Binds the handle to `device` (the reference hard-codes device 0, src/shgemm.cu:419-425),
+ * allocates the handle's workspace and error word once. */
+int shgemm_b200_create(shgemm_b200_handle_t* handle, int device);
+
+/* mtk::shgemm::destroy (include/shgemm/shgemm.hpp:95; src/shgemm.cu:492-496). */
+int shgemm_b200_destroy(shgemm_b200_handle_t handle);
+
+/* mtk::shgemm::set_cuda_stream (include/shgemm/shgemm.hpp:102; src/shgemm.cu:498-503).
+ * `cuda_stream` is a cudaStream_t (NULL = legacy default stream). */
+int shgemm_b200_set_stream(shgemm_b200_handle_t handle, void* cuda_stream);
+
+/* mtk::shgemm::enable_kernel_level_fixing / disable_kernel_level_fixing
+ * (include/shgemm/shgemm.hpp:97-98; src/shgemm.cu:505-515). SHGEMM_LEVEL_AUTO disables. */
+int shgemm_b200_set_kernel_level(shgemm_b200_handle_t handle, int level);
+
+/* mtk::shgemm::set_debug_mode (include/shgemm/shgemm.hpp:100; src/shgemm.cu:688-690). */
+int shgemm_b200_set_debug_mode(shgemm_b200_handle_t handle, unsigned on);
+
+/* mtk::shgemm::shgemm (include/shgemm/shgemm.hpp:105-119; src/shgemm.cu:517-686):
+ * C = alpha * op(A) * op(B) + beta * C, A FP32, B binary16 (`b` points to __half),
+ * op_c == SHGEMM_OP_T stores C transposed. *level_out (may be NULL) receives the
+ * kernel level used, like the reference's return value. */
+int shgemm_b200_shgemm(shgemm_b200_handle_t handle, int op_a, int op_b, size_t m, size_t n, size_t k,
+                       const float* alpha, const float* a, size_t lda, const void* b, size_t ldb,
+                       const float* beta, float* c, size_t ldc, int compute_type, int op_c, int* level_out);
+
+/* mtk::shgemm::hsgemm (include/shgemm/shgemm.hpp:121-157): A binary16, B FP32,
+ * computed through the same transposition identity as the reference. */
+int shgemm_b200_hsgemm(shgemm_b200_handle_t handle, int op_a, int op_b, size_t m, size_t n, size_t k,
+                       const float* alpha, const void* a, size_t lda, const float* b, size_t ldb,
+                       const float* beta, float* c, size_t ldc, int compute_type, int op_c, int* level_out);
+
+/* Tunables (no reference counterpart). */
+int shgemm_b200_set_config(shgemm_b200_handle_t handle, int key, long long value);
+int shgemm_b200_get_config(shgemm_b200_handle_t handle, int key, long long* value);
+
+/* Resizes the handle-owned split-K workspace (the reference's w_ptr,
+ * src/shgemm.cu:417). Allocation happens here, never inside shgemm calls. */
+int shgemm_b200_set_workspace_size(shgemm_b200_handle_t handle, size_t bytes);
+
+/* Synchronises the handle's stream and reports (then clears) the device-side
+ * error word: SHGEMM_STATUS_TIMEOUT when a kernel gave up a bounded wait
+ * (*device_code = which role), SHGEMM_STATUS_CUDA_ERROR on a CUDA error.
+ * No reference counterpart (the reference checks no launch). */
+int shgemm_b200_check_error(shgemm_b200_handle_t handle, int* device_code);
+
+/* Number of kernels this library enqueued since the handle was created. */
+int shgemm_b200_get_launch_count(shgemm_b200_handle_t handle, long long* count);
+
+/* Human-readable status name. */
+const char* shgemm_b200_status_string(int status);
+
+/* Self-test of the bounded in-kernel wait: launches one CTA that waits on an
+ * mbarrier nothing arrives at, with a limit of `limit_us`; the kernel must give
+ * up, record the timeout and return. *observed receives the device error code.
+ * No reference counterpart. */
+int shgemm_b200_selftest_wait_timeout(shgemm_b200_handle_t handle, unsigned limit_us, int* observed);
+
+/* ------------------------------------------------------------------------
+ * Evaluation helpers (FP64 on the GPU, used only to measure error; the
+ * reference's role for these is mateval, test/shgemm_test.cu:91-100).
+ * ------------------------------------------------------------------------ */
+
+/* C64 (m x n, ld = m, column-major) = op(A) * op(B) in FP64 from FP32 A and binary16 B. */
+int shgemm_b200_eval_dgemm(shgemm_b200_handle_t handle, int op_a, int op_b, size_t m, size_t n, size_t k,
+                           const float* a, size_t lda, const void* b, size_t ldb, double* c64);
+
+/* Same with the operand types swapped (A binary16, B FP32), for HSGEMM results. */
+int shgemm_b200_eval_dgemm_hs(shgemm_b200_handle_t handle, int op_a, int op_b, size_t m, size_t n, size_t k,
+                              const void* a, size_t lda, const float* b, size_t ldb, double* c64);
+
+/* Error of C (op_c layout, ldc) against ref = alpha*C64 + beta*C0 (C0 may be NULL when beta == 0):
+ * out[0] = ||C - ref||_F over entries finite in both, out[1] = ||ref||_F over the same,
+ * out[2] = max |C - ref| / |ref| over those entries with ref != 0,
+ * out[3] = number of entries where C and ref disagree on being finite. */
+int shgemm_b200_eval_error(shgemm_b200_handle_t handle, size_t m, size_t n, const float* c, size_t ldc, int op_c,
+                           const double* c64, double alpha, double beta, const float* c0, double* out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SHGEMM_B200_H_ */

@@ -1,0 +1,229 @@
+"""shgemm_b200 -- B200 (sm_100a) SHGEMM/HSGEMM with the reference's error-corrected method.
+
+Host-side Python mirror of the reference's ``mtk::shgemm`` interface
+(include/shgemm/shgemm.hpp:94-157) over the C ABI of ``libshgemm_b200.so``
+(include/shgemm_b200.h). Operands are CUDA device buffers: torch tensors (their
+data pointers are used) or raw integer device addresses. Column-major BLAS
+semantics, host-side alpha/beta, asynchronous execution on the handle's stream.
+
+There is no CPU fallback: every call goes to the CUDA library, and importing
+this package fails loudly when the shared library is missing.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+__all__ = [
+    "op_n", "op_t", "fp16", "tf32", "P0", "P1", "ShgemmError", "Handle", "create", "destroy",
+    "set_cuda_stream", "enable_kernel_level_fixing", "disable_kernel_level_fixing", "set_debug_mode",
+    "shgemm", "hsgemm", "library_path",
+]
+
+op_n, op_t = 0, 1          # operation_t (include/shgemm/shgemm.hpp:36-39)
+fp16, tf32 = 0, 1          # tc_t (include/shgemm/shgemm.hpp:41-44)
+P0, P1 = 0, 1              # detail::kernel_level (include/shgemm/shgemm.hpp:30-34)
+
+CFG_CHUNK_K, CFG_SPLIT_K, CFG_WAIT_LIMIT_MS, CFG_GROUP_M = 1, 2, 3, 4
+
+STATUS = {0: "OK", 1: "INVALID_VALUE", 2: "NOT_SUPPORTED", 3: "ALLOC_FAILED", 4: "LAUNCH_FAILED",
+          5: "TIMEOUT", 6: "CUDA_ERROR"}
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "libshgemm_b200.so")
+_lib = None
+
+
+class ShgemmError(RuntimeError):
+    def __init__(self, status: int, what: str):
+        self.status = status
+        super().__init__(f"{what}: SHGEMM_STATUS_{STATUS.get(status, status)}")
+
+
+def library_path() -> str:
+    return _LIB_PATH
+
+
+def lib() -> ctypes.CDLL:
+    """Loads the CUDA library (raises if it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(_LIB_PATH):
+        raise ImportError(f"{_LIB_PATH} is missing: build it with `python -m shgemm_b200.build`")
+    L = ctypes.CDLL(_LIB_PATH)
+    vp, sz, i, f, d = ctypes.c_void_p, ctypes.c_size_t, ctypes.c_int, ctypes.c_float, ctypes.c_double
+    pi, pf, pd = ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_double)
+    sig = {
+        "shgemm_b200_create": [ctypes.POINTER(vp), i],
+        "shgemm_b200_destroy": [vp],
+        "shgemm_b200_set_stream": [vp, vp],
+        "shgemm_b200_set_kernel_level": [vp, i],
+        "shgemm_b200_set_debug_mode": [vp, ctypes.c_uint],
+        "shgemm_b200_shgemm": [vp, i, i, sz, sz, sz, pf, vp, sz, vp, sz, pf, vp, sz, i, i, pi],
+        "shgemm_b200_hsgemm": [vp, i, i, sz, sz, sz, pf, vp, sz, vp, sz, pf, vp, sz, i, i, pi],
+        "shgemm_b200_set_config": [vp, i, ctypes.c_longlong],
+        "shgemm_b200_get_config": [vp, i, ctypes.POINTER(ctypes.c_longlong)],
+        "shgemm_b200_set_workspace_size": [vp, sz],
+        "shgemm_b200_check_error": [vp, pi],
+        "shgemm_b200_get_launch_count": [vp, ctypes.POINTER(ctypes.c_longlong)],
+        "shgemm_b200_selftest_wait_timeout": [vp, ctypes.c_uint, pi],
+        "shgemm_b200_eval_dgemm": [vp, i, i, sz, sz, sz, vp, sz, vp, sz, vp],
+        "shgemm_b200_eval_dgemm_hs": [vp, i, i, sz, sz, sz, vp, sz, vp, sz, vp],
+        "shgemm_b200_eval_error": [vp, sz, sz, vp, sz, i, vp, d, d, vp, pd],
+    }
+    for name, args in sig.items():
+        fn = getattr(L, name)
+        fn.argtypes = args
+        fn.restype = i
+    L.shgemm_b200_status_string.argtypes = [i]
+    L.shgemm_b200_status_string.restype = ctypes.c_char_p
+    _lib = L
+    return L
+
+
+def _check(status: int, what: str) -> None:
+    if status != 0:
+        raise ShgemmError(status, what)
+
+
+def _addr(x) -> int:
+    """Device address of a torch tensor or an integer pointer."""
+    if x is None:
+        return 0
+    if isinstance(x, int):
+        return x
+    ptr = getattr(x, "data_ptr", None)
+    if ptr is None:
+        raise TypeError(f"expected a CUDA tensor or a device address, got {type(x)!r}")
+    if not getattr(x, "is_cuda", True):
+        raise ValueError("operands must live in CUDA device memory")
+    return ptr()
+
+
+def _stream_addr(stream) -> int:
+    if stream is None:
+        return 0
+    if isinstance(stream, int):
+        return stream
+    return int(stream.cuda_stream)
+
+
+class Handle:
+    """The reference's shgemmHandle_t (include/shgemm/shgemm.hpp:46-92)."""
+
+    def __init__(self, device: int = 0):
+        self._h = ctypes.c_void_p()
+        self.device = device
+        _check(lib().shgemm_b200_create(ctypes.byref(self._h), device), "shgemm_b200_create")
+        self.cuda_stream = 0
+
+    @property
+    def ptr(self) -> ctypes.c_void_p:
+        if not self._h:
+            raise ShgemmError(1, "handle destroyed")
+        return self._h
+
+    def close(self) -> None:
+        if self._h:
+            _check(lib().shgemm_b200_destroy(self._h), "shgemm_b200_destroy")
+            self._h = ctypes.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_stream(self, stream) -> None:
+        self.cuda_stream = _stream_addr(stream)
+        _check(lib().shgemm_b200_set_stream(self.ptr, ctypes.c_void_p(self.cuda_stream)), "set_stream")
+
+    def set_config(self, key: int, value: int) -> None:
+        _check(lib().shgemm_b200_set_config(self.ptr, key, value), "set_config")
+
+    def get_config(self, key: int) -> int:
+        v = ctypes.c_longlong()
+        _check(lib().shgemm_b200_get_config(self.ptr, key, ctypes.byref(v)), "get_config")
+        return v.value
+
+    def set_workspace_size(self, nbytes: int) -> None:
+        _check(lib().shgemm_b200_set_workspace_size(self.ptr, nbytes), "set_workspace_size")
+
+    def check_error(self) -> int:
+        """Synchronises and returns the device error code (0 = none)."""
+        code = ctypes.c_int()
+        st = lib().shgemm_b200_check_error(self.ptr, ctypes.byref(code))
+        if st not in (0, 5):
+            raise ShgemmError(st, "check_error")
+        return code.value
+
+    def launch_count(self) -> int:
+        v = ctypes.c_longlong()
+        _check(lib().shgemm_b200_get_launch_count(self.ptr, ctypes.byref(v)), "get_launch_count")
+        return v.value
+
+    def selftest_wait_timeout(self, limit_us: int = 20000) -> tuple[int, int]:
+        code = ctypes.c_int()
+        st = lib().shgemm_b200_selftest_wait_timeout(self.ptr, limit_us, ctypes.byref(code))
+        return st, code.value
+
+
+# ---------------------------------------------------------------- reference-shaped API
+def create(device: int = 0) -> Handle:
+    """mtk::shgemm::create (include/shgemm/shgemm.hpp:94)."""
+    return Handle(device)
+
+
+def destroy(handle: Handle) -> None:
+    """mtk::shgemm::destroy (include/shgemm/shgemm.hpp:95)."""
+    handle.close()
+
+
+def set_cuda_stream(handle: Handle, stream) -> None:
+    """mtk::shgemm::set_cuda_stream (include/shgemm/shgemm.hpp:102)."""
+    handle.set_stream(stream)
+
+
+def enable_kernel_level_fixing(handle: Handle, level: int) -> None:
+    """include/shgemm/shgemm.hpp:97."""
+    _check(lib().shgemm_b200_set_kernel_level(handle.ptr, level), "enable_kernel_level_fixing")
+
+
+def disable_kernel_level_fixing(handle: Handle) -> None:
+    """include/shgemm/shgemm.hpp:98."""
+    _check(lib().shgemm_b200_set_kernel_level(handle.ptr, -1), "disable_kernel_level_fixing")
+
+
+def set_debug_mode(handle: Handle, on: int) -> None:
+    """include/shgemm/shgemm.hpp:100."""
+    _check(lib().shgemm_b200_set_debug_mode(handle.ptr, on), "set_debug_mode")
+
+
+def shgemm(handle: Handle, op_a: int, op_b: int, m: int, n: int, k: int, alpha: float, a, lda: int, b, ldb: int,
+           beta: float, c, ldc: int, compute_type: int, op_c: int = op_n) -> int:
+    """mtk::shgemm::shgemm (include/shgemm/shgemm.hpp:105-119): A FP32, B binary16.
+
+    Returns the kernel level, like the reference. Raises ShgemmError on failure.
+    """
+    al, be, lv = ctypes.c_float(alpha), ctypes.c_float(beta), ctypes.c_int(0)
+    st = lib().shgemm_b200_shgemm(handle.ptr, op_a, op_b, m, n, k, ctypes.byref(al), _addr(a), lda, _addr(b), ldb,
+                                  ctypes.byref(be), _addr(c), ldc, compute_type, op_c, ctypes.byref(lv))
+    _check(st, "shgemm")
+    return lv.value
+
+
+def hsgemm(handle: Handle, op_a: int, op_b: int, m: int, n: int, k: int, alpha: float, a, lda: int, b, ldb: int,
+           beta: float, c, ldc: int, compute_type: int, op_c: int = op_n) -> int:
+    """mtk::shgemm::hsgemm (include/shgemm/shgemm.hpp:121-157): A binary16, B FP32."""
+    al, be, lv = ctypes.c_float(alpha), ctypes.c_float(beta), ctypes.c_int(0)
+    st = lib().shgemm_b200_hsgemm(handle.ptr, op_a, op_b, m, n, k, ctypes.byref(al), _addr(a), lda, _addr(b), ldb,
+                                  ctypes.byref(be), _addr(c), ldc, compute_type, op_c, ctypes.byref(lv))
+    _check(st, "hsgemm")
+    return lv.value

@@ -1,0 +1,686 @@
+// Host side of the C ABI (include/shgemm_b200.h): handle, dispatch, TMA
+// descriptors and launches of the sm_100a kernels, plus the split-K reduction,
+// the k == 0 scaling kernel, the bounded-wait self test and the FP64 evaluation
+// kernels used to measure error.
+#include <cuda.h>
+#include <cuda_fp16.h>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <atomic>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <mutex>
+#include <vector>
+
+#include "shgemm_b200.h"
+#include "shgemm_kernel.cuh"
+
+using namespace shgemm_b200;
+
+struct shgemm_b200_handle {
+    int device = 0;
+    int num_sms = 148;
+    cudaStream_t stream = nullptr;
+    unsigned debug_mode = 0;
+    int fixed_level = SHGEMM_LEVEL_AUTO;
+    long long chunk_k = 256;
+    long long split_k = 0;
+    long long wait_limit_ms = 2000;
+    long long group_m = 8;
+    float* workspace = nullptr;
+    size_t workspace_bytes = 0;
+    int* error_word = nullptr;
+    std::atomic<long long> launches{0};
+};
+
+namespace {
+
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiledFn encode_fn() {
+    static EncodeTiledFn fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess) {
+            fn = reinterpret_cast<EncodeTiledFn>(p);
+        }
+    });
+    return fn;
+}
+
+// 2-D tiled tensor map: dim0 contiguous (`d0` elements), dim1 with a stride of
+// `stride1_bytes`; box {b0, b1}. Out-of-range elements read as zero.
+bool make_tmap(CUtensorMap* map, CUtensorMapDataType dtype, const void* base, uint64_t d0, uint64_t d1,
+               uint64_t stride1_bytes, uint32_t b0, uint32_t b1, CUtensorMapSwizzle swz) {
+    EncodeTiledFn fn = encode_fn();
+    if (!fn) return false;
+    cuuint64_t dims[2] = {d0, d1};
+    cuuint64_t strides[1] = {stride1_bytes};
+    cuuint32_t box[2] = {b0, b1};
+    cuuint32_t estr[2] = {1, 1};
+    CUresult r = fn(map, dtype, 2, const_cast<void*>(base), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                    swz, CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS;
+}
+
+using TileKernelFn = void (*)(TileGemmParams);
+
+template <int TC, int BN, bool AK, bool BK>
+void* tile_kernel_ptr() {
+    return reinterpret_cast<void*>(&shgemm_tile_kernel<TC, BN, AK, BK>);
+}
+
+template <int TC, int BN, bool AK, bool BK>
+int tile_smem() {
+    return TileCfg<TC, BN, AK, BK>::SMEM_BYTES;
+}
+
+struct KernelEntry {
+    void* fn;
+    int smem;
+};
+
+// [tc][bn128][a_kmajor][b_kmajor]
+KernelEntry kernel_table(int tc, int bn128, int ak, int bk) {
+#define SHG_ENTRY(TC, BN, AK, BK) \
+    if (tc == TC && bn128 == (BN == 128) && ak == AK && bk == BK) return {tile_kernel_ptr<TC, BN, AK, BK>(), tile_smem<TC, BN, AK, BK>()};
+    SHG_ENTRY(kFP16, 128, 0, 0) SHG_ENTRY(kFP16, 128, 0, 1) SHG_ENTRY(kFP16, 128, 1, 0) SHG_ENTRY(kFP16, 128, 1, 1)
+    SHG_ENTRY(kFP16, 64, 0, 0) SHG_ENTRY(kFP16, 64, 0, 1) SHG_ENTRY(kFP16, 64, 1, 0) SHG_ENTRY(kFP16, 64, 1, 1)
+    SHG_ENTRY(kTF32, 128, 0, 0) SHG_ENTRY(kTF32, 128, 0, 1) SHG_ENTRY(kTF32, 128, 1, 0) SHG_ENTRY(kTF32, 128, 1, 1)
+    SHG_ENTRY(kTF32, 64, 0, 0) SHG_ENTRY(kTF32, 64, 0, 1) SHG_ENTRY(kTF32, 64, 1, 0) SHG_ENTRY(kTF32, 64, 1, 1)
+#undef SHG_ENTRY
+    return {nullptr, 0};
+}
+
+// ------------------------------------------------------------------ small kernels
+// C = beta * C (k == 0: the product is empty).
+__global__ void scale_c_kernel(float* c, uint64_t ldc, int rows, int cols, float beta) {
+    const size_t total = static_cast<size_t>(rows) * cols;
+    for (size_t idx = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; idx < total;
+         idx += static_cast<size_t>(gridDim.x) * blockDim.x) {
+        const int r = static_cast<int>(idx % rows);
+        const int cc = static_cast<int>(idx / rows);
+        float* d = c + r + static_cast<size_t>(cc) * ldc;
+        *d = (beta == 0.0f) ? 0.0f : __fmul_rn(beta, *d);
+    }
+}
+
+// Deterministic split-K reduction: slices summed in fixed order 0..S-1, then the
+// same alpha/beta epilogue as the tile kernel (C is not read when beta == 0).
+__global__ void splitk_reduce_kernel(const float* __restrict__ ws, int slices, int m, int n, float* c,
+                                     uint64_t ldc, int op_c, float alpha, float beta) {
+    const size_t mn = static_cast<size_t>(m) * n;
+    for (size_t idx = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; idx < mn;
+         idx += static_cast<size_t>(gridDim.x) * blockDim.x) {
+        size_t row, col;
+        if (op_c == kOpN) {
+            row = idx % m;
+            col = idx / m;
+        } else {  // walk C's memory order so stores stay coalesced
+            col = idx % n;
+            row = idx / n;
+        }
+        const size_t w = row + col * m;
+        float s = ws[w];
+        for (int sl = 1; sl < slices; ++sl) s = __fadd_rn(s, ws[w + static_cast<size_t>(sl) * mn]);
+        float* d = (op_c == kOpN) ? c + row + col * ldc : c + col + row * ldc;
+        *d = (beta == 0.0f) ? __fmul_rn(s, alpha) : __fmaf_rn(s, alpha, __fmul_rn(beta, *d));
+    }
+}
+
+__global__ void selftest_wait_kernel(int* error_flag, uint64_t limit_ns) {
+    __shared__ __align__(8) uint64_t bar;
+    __shared__ int abort_flag;
+    if (threadIdx.x == 0) {
+        ptx::mbar_init(&bar, 1);
+        abort_flag = 0;
+        ptx::fence_mbarrier_init();
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        // Nothing ever arrives on `bar`: the bounded wait must give up.
+        if (!ptx::mbar_wait(&bar, 0, &abort_flag, limit_ns)) atomicCAS(error_flag, 0, kErrMmaTimeout);
+    }
+    __syncthreads();
+}
+
+// ------------------------------------------------------------------ FP64 evaluation
+template <typename T>
+__device__ __forceinline__ double to_d(T v);
+template <>
+__device__ __forceinline__ double to_d<float>(float v) { return static_cast<double>(v); }
+template <>
+__device__ __forceinline__ double to_d<__half>(__half v) { return static_cast<double>(__half2float(v)); }
+
+// 64x64 output tile per 256-thread block, 4x4 doubles per thread.
+template <typename TA, typename TB>
+__global__ void __launch_bounds__(256) eval_dgemm_kernel(int op_a, int op_b, int m, int n, int k, const TA* a,
+                                                         uint64_t lda, const TB* b, uint64_t ldb, double* c) {
+    __shared__ double As[16][64 + 1];
+    __shared__ double Bs[16][64 + 1];
+    const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+    const int m0 = blockIdx.x * 64, n0 = blockIdx.y * 64;
+    double acc[4][4] = {};
+    for (int k0 = 0; k0 < k; k0 += 16) {
+        for (int i = threadIdx.x; i < 16 * 64; i += 256) {
+            const int kk = i / 64, r = i % 64;
+            const int gi = m0 + r, gk = k0 + kk;
+            double va = 0.0;
+            if (gi < m && gk < k) va = to_d(op_a == kOpN ? a[gi + gk * lda] : a[gk + gi * lda]);
+            As[kk][r] = va;
+            const int gj = n0 + r;
+            double vb = 0.0;
+            if (gj < n && gk < k) vb = to_d(op_b == kOpN ? b[gk + gj * ldb] : b[gj + gk * ldb]);
+            Bs[kk][r] = vb;
+        }
+        __syncthreads();
+#pragma unroll
+        for (int kk = 0; kk < 16; ++kk) {
+            double ar[4], br[4];
+#pragma unroll
+            for (int i = 0; i < 4; ++i) ar[i] = As[kk][tx + 16 * i];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) br[j] = Bs[kk][ty + 16 * j];
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+#pragma unroll
+                for (int j = 0; j < 4; ++j) acc[i][j] = fma(ar[i], br[j], acc[i][j]);
+        }
+        __syncthreads();
+    }
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const int gi = m0 + tx + 16 * i, gj = n0 + ty + 16 * j;
+            if (gi < m && gj < n) c[gi + static_cast<size_t>(gj) * m] = acc[i][j];
+        }
+}
+
+__global__ void eval_error_kernel(size_t m, size_t n, const float* c, uint64_t ldc, int op_c, const double* c64,
+                                  double alpha, double beta, const float* c0, double* partial) {
+    double s_diff = 0.0, s_ref = 0.0, s_max = 0.0, s_mismatch = 0.0;
+    const size_t total = m * n;
+    for (size_t idx = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; idx < total;
+         idx += static_cast<size_t>(gridDim.x) * blockDim.x) {
+        const size_t i = idx % m, j = idx / m;
+        const size_t ci = (op_c == kOpN) ? i + j * ldc : j + i * ldc;
+        double ref = alpha * c64[idx];
+        if (beta != 0.0) ref += beta * static_cast<double>(c0[ci]);
+        const double v = static_cast<double>(c[ci]);
+        const bool fv = isfinite(v), fr = isfinite(ref);
+        if (fv && fr) {
+            const double d = v - ref;
+            s_diff += d * d;
+            s_ref += ref * ref;
+            if (ref != 0.0) s_max = fmax(s_max, fabs(d) / fabs(ref));
+        } else if (fv != fr) {
+            s_mismatch += 1.0;
+        }
+    }
+    __shared__ double red[4][256];
+    red[0][threadIdx.x] = s_diff;
+    red[1][threadIdx.x] = s_ref;
+    red[2][threadIdx.x] = s_max;
+    red[3][threadIdx.x] = s_mismatch;
+    __syncthreads();
+    for (int s = 128; s > 0; s >>= 1) {
+        if (threadIdx.x < s) {
+            red[0][threadIdx.x] += red[0][threadIdx.x + s];
+            red[1][threadIdx.x] += red[1][threadIdx.x + s];
+            red[2][threadIdx.x] = fmax(red[2][threadIdx.x], red[2][threadIdx.x + s]);
+            red[3][threadIdx.x] += red[3][threadIdx.x + s];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        for (int q = 0; q < 4; ++q) partial[blockIdx.x * 4 + q] = red[q][0];
+    }
+}
+
+struct DeviceGuard {
+    int prev = -1;
+    explicit DeviceGuard(int dev) {
+        if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+        if (prev != dev) cudaSetDevice(dev);
+    }
+    ~DeviceGuard() {
+        int cur;
+        if (prev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev) cudaSetDevice(prev);
+    }
+};
+
+int launch_status() {
+    const cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? SHGEMM_STATUS_OK : SHGEMM_STATUS_LAUNCH_FAILED;
+}
+
+struct Plan {
+    int level;  // 0: BN = 64, 1: BN = 128
+    int bn;
+    int tiles_m, tiles_n;
+    int total_steps;
+    int slices;
+    int steps_per_slice;
+    int chunk_steps;
+};
+
+double wave_efficiency(long long units, int sms) {
+    const long long waves = (units + sms - 1) / sms;
+    return static_cast<double>(units) / static_cast<double>(waves * sms);
+}
+
+Plan make_plan(const shgemm_b200_handle* h, size_t m, size_t n, size_t k, int tc) {
+    Plan p{};
+    const int bk = (tc == kFP16) ? 64 : 32;
+    p.total_steps = static_cast<int>((k + bk - 1) / bk);
+    const long long chunk_k = std::max<long long>(bk, h->chunk_k);
+    p.chunk_steps = static_cast<int>(std::max<long long>(1, chunk_k / bk));
+    p.tiles_m = static_cast<int>((m + 127) / 128);
+    // Level choice mirrors the reference (src/shgemm.cu:643-656): the large tile when it
+    // still fills the machine, else the small one; a fixed level overrides.
+    const long long tiles128 = static_cast<long long>(p.tiles_m) * ((n + 127) / 128);
+    int level = (n <= 64 || tiles128 < h->num_sms) ? 0 : 1;
+    if (h->fixed_level == SHGEMM_LEVEL_P0 || h->fixed_level == SHGEMM_LEVEL_P1) level = h->fixed_level;
+    p.level = level;
+    p.bn = level ? 128 : 64;
+    p.tiles_n = static_cast<int>((n + p.bn - 1) / p.bn);
+    const long long tiles = static_cast<long long>(p.tiles_m) * p.tiles_n;
+    // Split-K: deterministic slices when the tiles alone leave SMs idle and k is long.
+    int slices = 1;
+    if (h->split_k > 1) {
+        slices = static_cast<int>(h->split_k);
+    } else if (h->split_k == 0 && tiles < h->num_sms && k >= 4096) {
+        double best = wave_efficiency(tiles, h->num_sms);
+        for (int s = 2; s <= 64; ++s) {
+            if (p.total_steps / s < 2 * p.chunk_steps) break;
+            const double e = wave_efficiency(tiles * s, h->num_sms);
+            if (e > best + 0.02) {
+                best = e;
+                slices = s;
+            }
+        }
+    }
+    // The workspace bounds the slice count (no allocation inside a call).
+    const size_t per_slice = m * n * sizeof(float);
+    if (slices > 1 && per_slice > 0) {
+        const size_t fit = h->workspace_bytes / per_slice;
+        if (fit < 2) slices = 1;
+        else if (static_cast<size_t>(slices) > fit) slices = static_cast<int>(fit);
+    }
+    slices = std::max(1, std::min(slices, p.total_steps));
+    p.steps_per_slice = (p.total_steps + slices - 1) / slices;
+    p.slices = (p.total_steps + p.steps_per_slice - 1) / p.steps_per_slice;
+    return p;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* shgemm_b200_status_string(int s) {
+    switch (s) {
+        case SHGEMM_STATUS_OK: return "SHGEMM_STATUS_OK";
+        case SHGEMM_STATUS_INVALID_VALUE: return "SHGEMM_STATUS_INVALID_VALUE";
+        case SHGEMM_STATUS_NOT_SUPPORTED: return "SHGEMM_STATUS_NOT_SUPPORTED";
+        case SHGEMM_STATUS_ALLOC_FAILED: return "SHGEMM_STATUS_ALLOC_FAILED";
+        case SHGEMM_STATUS_LAUNCH_FAILED: return "SHGEMM_STATUS_LAUNCH_FAILED";
+        case SHGEMM_STATUS_TIMEOUT: return "SHGEMM_STATUS_TIMEOUT";
+        case SHGEMM_STATUS_CUDA_ERROR: return "SHGEMM_STATUS_CUDA_ERROR";
+        default: return "SHGEMM_STATUS_UNKNOWN";
+    }
+}
+
+int shgemm_b200_create(shgemm_b200_handle_t* out, int device) {
+    if (!out) return SHGEMM_STATUS_INVALID_VALUE;
+    *out = nullptr;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev) {
+        cudaGetLastError();
+        return SHGEMM_STATUS_INVALID_VALUE;
+    }
+    DeviceGuard g(device);
+    int major = 0, minor = 0, sms = 0;
+    cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, device);
+    cudaDeviceGetAttribute(&minor, cudaDevAttrComputeCapabilityMinor, device);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    if (major != 10 || minor != 0) return SHGEMM_STATUS_NOT_SUPPORTED;  // sm_100a code only
+    if (!encode_fn()) return SHGEMM_STATUS_NOT_SUPPORTED;
+    auto* h = new shgemm_b200_handle();
+    h->device = device;
+    h->num_sms = sms;
+    const char* dbg = std::getenv("MTK_SHGEMM_DEBUG");  // same switch as src/shgemm.cu:407-410
+    if (dbg && dbg[0] == '1') h->debug_mode = 1;
+    const char* lvl = std::getenv("MTK_SHGEMM_KERNEL_LEVEL");  // src/shgemm.cu:411-414
+    if (lvl && (lvl[0] == '0' || lvl[0] == '1') && lvl[1] == '\0') h->fixed_level = lvl[0] - '0';
+    if (cudaMalloc(&h->error_word, sizeof(int)) != cudaSuccess) {
+        delete h;
+        return SHGEMM_STATUS_ALLOC_FAILED;
+    }
+    cudaMemset(h->error_word, 0, sizeof(int));
+    // Default split-K workspace: 64 MiB (room for e.g. 16 slices of a 1024 x 1024 C).
+    h->workspace_bytes = size_t(64) << 20;
+    if (cudaMalloc(&h->workspace, h->workspace_bytes) != cudaSuccess) {
+        cudaFree(h->error_word);
+        delete h;
+        return SHGEMM_STATUS_ALLOC_FAILED;
+    }
+    for (int tc = 0; tc < 2; ++tc)
+        for (int b = 0; b < 2; ++b)
+            for (int ak = 0; ak < 2; ++ak)
+                for (int bk = 0; bk < 2; ++bk) {
+                    KernelEntry e = kernel_table(tc, b, ak, bk);
+                    if (cudaFuncSetAttribute(e.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, e.smem) !=
+                        cudaSuccess) {
+                        cudaGetLastError();
+                        cudaFree(h->workspace);
+                        cudaFree(h->error_word);
+                        delete h;
+                        return SHGEMM_STATUS_NOT_SUPPORTED;
+                    }
+                }
+    *out = h;
+    return SHGEMM_STATUS_OK;
+}
+
+int shgemm_b200_destroy(shgemm_b200_handle_t h) {
+    if (!h) return SHGEMM_STATUS_INVALID_VALUE;
+    DeviceGuard g(h->device);
+    cudaFree(h->workspace);
+    cudaFree(h->error_word);
+    delete h;
+    return SHGEMM_STATUS_OK;
+}
+
+int shgemm_b200_set_stream(shgemm_b200_handle_t h, void* s) {
+    if (!h) return SHGEMM_STATUS_INVALID_VALUE;
+    h->stream = static_cast<cudaStream_t>(s);
+    return SHGEMM_STATUS_OK;
+}
+
+int shgemm_b200_set_kernel_level(shgemm_b200_handle_t h, int level) {
+    if (!h || level < SHGEMM_LEVEL_AUTO || level > SHGEMM_LEVEL_P1) return SHGEMM_STATUS_INVALID_VALUE;
+    h->fixed_level = level;
+    return SHGEMM_STATUS_OK;
+}
+
+int shgemm_b200_set_debug_mode(shgemm_b200_handle_t h, unsigned on) {
+    if (!h) return SHGEMM_STATUS_INVALID_VALUE;
+    h->debug_mode = on;
+    return SHGEMM_STATUS_OK;
+}
+
+int shgemm_b200_set_config(shgemm_b200_handle_t h, int key, long long v) {
+    if (!h) return SHGEMM_STATUS_INVALID_VALUE;
+    switch (key) {
+        case SHGEMM_CFG_CHUNK_K:
+            if (v < 64 || v % 64) return SHGEMM_STATUS_INVALID_VALUE;
+            h->chunk_k = v;
+            return SHGEMM_STATUS_OK;
+        case SHGEMM_CFG_SPLIT_K:
+            if (v < 0 || v > 1024) return SHGEMM_STATUS_INVALID_VALUE;
+            h->split_k = v;
+            return SHGEMM_STATUS_OK;
+        case SHGEMM_CFG_WAIT_LIMIT_MS:
+            if (v < 1 || v > 600000) return SHGEMM_STATUS_INVALID_VALUE;
+            h->wait_limit_ms = v;
+            return SHGEMM_STATUS_OK;
+        case SHGEMM_CFG_GROUP_M:
+            if (v < 1 || v > 1024) return SHGEMM_STATUS_INVALID_VALUE;
+            h->group_m = v;
+            return SHGEMM_STATUS_OK;
+        default:
+            return SHGEMM_STATUS_INVALID_VALUE;
+    }
+}
+
+int shgemm_b200_get_config(shgemm_b200_handle_t h, int key, long long* v) {
+    if (!h || !v) return SHGEMM_STATUS_INVALID_VALUE;
+    switch (key) {
+        case SHGEMM_CFG_CHUNK_K: *v = h->chunk_k; return SHGEMM_STATUS_OK;
+        case SHGEMM_CFG_SPLIT_K: *v = h->split_k; return SHGEMM_STATUS_OK;
+        case SHGEMM_CFG_WAIT_LIMIT_MS: *v = h->wait_limit_ms; return SHGEMM_STATUS_OK;
+        case SHGEMM_CFG_GROUP_M: *v = h->group_m; return SHGEMM_STATUS_OK;
+        default: return SHGEMM_STATUS_INVALID_VALUE;
+    }
+}
+
+int shgemm_b200_set_workspace_size(shgemm_b200_handle_t h, size_t bytes) {
+    if (!h) return SHGEMM_STATUS_INVALID_VALUE;
+    DeviceGuard g(h->device);
+    if (cudaStreamSynchronize(h->stream) != cudaSuccess) return SHGEMM_STATUS_CUDA_ERROR;
+    float* w = nullptr;
+    if (bytes > 0 && cudaMalloc(&w, bytes) != cudaSuccess) {
+        cudaGetLastError();
+        return SHGEMM_STATUS_ALLOC_FAILED;
+    }
+    cudaFree(h->workspace);
+    h->workspace = w;
+    h->workspace_bytes = bytes;
+    return SHGEMM_STATUS_OK;
+}
+
+int shgemm_b200_check_error(shgemm_b200_handle_t h, int* device_code) {
+    if (!h) return SHGEMM_STATUS_INVALID_VALUE;
+    DeviceGuard g(h->device);
+    if (cudaStreamSynchronize(h->stream) != cudaSuccess) return SHGEMM_STATUS_CUDA_ERROR;
+    int code = 0;
+    if (cudaMemcpy(&code, h->error_word, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess)
+        return SHGEMM_STATUS_CUDA_ERROR;
+    if (code) cudaMemset(h->error_word, 0, sizeof(int));
+    if (device_code) *device_code = code;
+    return code ? SHGEMM_STATUS_TIMEOUT : SHGEMM_STATUS_OK;
+}
+
+int shgemm_b200_get_launch_count(shgemm_b200_handle_t h, long long* count) {
+    if (!h || !count) return SHGEMM_STATUS_INVALID_VALUE;
+    *count = h->launches.load();
+    return SHGEMM_STATUS_OK;
+}
+
+int shgemm_b200_selftest_wait_timeout(shgemm_b200_handle_t h, unsigned limit_us, int* observed) {
+    if (!h) return SHGEMM_STATUS_INVALID_VALUE;
+    DeviceGuard g(h->device);
+    selftest_wait_kernel<<<1, 32, 0, h->stream>>>(h->error_word, static_cast<uint64_t>(limit_us) * 1000ull);
+    h->launches++;
+    if (launch_status() != SHGEMM_STATUS_OK) return SHGEMM_STATUS_LAUNCH_FAILED;
+    int code = 0;
+    const int st = shgemm_b200_check_error(h, &code);
+    if (observed) *observed = code;
+    return st;
+}
+
+int shgemm_b200_shgemm(shgemm_b200_handle_t h, int op_a, int op_b, size_t m, size_t n, size_t k,
+                       const float* alpha_ptr, const float* a, size_t lda, const void* b, size_t ldb,
+                       const float* beta_ptr, float* c, size_t ldc, int tc, int op_c, int* level_out) {
+    if (!h || !alpha_ptr || !beta_ptr) return SHGEMM_STATUS_INVALID_VALUE;
+    if ((op_a != kOpN && op_a != kOpT) || (op_b != kOpN && op_b != kOpT) || (op_c != kOpN && op_c != kOpT) ||
+        (tc != kFP16 && tc != kTF32))
+        return SHGEMM_STATUS_INVALID_VALUE;
+    if (m == 0 || n == 0) {
+        if (level_out) *level_out = SHGEMM_LEVEL_P0;
+        return SHGEMM_STATUS_OK;
+    }
+    const size_t a_rows = (op_a == kOpN) ? m : k;
+    const size_t b_rows = (op_b == kOpN) ? k : n;
+    const size_t c_rows = (op_c == kOpN) ? m : n;
+    if (!c || ldc < c_rows) return SHGEMM_STATUS_INVALID_VALUE;
+    if (k > 0 && (!a || !b || lda < std::max<size_t>(1, a_rows) || ldb < std::max<size_t>(1, b_rows)))
+        return SHGEMM_STATUS_INVALID_VALUE;
+    if (m >= (1u << 31) || n >= (1u << 31) || k >= (1u << 31)) return SHGEMM_STATUS_NOT_SUPPORTED;
+    const float alpha = *alpha_ptr, beta = *beta_ptr;
+    DeviceGuard g(h->device);
+
+    if (k == 0) {  // empty product: C = beta * C
+        const size_t rows = c_rows, cols = (op_c == kOpN) ? n : m;
+        const int blocks = static_cast<int>(std::min<size_t>((rows * cols + 255) / 256, 4096));
+        scale_c_kernel<<<blocks, 256, 0, h->stream>>>(c, ldc, static_cast<int>(rows), static_cast<int>(cols), beta);
+        h->launches++;
+        if (level_out) *level_out = SHGEMM_LEVEL_P0;
+        return launch_status();
+    }
+    // TMA needs 16-byte aligned bases and leading dimensions.
+    if ((reinterpret_cast<uintptr_t>(a) & 15) || (reinterpret_cast<uintptr_t>(b) & 15) || (lda * 4) % 16 ||
+        (ldb * 2) % 16)
+        return SHGEMM_STATUS_NOT_SUPPORTED;
+
+    const Plan pl = make_plan(h, m, n, k, tc);
+    const bool a_kmajor = (op_a == kOpT);
+    const bool b_kmajor = (op_b == kOpN);
+    const int bk = (tc == kFP16) ? 64 : 32;
+
+    TileGemmParams P;
+    std::memset(&P, 0, sizeof(P));
+    bool ok;
+    // FP32 operand: K-major tiles are [128 rows][32 floats] with a 128-byte swizzle;
+    // M-major tiles are [bk][128 floats] unswizzled.
+    if (a_kmajor)
+        ok = make_tmap(&P.tmap_a, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, a, k, m, lda * 4, 32, 128,
+                       CU_TENSOR_MAP_SWIZZLE_128B);
+    else
+        ok = make_tmap(&P.tmap_a, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, a, m, k, lda * 4, 128, bk,
+                       CU_TENSOR_MAP_SWIZZLE_NONE);
+    if (!ok) return SHGEMM_STATUS_NOT_SUPPORTED;
+    if (tc == kFP16) {
+        if (b_kmajor)
+            ok = make_tmap(&P.tmap_b, CU_TENSOR_MAP_DATA_TYPE_FLOAT16, b, k, n, ldb * 2, 64, pl.bn,
+                           CU_TENSOR_MAP_SWIZZLE_128B);
+        else
+            ok = make_tmap(&P.tmap_b, CU_TENSOR_MAP_DATA_TYPE_FLOAT16, b, n, k, ldb * 2, 64, 64,
+                           CU_TENSOR_MAP_SWIZZLE_128B);
+    } else {
+        if (b_kmajor)
+            ok = make_tmap(&P.tmap_b, CU_TENSOR_MAP_DATA_TYPE_FLOAT16, b, k, n, ldb * 2, 32, pl.bn,
+                           CU_TENSOR_MAP_SWIZZLE_64B);
+        else
+            ok = make_tmap(&P.tmap_b, CU_TENSOR_MAP_DATA_TYPE_FLOAT16, b, n, k, ldb * 2, pl.bn, 32,
+                           CU_TENSOR_MAP_SWIZZLE_NONE);
+    }
+    if (!ok) return SHGEMM_STATUS_NOT_SUPPORTED;
+
+    P.c = c;
+    P.ldc = ldc;
+    P.workspace = h->workspace;
+    P.error_flag = h->error_word;
+    P.wait_limit_ns = static_cast<uint64_t>(h->wait_limit_ms) * 1000000ull;
+    P.m = static_cast<int>(m);
+    P.n = static_cast<int>(n);
+    P.k = static_cast<int>(k);
+    P.op_c = op_c;
+    P.alpha = alpha;
+    P.beta = beta;
+    P.tiles_m = pl.tiles_m;
+    P.tiles_n = pl.tiles_n;
+    P.num_slices = pl.slices;
+    P.steps_per_slice = pl.steps_per_slice;
+    P.num_units = pl.tiles_m * pl.tiles_n * pl.slices;
+    P.group_m = static_cast<int>(h->group_m);
+    P.chunk_steps = pl.chunk_steps;
+
+    const KernelEntry e = kernel_table(tc, pl.bn == 128, a_kmajor, b_kmajor);
+    const int grid = std::min(P.num_units, h->num_sms);
+    if (h->debug_mode) {
+        std::printf("[shape=(%zu,%zu,%zu),op_a=%s,op_b=%s,compute_type=%s] kernel_level = %d, tile = 128x%d, "
+                    "k_slices = %d, chunk_k = %d, grid = %d\n",
+                    m, n, k, op_a == kOpN ? "N" : "T", op_b == kOpN ? "N" : "T", tc == kTF32 ? "TF32" : "FP16",
+                    pl.level, pl.bn, pl.slices, pl.chunk_steps * bk, grid);
+    }
+    void* args[] = {&P};
+    cudaError_t err = cudaLaunchKernel(e.fn, dim3(grid), dim3(448), args, e.smem, h->stream);
+    h->launches++;
+    if (err != cudaSuccess) {
+        cudaGetLastError();
+        return SHGEMM_STATUS_LAUNCH_FAILED;
+    }
+    if (pl.slices > 1) {
+        const size_t mn = m * n;
+        const int blocks = static_cast<int>(std::min<size_t>((mn + 255) / 256, size_t(h->num_sms) * 8));
+        splitk_reduce_kernel<<<blocks, 256, 0, h->stream>>>(h->workspace, pl.slices, P.m, P.n, c, ldc, op_c, alpha,
+                                                            beta);
+        h->launches++;
+        if (launch_status() != SHGEMM_STATUS_OK) return SHGEMM_STATUS_LAUNCH_FAILED;
+    }
+    if (level_out) *level_out = (pl.slices > 1) ? SHGEMM_LEVEL_P0 : pl.level;
+    return SHGEMM_STATUS_OK;
+}
+
+int shgemm_b200_hsgemm(shgemm_b200_handle_t h, int op_a, int op_b, size_t m, size_t n, size_t k,
+                       const float* alpha, const void* a, size_t lda, const float* b, size_t ldb, const float* beta,
+                       float* c, size_t ldc, int tc, int op_c, int* level_out) {
+    // C = A B  <=>  C^T = B^T A^T with the FP32 operand on the left and C written
+    // transposed (include/shgemm/shgemm.hpp:142-156).
+    auto inv = [](int op) { return op == kOpN ? kOpT : kOpN; };
+    if ((op_a != kOpN && op_a != kOpT) || (op_b != kOpN && op_b != kOpT) || (op_c != kOpN && op_c != kOpT))
+        return SHGEMM_STATUS_INVALID_VALUE;
+    return shgemm_b200_shgemm(h, inv(op_b), inv(op_a), n, m, k, alpha, b, ldb, a, lda, beta, c, ldc, tc, inv(op_c),
+                              level_out);
+}
+
+static int eval_dgemm_impl(shgemm_b200_handle_t h, int op_a, int op_b, size_t m, size_t n, size_t k, const void* a,
+                           size_t lda, const void* b, size_t ldb, double* c64, bool a_is_float) {
+    if (!h || !a || !b || !c64 || m == 0 || n == 0) return SHGEMM_STATUS_INVALID_VALUE;
+    if (m >= (1u << 31) || n >= (1u << 31) || k >= (1u << 31)) return SHGEMM_STATUS_NOT_SUPPORTED;
+    DeviceGuard g(h->device);
+    const dim3 grid(static_cast<unsigned>((m + 63) / 64), static_cast<unsigned>((n + 63) / 64));
+    if (a_is_float)
+        eval_dgemm_kernel<float, __half><<<grid, 256, 0, h->stream>>>(
+            op_a, op_b, (int)m, (int)n, (int)k, static_cast<const float*>(a), lda, static_cast<const __half*>(b), ldb,
+            c64);
+    else
+        eval_dgemm_kernel<__half, float><<<grid, 256, 0, h->stream>>>(
+            op_a, op_b, (int)m, (int)n, (int)k, static_cast<const __half*>(a), lda, static_cast<const float*>(b), ldb,
+            c64);
+    return launch_status();
+}
+
+int shgemm_b200_eval_dgemm(shgemm_b200_handle_t h, int op_a, int op_b, size_t m, size_t n, size_t k, const float* a,
+                           size_t lda, const void* b, size_t ldb, double* c64) {
+    return eval_dgemm_impl(h, op_a, op_b, m, n, k, a, lda, b, ldb, c64, true);
+}
+
+int shgemm_b200_eval_dgemm_hs(shgemm_b200_handle_t h, int op_a, int op_b, size_t m, size_t n, size_t k,
+                              const void* a, size_t lda, const float* b, size_t ldb, double* c64) {
+    return eval_dgemm_impl(h, op_a, op_b, m, n, k, a, lda, b, ldb, c64, false);
+}
+
+int shgemm_b200_eval_error(shgemm_b200_handle_t h, size_t m, size_t n, const float* c, size_t ldc, int op_c,
+                           const double* c64, double alpha, double beta, const float* c0, double* out) {
+    if (!h || !c || !c64 || !out || (beta != 0.0 && !c0)) return SHGEMM_STATUS_INVALID_VALUE;
+    DeviceGuard g(h->device);
+    const int blocks = 1024;
+    double* partial = nullptr;
+    if (cudaMalloc(&partial, sizeof(double) * 4 * blocks) != cudaSuccess) return SHGEMM_STATUS_ALLOC_FAILED;
+    eval_error_kernel<<<blocks, 256, 0, h->stream>>>(m, n, c, ldc, op_c, c64, alpha, beta, c0, partial);
+    int st = launch_status();
+    std::vector<double> hp(4 * blocks);
+    if (st == SHGEMM_STATUS_OK) {
+        if (cudaMemcpyAsync(hp.data(), partial, sizeof(double) * 4 * blocks, cudaMemcpyDeviceToHost, h->stream) !=
+                cudaSuccess ||
+            cudaStreamSynchronize(h->stream) != cudaSuccess)
+            st = SHGEMM_STATUS_CUDA_ERROR;
+    }
+    cudaFree(partial);
+    if (st != SHGEMM_STATUS_OK) return st;
+    double d = 0, r = 0, mx = 0, mm = 0;
+    for (int i = 0; i < blocks; ++i) {
+        d += hp[4 * i];
+        r += hp[4 * i + 1];
+        mx = std::max(mx, hp[4 * i + 2]);
+        mm += hp[4 * i + 3];
+    }
+    out[0] = std::sqrt(d);
+    out[1] = std::sqrt(r);
+    out[2] = mx;
+    out[3] = mm;
+    return SHGEMM_STATUS_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,76 @@
+"""The C-ABI library builds, loads without a GPU and exports every entry point
+that include/shgemm_b200.h declares (no compute calls here)."""
+import ctypes
+import os
+import re
+import subprocess
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_symbols():
+    names = []
+    for hdr in ("shgemm_b200.h",):
+        text = open(os.path.join(ROOT, "include", hdr)).read()
+        text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+        names += re.findall(r"\b(shgemm_b200_\w+)\s*\(", text)
+    return sorted(set(names))
+
+
+def test_header_declares_entry_points():
+    names = declared_symbols()
+    assert "shgemm_b200_shgemm" in names and "shgemm_b200_hsgemm" in names
+    assert len(names) >= 15
+
+
+def test_library_exports_every_declared_symbol():
+    import shgemm_b200
+
+    path = shgemm_b200.library_path()
+    assert os.path.exists(path), "run __graft_entry__.build() first"
+    lib = ctypes.CDLL(path)
+    missing = [n for n in declared_symbols() if not hasattr(lib, n)]
+    assert not missing, missing
+    out = subprocess.run(["nm", "-D", "--defined-only", path], capture_output=True, text=True).stdout
+    for n in declared_symbols():
+        assert re.search(rf"\bT {n}$", out, flags=re.M), n
+
+
+def test_cpp_api_symbols_exported():
+    import shgemm_b200
+
+    out = subprocess.run(["nm", "-DC", "--defined-only", shgemm_b200.library_path()], capture_output=True,
+                         text=True).stdout
+    for fn in ("mtk::shgemm::create", "mtk::shgemm::destroy", "mtk::shgemm::set_cuda_stream",
+               "mtk::shgemm::enable_kernel_level_fixing", "mtk::shgemm::disable_kernel_level_fixing",
+               "mtk::shgemm::set_debug_mode", "mtk::shgemm::shgemm("):
+        assert fn in out, fn
+
+
+def test_status_strings_without_gpu():
+    import shgemm_b200
+
+    L = shgemm_b200.lib()
+    assert L.shgemm_b200_status_string(0) == b"SHGEMM_STATUS_OK"
+    assert L.shgemm_b200_status_string(5) == b"SHGEMM_STATUS_TIMEOUT"
+
+
+def test_create_without_gpu_fails_cleanly():
+    import torch
+
+    import shgemm_b200
+
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    with pytest.raises(shgemm_b200.ShgemmError):
+        shgemm_b200.Handle(0)
+
+
+def test_library_is_sm100a_only():
+    import shgemm_b200
+
+    out = subprocess.run(["cuobjdump", "--list-elf", shgemm_b200.library_path()], capture_output=True,
+                         text=True).stdout
+    assert "sm_100a" in out

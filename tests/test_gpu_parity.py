@@ -1,0 +1,216 @@
+"""Parity of the CUDA path (through the C ABI) with the CPU oracle.
+
+Mirrors the reference's test programs (test/shgemm_test.cu: every op_a x op_b x
+op_c x compute type; test/exponent_test.cu: exponent ranges; test/
+shgemm_k_slicing_test.cu: long k), at sizes the oracle finishes in seconds,
+plus the edge cases they do not cover (ragged shapes, alpha/beta, padded
+leading dimensions, k = 0, hsgemm).
+"""
+import os
+
+import numpy as np
+import pytest
+
+import oracle
+from tests import _cases as K
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def h(cuda_device):
+    import shgemm_b200 as sg
+
+    hd = sg.Handle(0)
+    yield hd
+    hd.close()
+
+
+def chunk_of(h):
+    import shgemm_b200 as sg
+
+    return h.get_config(sg.CFG_CHUNK_K)
+
+
+def _parity(h, tc, op_a, op_b, op_c, m, n, k, alpha=1.0, beta=0.0, dist="uniform", pad=0, seed=0):
+    rng = np.random.default_rng(seed)
+    inp = K.make_inputs(rng, m, n, k, op_a, op_b, op_c, dist=dist, pad=pad)
+    gpu_c, level = K.run_gpu(h, tc, op_a, op_b, m, n, k, alpha, inp, beta, op_c)
+    orc = K.run_oracle(tc, op_a, op_b, m, n, k, alpha, inp, beta, op_c, chunk=0)
+    ref = K.fp64(op_a, op_b, m, n, k, alpha, inp, beta, op_c)
+    sg_c = K.sgemm(op_a, op_b, m, n, k, alpha, inp, beta, op_c)
+    r = K.parity_report(gpu_c, orc, ref, sg_c, m, n, inp["ldc"], op_c)
+    r["level"] = level
+    return r, gpu_c, inp
+
+
+OPS = [(a, b) for a in (0, 1) for b in (0, 1)]
+
+
+@pytest.mark.parametrize("tc", [oracle.FP16, oracle.TF32])
+@pytest.mark.parametrize("op_a,op_b", OPS)
+@pytest.mark.parametrize("op_c", [0, 1])
+def test_square_1024(h, tc, op_a, op_b, op_c):
+    """Config 1 shape (1024^3) for every op combination (test/shgemm_test.cu:276-306)."""
+    r, _, _ = _parity(h, tc, op_a, op_b, op_c, 1024, 1024, 1024)
+    K.assert_parity(r)
+
+
+@pytest.mark.parametrize("tc", [oracle.FP16, oracle.TF32])
+@pytest.mark.parametrize("op_a,op_b", OPS)
+@pytest.mark.parametrize("mnk", [(1, 1, 1), (7, 5, 3), (33, 17, 70), (129, 65, 257), (200, 300, 1000),
+                                 (128, 128, 64), (257, 130, 4097)])
+def test_ragged_shapes(h, tc, op_a, op_b, mnk):
+    m, n, k = mnk
+    r, _, _ = _parity(h, tc, op_a, op_b, (op_a + op_b) % 2, m, n, k, seed=m + n + k)
+    K.assert_parity(r)
+
+
+@pytest.mark.parametrize("tc", [oracle.FP16, oracle.TF32])
+def test_alpha_beta_padded_ld(h, tc):
+    r, _, _ = _parity(h, tc, 0, 1, 0, 300, 200, 500, alpha=-1.5, beta=0.5, pad=8, seed=3)
+    K.assert_parity(r)
+    r, _, _ = _parity(h, tc, 1, 0, 1, 300, 200, 500, alpha=0.25, beta=2.0, pad=16, seed=4)
+    K.assert_parity(r)
+
+
+def test_beta_zero_does_not_read_c(h):
+    import torch
+
+    import shgemm_b200 as sg
+
+    m = n = k = 256
+    rng = np.random.default_rng(9)
+    A = torch.from_numpy(rng.uniform(-1, 1, m * k).astype(np.float32)).cuda()
+    B = torch.from_numpy(rng.uniform(-1, 1, k * n).astype(np.float16).view(np.int16)).cuda().view(torch.float16)
+    C = torch.full((m * n,), float("nan"), device="cuda")
+    sg.shgemm(h, 0, 0, m, n, k, 1.0, A, m, B, k, 0.0, C, m, sg.fp16)
+    torch.cuda.synchronize()
+    assert torch.isfinite(C).all()
+
+
+@pytest.mark.parametrize("tc", [oracle.FP16, oracle.TF32])
+def test_permutation_b_is_bit_exact(h, tc):
+    """B = a column permutation: every C entry is one split element folded back,
+    hi + lo * 2^-11, so the GPU must equal the oracle bit for bit."""
+    rng = np.random.default_rng(21)
+    m, k = 300, 192
+    n = k
+    A = (rng.standard_normal(m * k) * np.exp2(rng.uniform(-20, 10, m * k))).astype(np.float32)
+    perm = rng.permutation(k)
+    Bm = np.zeros((k, n), np.float16)
+    Bm[perm, np.arange(n)] = 1.0
+    inp = dict(A=A, B=Bm.ravel(order="F"), C=np.zeros(m * n, np.float32), lda=m, ldb=k, ldc=m)
+    gpu_c, _ = K.run_gpu(h, tc, 0, 0, m, n, k, 1.0, inp, 0.0, 0)
+    orc = K.run_oracle(tc, 0, 0, m, n, k, 1.0, inp, 0.0, 0, chunk=chunk_of(h))
+    same = (gpu_c.view(np.uint32) == orc.view(np.uint32)) | (np.isnan(gpu_c) & np.isnan(orc))
+    assert same.all(), np.argwhere(~same)[:5]
+
+
+@pytest.mark.parametrize("tc", [oracle.FP16, oracle.TF32])
+def test_exact_gemm_fixture(h, tc):
+    g = np.load(os.path.join(os.path.dirname(__file__), "golden", "gemm_exact.npz"))
+    m, n, k = int(g["m"]), int(g["n"]), int(g["k"])
+    inp = dict(A=g["A"], B=g["B"].view(np.float16), C=np.zeros(m * n, np.float32), lda=m, ldb=k, ldc=m)
+    gpu_c, _ = K.run_gpu(h, tc, 0, 0, m, n, k, 1.0, inp, 0.0, 0)
+    assert np.array_equal(gpu_c.astype(np.float64), g["C"])
+
+
+@pytest.mark.parametrize("tc", [oracle.FP16, oracle.TF32])
+@pytest.mark.parametrize("op_a,op_b", OPS)
+def test_wide_exponent_nonfinite_mask(h, tc, op_a, op_b):
+    """Config 2's FP32 distribution N(0,1) 2^U(-15,15): in fp16 mode elements past
+    65504 overflow to inf in hi (no rescaling, like the reference) and the
+    non-finite pattern must match the oracle exactly."""
+    r, _, _ = _parity(h, tc, op_a, op_b, 0, 256, 192, 640, dist="wide", beta=0.5, seed=17)
+    K.assert_parity(r)
+
+
+@pytest.mark.parametrize("tc", [oracle.FP16, oracle.TF32])
+@pytest.mark.parametrize("lo_e,hi_e", [(-15, 14), (-36, -15), (-100, -36)])
+def test_exponent_ranges(h, tc, lo_e, hi_e):
+    """test/exponent_test.cu:249-252: A = 2^U(lo, hi), B uniform (0, 1]; the lo term
+    carries the value once hi underflows and the GPU must follow the oracle."""
+    rng = np.random.default_rng(lo_e & 0xFF)
+    m, n, k = 256, 256, 256
+    A = np.exp2(rng.uniform(lo_e, hi_e, m * k)).astype(np.float32)
+    B = rng.uniform(0, 1, k * n).astype(np.float16)
+    inp = dict(A=A, B=B, C=np.zeros(m * n, np.float32), lda=m, ldb=k, ldc=m)
+    gpu_c, _ = K.run_gpu(h, tc, 0, 0, m, n, k, 1.0, inp, 0.0, 0)
+    orc = K.run_oracle(tc, 0, 0, m, n, k, 1.0, inp, 0.0, 0, chunk=0)
+    ref = K.fp64(0, 0, m, n, k, 1.0, inp, 0.0, 0)
+    e_g = oracle.rel_fro(oracle.logical_c(gpu_c, m, n, m), ref)
+    e_o = oracle.rel_fro(oracle.logical_c(orc, m, n, m), ref)
+    # where the split loses bits (deep underflow) both lose the same ones
+    assert e_g <= 2.0 * e_o + K.ULP_FLOOR, (e_g, e_o)
+
+
+@pytest.mark.parametrize("tc", [oracle.FP16, oracle.TF32])
+@pytest.mark.parametrize("op_a,op_b", OPS)
+def test_hsgemm(h, tc, op_a, op_b):
+    """hsgemm through the transposition identity (include/shgemm/shgemm.hpp:121-157)."""
+    rng = np.random.default_rng(31)
+    m, n, k = 96, 160, 320
+    lda = m if op_a == 0 else k
+    ldb = k if op_b == 0 else n
+    Ah = rng.uniform(-1, 1, lda * (k if op_a == 0 else m)).astype(np.float16)
+    Bf = rng.uniform(-1, 1, ldb * (n if op_b == 0 else k)).astype(np.float32)
+    inp = dict(A=Bf, B=Ah, C=np.zeros(m * n, np.float32), lda=ldb, ldb=lda, ldc=m)
+    gpu_c, _ = K.run_gpu(h, tc, op_a, op_b, m, n, k, 1.0, inp, 0.0, 0, hs=True)
+    C = np.zeros(m * n, np.float32)
+    oracle.hsgemm(tc, op_a, op_b, m, n, k, 1.0, Ah, lda, Bf, ldb, 0.0, C, m, 0)
+    Am = Ah.astype(np.float64).reshape(-1, lda).T  # columns of the stored buffer
+    Aop = Am[:m, :k] if op_a == 0 else Am[:k, :m].T
+    Bm = Bf.astype(np.float64).reshape(-1, ldb).T
+    Bop = Bm[:k, :n] if op_b == 0 else Bm[:n, :k].T
+    ref = Aop @ Bop
+    e_g = oracle.rel_fro(oracle.logical_c(gpu_c, m, n, m), ref)
+    e_o = oracle.rel_fro(oracle.logical_c(C, m, n, m), ref)
+    assert e_g <= 2.0 * e_o + K.ULP_FLOOR, (e_g, e_o)
+
+
+def test_k_zero_scales_c(h):
+    r, gpu_c, inp = _parity(h, oracle.FP16, 0, 0, 0, 64, 48, 0, beta=0.5)
+    assert np.array_equal(gpu_c, (inp["C"] * np.float32(0.5)).astype(np.float32))
+
+
+@pytest.mark.parametrize("level", [0, 1])
+def test_kernel_level_fixing(h, level):
+    import shgemm_b200 as sg
+
+    sg.enable_kernel_level_fixing(h, level)
+    try:
+        r, _, _ = _parity(h, oracle.FP16, 0, 0, 0, 320, 192, 384, seed=level)
+    finally:
+        sg.disable_kernel_level_fixing(h)
+    assert r["level"] == level
+    K.assert_parity(r)
+
+
+def test_unaligned_leading_dimension_is_rejected(h):
+    import torch
+
+    import shgemm_b200 as sg
+
+    m, n, k = 33, 17, 35
+    A = torch.zeros(m * k + 8, device="cuda")
+    B = torch.zeros(k * n + 8, device="cuda", dtype=torch.float16)
+    C = torch.zeros(m * n + 8, device="cuda")
+    with pytest.raises(sg.ShgemmError) as ei:
+        sg.shgemm(h, 0, 0, m, n, k, 1.0, A, m, B, k, 0.0, C, m, sg.fp16)
+    assert ei.value.status == 2
+
+
+def test_bounded_wait_times_out_and_context_survives(h):
+    """A wait on an mbarrier that nothing arrives at gives up after its limit, the
+    host reads the timeout status, and the context keeps working."""
+    st, code = h.selftest_wait_timeout(20000)
+    assert st == 5 and code != 0
+    r, _, _ = _parity(h, oracle.FP16, 0, 0, 0, 128, 128, 128)
+    K.assert_parity(r)
+
+
+def test_launch_count_increments(h):
+    before = h.launch_count()
+    _parity(h, oracle.FP16, 0, 0, 0, 64, 64, 64)
+    assert h.launch_count() > before

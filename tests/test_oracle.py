@@ -1,0 +1,141 @@
+"""The CPU oracle against the golden fixtures (independent implementations)."""
+import os
+
+import numpy as np
+import pytest
+
+import oracle
+
+GOLD = os.path.join(os.path.dirname(__file__), "golden")
+
+
+def _same_float(a, b):
+    a = np.asarray(a, dtype=np.float32)
+    b = np.asarray(b, dtype=np.float32)
+    both_nan = np.isnan(a) & np.isnan(b)
+    return np.all(both_nan | (a.view(np.uint32) == b.view(np.uint32)))
+
+
+def test_split_fp16_matches_numpy_ieee_cast():
+    g = np.load(os.path.join(GOLD, "split_fp16.npz"))
+    hi, lo = oracle.split(oracle.FP16, g["v"])
+    assert _same_float(hi, g["hi"].view(np.float16).astype(np.float32))
+    assert _same_float(lo, g["lo"].view(np.float16).astype(np.float32))
+
+
+def test_f16_bits_roundtrip_all_halves():
+    bits = np.arange(0, 1 << 16, dtype=np.uint32).astype(np.uint16)
+    vals = bits.view(np.float16).astype(np.float32)
+    finite = np.isfinite(vals)
+    back = oracle.f32_to_f16_bits(vals[finite])
+    assert np.array_equal(back, bits[finite])
+
+
+def test_split_tf32_matches_exact_rounding():
+    g = np.load(os.path.join(GOLD, "split_tf32.npz"))
+    hi, lo = oracle.split(oracle.TF32, g["v"])
+    assert _same_float(hi, g["hi"])
+    assert _same_float(lo, g["lo"])
+
+
+@pytest.mark.parametrize("tc", [oracle.FP16, oracle.TF32])
+def test_split_recovers_22_bits(tc):
+    rng = np.random.default_rng(1)
+    v = rng.uniform(-1, 1, 20000).astype(np.float32)
+    v = v[np.abs(v) > 2.0 ** -10]
+    hi, lo = oracle.split(tc, v)
+    rec = hi.astype(np.float64) + lo.astype(np.float64) / 2048.0
+    rel = np.abs(rec - v) / np.abs(v)
+    assert rel.max() <= 2.0 ** -21
+
+
+def test_fp16_overflow_and_underflow_handling():
+    # 7e4 overflows binary16: hi = inf and lo = -inf (reference behaviour, no rescaling)
+    hi, lo = oracle.split(oracle.FP16, np.array([7e4], np.float32))
+    assert np.isinf(hi[0]) and np.isinf(lo[0]) and hi[0] > 0 > lo[0]
+    # 2^-30 is below binary16's range: hi = 0 and it survives only in lo (x 2^11)
+    hi, lo = oracle.split(oracle.FP16, np.array([2.0 ** -30], np.float32))
+    assert hi[0] == 0.0 and lo[0] == np.float32(2.0 ** -19)
+
+
+@pytest.mark.parametrize("tc", [oracle.FP16, oracle.TF32])
+@pytest.mark.parametrize("chunk", [0, 64, 256])
+def test_gemm_exact_fixture(tc, chunk):
+    g = np.load(os.path.join(GOLD, "gemm_exact.npz"))
+    m, n, k = int(g["m"]), int(g["n"]), int(g["k"])
+    C = np.zeros(m * n, np.float32)
+    oracle.shgemm(tc, 0, 0, m, n, k, 1.0, g["A"], m, g["B"], k, 0.0, C, m, 0, chunk)
+    assert np.array_equal(C.astype(np.float64), g["C"])
+
+
+def _rand_case(rng, m, n, k, op_a, op_b):
+    A = rng.uniform(-1, 1, m * k).astype(np.float32)
+    B = rng.uniform(-1, 1, k * n).astype(np.float16)
+    lda = m if op_a == 0 else k
+    ldb = k if op_b == 0 else n
+    return A, lda, B, ldb
+
+
+@pytest.mark.parametrize("op_a", [0, 1])
+@pytest.mark.parametrize("op_b", [0, 1])
+@pytest.mark.parametrize("op_c", [0, 1])
+def test_shgemm_error_well_below_sgemm(op_a, op_b, op_c):
+    rng = np.random.default_rng(7)
+    m, n, k = 45, 38, 300
+    A, lda, B, ldb = _rand_case(rng, m, n, k, op_a, op_b)
+    ldc = m if op_c == 0 else n
+    ref = oracle.dgemm_ref(op_a, op_b, m, n, k, 1.0, A, lda, B, ldb)
+    errs = {}
+    for tc in (oracle.FP16, oracle.TF32):
+        C = np.zeros(m * n, np.float32)
+        oracle.shgemm(tc, op_a, op_b, m, n, k, 1.0, A, lda, B, ldb, 0.0, C, ldc, op_c)
+        errs[tc] = oracle.rel_fro(oracle.logical_c(C, m, n, ldc, op_c), ref)
+    S = np.zeros(m * n, np.float32)
+    oracle.sgemm(op_a, op_b, m, n, k, 1.0, A, lda, B, ldb, 0.0, S, ldc, op_c)
+    e_s = oracle.rel_fro(oracle.logical_c(S, m, n, ldc, op_c), ref)
+    assert errs[oracle.FP16] < 2 * e_s and errs[oracle.TF32] < 2 * e_s
+    assert e_s < 1e-6
+
+
+def test_alpha_beta_and_beta_zero_ignores_c():
+    rng = np.random.default_rng(3)
+    m, n, k = 20, 12, 50
+    A, lda, B, ldb = _rand_case(rng, m, n, k, 0, 0)
+    C0 = rng.uniform(-1, 1, m * n).astype(np.float32)
+    C = C0.copy()
+    oracle.shgemm(oracle.FP16, 0, 0, m, n, k, 2.0, A, lda, B, ldb, 0.5, C, m, 0)
+    ref = oracle.dgemm_ref(0, 0, m, n, k, 2.0, A, lda, B, ldb, 0.5, C0, m, 0)
+    assert oracle.rel_fro(oracle.logical_c(C, m, n, m), ref) < 1e-6
+    Cn = np.full(m * n, np.nan, np.float32)  # beta == 0: C must not be read
+    oracle.shgemm(oracle.FP16, 0, 0, m, n, k, 1.0, A, lda, B, ldb, 0.0, Cn, m, 0)
+    assert np.isfinite(Cn).all()
+
+
+def test_hsgemm_identity():
+    rng = np.random.default_rng(5)
+    m, n, k = 23, 31, 64
+    Ah = rng.uniform(-1, 1, m * k).astype(np.float16)  # m x k col-major
+    Bf = rng.uniform(-1, 1, k * n).astype(np.float32)  # k x n col-major
+    C = np.zeros(m * n, np.float32)
+    oracle.hsgemm(oracle.FP16, 0, 0, m, n, k, 1.0, Ah, m, Bf, k, 0.0, C, m, 0)
+    ref = Ah.astype(np.float64).reshape(k, m).T @ Bf.astype(np.float64).reshape(n, k).T
+    assert oracle.rel_fro(oracle.logical_c(C, m, n, m), ref) < 1e-6
+
+
+def test_wide_exponent_lo_term_underflow():
+    """Exponent-range probe (reference test/exponent_test.cu:249-252): A = 2^U(lo,hi)."""
+    rng = np.random.default_rng(11)
+    m = n = k = 64
+    B = rng.uniform(0, 1, k * n).astype(np.float16)
+    res = {}
+    for lo_e, hi_e in [(-15, 14), (-36, -15), (-100, -36)]:
+        A = np.exp2(rng.uniform(lo_e, hi_e, m * k)).astype(np.float32)
+        ref = oracle.dgemm_ref(0, 0, m, n, k, 1.0, A, m, B, k)
+        C = np.zeros(m * n, np.float32)
+        oracle.shgemm(oracle.FP16, 0, 0, m, n, k, 1.0, A, m, B, k, 0.0, C, m, 0)
+        res[(lo_e, hi_e)] = oracle.rel_fro(oracle.logical_c(C, m, n, m), ref)
+    assert res[(-15, 14)] < 1e-6
+    # below binary16's range the hi term vanishes and only the lo term carries
+    # the value, with ever fewer bits: the error grows, as in the reference
+    assert res[(-36, -15)] > res[(-15, 14)]
+    assert res[(-100, -36)] > 0.5
