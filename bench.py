@@ -1,0 +1,421 @@
+"""Benchmark of the SHGEMM hot path on B200.
+
+Default workload: large square SHGEMM m = n = k = 16384, op_n/op_n, FP32 operand
+N(0,1) * 2^U(-15,15), binary16 operand N(0,1), alpha = 1, beta = 0.5 with C
+uniform[-1, 1], fp16 compute (seeded synthetic data of that shape and
+distribution). One step = one SHGEMM call over the whole problem; inputs (1.5 GiB)
+exceed the 126 MB L2, so no flush is needed between steps.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload square16k|square1k|sketch]
+    python bench.py --impl reference ...   # the reference algorithm on the host cores
+
+Prints one JSON line (rank 0). Under torchrun (N > 1) every rank runs an
+independent replica (the path has no cross-GPU exchange); time is the max over
+ranks and `value` the aggregate.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+METRIC = "served TFLOP/s & p99 latency vs per-call SHGEMM; rel. error vs FP64"
+
+WORKLOADS = {
+    # the large square SHGEMM
+    "square16k": dict(m=16384, n=16384, k=16384, op_a=0, op_b=0, tc=0, alpha=1.0, beta=0.5, dist="wide",
+                      desc="large square SHGEMM 16384^3 NN, fp16 compute, A N(0,1)*2^U(-15,15), B N(0,1), beta=0.5"),
+    # a smaller square case of the same kernel, for profiler captures (inputs still exceed L2)
+    "square8k": dict(m=8192, n=8192, k=8192, op_a=0, op_b=0, tc=0, alpha=1.0, beta=0.5, dist="wide",
+                     desc="square SHGEMM 8192^3 NN, fp16 compute, A N(0,1)*2^U(-15,15), B N(0,1), beta=0.5"),
+    # small square SHGEMM
+    "square1k": dict(m=1024, n=1024, k=1024, op_a=0, op_b=0, tc=0, alpha=1.0, beta=0.0, dist="uniform",
+                     desc="plain SHGEMM 1024^3 NN, fp16 compute, A U[-1,1], B U[-1,1]"),
+    # Y = Omega^T A as hsgemm(op_t, op_n) -> internal shgemm(op_t, op_n, 4096, 256, 2^20, op_c = t)
+    "sketch": dict(m=4096, n=256, k=1 << 20, op_a=1, op_b=0, tc=0, alpha=1.0, beta=0.0, dist="sketch",
+                   desc="left sketch Y = Omega^T A, A 2^20 x 4096 FP32 (low rank + noise), Omega 2^20 x 256 "
+                        "binary16 N(0,1/256), split-K, fp16 compute", op_c=1),
+}
+
+
+def load_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return d, "measured"
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0}, "fallback"
+
+
+class ClockSampler:
+    """Samples nvidia-smi clocks and throttle reasons while the timed region runs."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            time.sleep(0.2)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [x.strip() for x in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def make_inputs(wl, dev, seed=0):
+    import torch
+
+    g = torch.Generator(device=dev)
+    g.manual_seed(seed)
+    m, n, k = wl["m"], wl["n"], wl["k"]
+    a_rows = m if wl["op_a"] == 0 else k
+    b_rows = k if wl["op_b"] == 0 else n
+    na = m * k
+    nb = k * n
+    if wl["dist"] == "wide":
+        A = torch.randn(na, generator=g, device=dev)
+        A.mul_(torch.exp2(torch.empty(na, device=dev).uniform_(-15, 15, generator=g)))
+        B = torch.randn(nb, generator=g, device=dev).to(torch.float16)
+    elif wl["dist"] == "sketch":
+        # A (k x m, K-contiguous for op_t) = U diag(sigma) V^T, rank 512, sigma_i = i^-2, + N(0, 1e-6) noise
+        r = 512
+        U = torch.linalg.qr(torch.randn(k, r, generator=g, device=dev))[0]
+        V = torch.linalg.qr(torch.randn(m, r, generator=g, device=dev))[0]
+        sig = torch.arange(1, r + 1, device=dev, dtype=torch.float32).pow(-2.0)
+        Amat = (U * sig) @ V.T  # k x m; column-major storage of an (a_rows=k) x m matrix = row-major m x k
+        Amat.add_(torch.randn(k, m, generator=g, device=dev), alpha=1e-6)
+        A = Amat.T.contiguous().reshape(-1)  # element (kk, i) at kk + i * k
+        del U, V, Amat
+        B = (torch.randn(nb, generator=g, device=dev) / 16.0).to(torch.float16)  # N(0, 1/256)
+    else:
+        A = torch.empty(na, device=dev).uniform_(-1, 1, generator=g)
+        B = torch.empty(nb, device=dev).uniform_(-1, 1, generator=g).to(torch.float16)
+    op_c = wl.get("op_c", 0)
+    c_rows = m if op_c == 0 else n
+    C = torch.empty(m * n, device=dev).uniform_(-1, 1, generator=g)
+    return A, a_rows, B, b_rows, C, c_rows
+
+
+def gpu_error(h, wl, A, lda, B, ldb, C_out, ldc, C0):
+    """Relative Frobenius error vs the FP64 product (GPU), plus FP32 SGEMM's (torch, no TF32)."""
+    import torch
+
+    from shgemm_b200 import evaluation as ev
+
+    m, n, k = wl["m"], wl["n"], wl["k"]
+    op_c = wl.get("op_c", 0)
+    c64 = ev.fp64_product(h, wl["op_a"], wl["op_b"], m, n, k, A, lda, B, ldb)
+    e = ev.error(h, m, n, C_out, ldc, c64, wl["alpha"], wl["beta"], C0 if wl["beta"] != 0 else None, op_c)
+    # plain FP32 SGEMM of the same inputs for comparison
+    torch.backends.cuda.matmul.allow_tf32 = False
+    Am = A.view(-1, lda).T if wl["op_a"] == 0 else A.view(-1, lda)  # logical m x k
+    Bm = B.float().view(-1, ldb).T if wl["op_b"] == 0 else B.float().view(-1, ldb)
+    S = Am[:m, :k] @ Bm[:k, :n]  # m x n
+    S = S.mul_(wl["alpha"])
+    if wl["beta"] != 0:
+        C0m = C0.view(-1, ldc).T[:m, :n] if op_c == 0 else C0.view(-1, ldc)[:m, :n]
+        S.add_(C0m, alpha=wl["beta"])
+    Sbuf = S.T.contiguous().reshape(-1) if op_c == 0 else S.contiguous().reshape(-1)
+    es = ev.error(h, m, n, Sbuf, m if op_c == 0 else n, c64, wl["alpha"], wl["beta"],
+                  C0 if wl["beta"] != 0 else None, op_c)
+    del c64, S, Sbuf
+    return {"rel_err_fp64": e["rel_fro"], "max_rel_err_fp64": e["max_rel"],
+            "nonfinite_mismatch": e["nonfinite_mismatch"], "sgemm_rel_err_fp64": es["rel_fro"]}
+
+
+def cpu_baseline(wl, seconds_target=12.0):
+    """The oracle's restated SHGEMM (C, OpenMP) on a bounded sample of the workload."""
+    import numpy as np
+
+    import oracle
+
+    rng = np.random.default_rng(0)
+    k = min(wl["k"], 16384)
+    ms = ns = 256
+    # grow the sample until it takes a few seconds
+    while True:
+        A = rng.standard_normal(ms * k).astype(np.float32)
+        B = rng.standard_normal(k * ns).astype(np.float16)
+        C = np.zeros(ms * ns, np.float32)
+        t0 = time.perf_counter()
+        oracle.shgemm(wl["tc"], 0, 0, ms, ns, k, 1.0, A, ms, B, k, 0.0, C, ms, 0, 0)
+        dt = time.perf_counter() - t0
+        if dt > seconds_target / 4 or ms >= 4096:
+            break
+        ms *= 2
+        ns *= 2
+    flops = 2.0 * ms * ns * k
+    return {"value": flops / dt / 1e12, "unit": "TFLOP/s", "cores": oracle.num_threads(), "kind": "port",
+            "sample": f"restated reference SHGEMM (oracle, fp64 fragment sums) {ms}x{ns}x{k}, "
+                      f"{dt:.2f} s, 2mnk effective flops"}
+
+
+def run_reference_arm(args, wl):
+    """--impl reference: the reference algorithm on the host cores (the reference itself
+    cannot be built: its arithmetic submodule is not vendored), bounded sample per step."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    import numpy as np
+
+    import oracle
+
+    rng = np.random.default_rng(0)
+    k = min(wl["k"], 16384)
+    ms = ns = 512
+    A = rng.standard_normal(ms * k).astype(np.float32)
+    B = rng.standard_normal(k * ns).astype(np.float16)
+    C = np.zeros(ms * ns, np.float32)
+    for _ in range(args.warmup):
+        oracle.shgemm(wl["tc"], 0, 0, ms, ns, k, 1.0, A, ms, B, k, 0.0, C, ms, 0, 0)
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        oracle.shgemm(wl["tc"], 0, 0, ms, ns, k, 1.0, A, ms, B, k, 0.0, C, ms, 0, 0)
+        times.append(time.perf_counter() - t0)
+    dt = sum(times)
+    flops = 2.0 * ms * ns * k * args.steps
+    value = flops / dt / 1e12
+    sample = f"{ms}x{ns}x{k} per step (restated reference SHGEMM, OpenMP, the workload's k)"
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "TFLOP/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * dt / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32 split to fp16/tf32", "data": "synthetic",
+            "config": {"workload": wl["desc"], "sample": sample},
+            "cpu_baseline": {"value": value, "unit": "TFLOP/s", "cores": oracle.num_threads(), "kind": "port",
+                             "sample": sample},
+            "e2e": {"value": value, "unit": "TFLOP/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "note": "reference not buildable (wmma_extension/cutf submodules absent); its algorithm is timed "
+                    "through the oracle port"}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="square16k", choices=sorted(WORKLOADS))
+    ap.add_argument("--tc", default=None, choices=["fp16", "tf32"])
+    ap.add_argument("--no-error", action="store_true", help="skip the FP64 error measurement")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer end-to-end measurement")
+    args = ap.parse_args()
+    wl = dict(WORKLOADS[args.workload])
+    if args.tc:
+        wl["tc"] = 0 if args.tc == "fp16" else 1
+    args.warmup = max(3, args.warmup)
+    if args.impl == "reference":
+        return run_reference_arm(args, wl)
+
+    import torch
+
+    import shgemm_b200 as sg
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    dev = torch.device(f"cuda:{local}")
+    torch.cuda.set_device(dev)
+
+    h = sg.Handle(local)
+    stream = torch.cuda.current_stream(dev)
+    h.set_stream(stream)
+    m, n, k = wl["m"], wl["n"], wl["k"]
+    op_c = wl.get("op_c", 0)
+    A, lda, B, ldb, C, ldc = make_inputs(wl, dev, seed=rank)
+    C0 = C.clone() if wl["beta"] != 0 else None
+
+    def step():
+        return sg.shgemm(h, wl["op_a"], wl["op_b"], m, n, k, wl["alpha"], A, lda, B, ldb, wl["beta"], C, ldc, wl["tc"],
+                         op_c)
+
+    for _ in range(args.warmup):
+        level = step()
+    torch.cuda.synchronize(dev)
+    if h.check_error() != 0:
+        raise RuntimeError("device-side timeout during warm-up")
+
+    # ---- timed region: device events on the launching stream, barrier + sync on both sides
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize(dev)
+    launches0 = h.launch_count()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        ev0.record(stream)
+        for _ in range(args.steps):
+            step()
+        ev1.record(stream)
+        torch.cuda.synchronize(dev)
+    launches = h.launch_count() - launches0
+    if dist:
+        dist.barrier()
+    ms_total = ev0.elapsed_time(ev1)
+    t = torch.tensor([ms_total], device=dev, dtype=torch.float64)
+    if dist:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_total = float(t.item())
+    ms_step = ms_total / args.steps
+    flops_eff = 2.0 * m * n * k
+    flops_issued = 4.0 * m * n * k
+    value = world * flops_eff * args.steps / (ms_total * 1e-3) / 1e12
+    if h.check_error() != 0:
+        raise RuntimeError("device-side timeout in the timed region")
+
+    # ---- error vs FP64 (outside the timed region; fresh C from the same C0)
+    err = {}
+    if not args.no_error:
+        if C0 is not None:
+            C.copy_(C0)
+        step()
+        torch.cuda.synchronize(dev)
+        err = gpu_error(h, wl, A, lda, B, ldb, C, ldc, C0)
+
+    # ---- end to end through the public API with host buffers (pinned), copies timed
+    e2e = None
+    if not args.no_e2e:
+        hA = torch.empty(A.numel(), dtype=A.dtype, pin_memory=True)
+        hB = torch.empty(B.numel(), dtype=B.dtype, pin_memory=True)
+        hC = torch.empty(C.numel(), dtype=C.dtype, pin_memory=True)
+        hA.copy_(A)
+        hB.copy_(B)
+        hC.copy_(C0 if C0 is not None else C)
+        h2d = hA.numel() * 4 + hB.numel() * 2 + (hC.numel() * 4 if wl["beta"] != 0 else 0)
+        d2h = hC.numel() * 4
+        e2e_steps = max(1, min(args.steps, 5))
+
+        def e2e_step():
+            A.copy_(hA, non_blocking=True)
+            B.copy_(hB, non_blocking=True)
+            if wl["beta"] != 0:
+                C.copy_(hC, non_blocking=True)
+            step()
+            hC.copy_(C, non_blocking=True)
+
+        e2e_step()
+        torch.cuda.synchronize(dev)
+        if dist:
+            dist.barrier()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(e2e_steps):
+            e2e_step()
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+        te = torch.tensor([e0.elapsed_time(e1)], device=dev, dtype=torch.float64)
+        if dist:
+            dist.all_reduce(te, op=dist.ReduceOp.MAX)
+        e2e = {"value": world * flops_eff * e2e_steps / (float(te.item()) * 1e-3) / 1e12, "unit": "TFLOP/s",
+               "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h), "steps": e2e_steps}
+        del hA, hB, hC
+
+    # ---- roofline of the tile kernel (its launches are the timed steps)
+    peaks, peak_kind = load_peaks()
+    peak = peaks.get("bf16_tflops", 1590.0)
+    achieved = flops_issued / (ms_step * 1e-3) / 1e12
+    roofline = {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
+                "traffic": None, "peak_kind": f"{peak_kind} bf16 dense burst",
+                "work_per_launch": f"4mnk = {flops_issued:.4e} issued tensor flops (two MMAs per k: hi and lo)"}
+    traffic_file = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(traffic_file):
+        with open(traffic_file) as f:
+            tr = json.load(f).get(args.workload + ("_tf32" if wl["tc"] else ""))
+        if tr:
+            roofline["traffic"] = tr
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        cpu = cpu_baseline(wl)
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "TFLOP/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32 split to fp16 (tensor) / f32 accumulate" if wl["tc"] == 0
+            else "f32 split to tf32 (tensor) / f32 accumulate",
+            "data": "synthetic (seeded, workload's shapes and distributions)",
+            "config": {"workload": wl["desc"], "m": m, "n": n, "k": k, "op_a": "NT"[wl["op_a"]],
+                       "op_b": "NT"[wl["op_b"]], "op_c": "NT"[op_c], "compute_type": ["fp16", "tf32"][wl["tc"]],
+                       "kernel_level": level, "l2": "inputs exceed L2 (no flush needed)",
+                       "parallelism": f"replicas x{world}"},
+            "issued_tflops": world * flops_issued * args.steps / (ms_total * 1e-3) / 1e12,
+            "gpu_launches": launches,
+            "roofline": roofline,
+            "clocks": clk.summary(),
+            "error": err,
+            "e2e": e2e,
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    h.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -26,7 +26,7 @@ struct shgemm_b200_handle {
     cudaStream_t stream = nullptr;
     unsigned debug_mode = 0;
     int fixed_level = SHGEMM_LEVEL_AUTO;
-    long long chunk_k = 256;
+    long long chunk_k = 0;  // 0: one k-step (4 UMMA instructions) per hi drain
     long long split_k = 0;
     long long wait_limit_ms = 2000;
     long long group_m = 8;
@@ -110,6 +110,19 @@ __global__ void scale_c_kernel(float* c, uint64_t ldc, int rows, int cols, float
         const int cc = static_cast<int>(idx / rows);
         float* d = c + r + static_cast<size_t>(cc) * ldc;
         *d = (beta == 0.0f) ? 0.0f : __fmul_rn(beta, *d);
+    }
+}
+
+// Copies a rows x cols column-major block into a buffer with a 16-byte aligned
+// leading dimension (the staging path for operands TMA cannot address).
+template <typename T>
+__global__ void pack_kernel(const T* __restrict__ src, uint64_t ld_src, T* __restrict__ dst, uint64_t ld_dst,
+                            int rows, int cols) {
+    const size_t total = static_cast<size_t>(rows) * cols;
+    for (size_t idx = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; idx < total;
+         idx += static_cast<size_t>(gridDim.x) * blockDim.x) {
+        const size_t r = idx % rows, c = idx / rows;
+        dst[r + c * ld_dst] = src[r + c * ld_src];
     }
 }
 
@@ -278,11 +291,11 @@ double wave_efficiency(long long units, int sms) {
     return static_cast<double>(units) / static_cast<double>(waves * sms);
 }
 
-Plan make_plan(const shgemm_b200_handle* h, size_t m, size_t n, size_t k, int tc) {
+Plan make_plan(const shgemm_b200_handle* h, size_t m, size_t n, size_t k, int tc, size_t ws_bytes) {
     Plan p{};
     const int bk = (tc == kFP16) ? 64 : 32;
     p.total_steps = static_cast<int>((k + bk - 1) / bk);
-    const long long chunk_k = std::max<long long>(bk, h->chunk_k);
+    const long long chunk_k = h->chunk_k <= 0 ? bk : std::max<long long>(bk, h->chunk_k);
     p.chunk_steps = static_cast<int>(std::max<long long>(1, chunk_k / bk));
     p.tiles_m = static_cast<int>((m + 127) / 128);
     // Level choice mirrors the reference (src/shgemm.cu:643-656): the large tile when it
@@ -312,7 +325,7 @@ Plan make_plan(const shgemm_b200_handle* h, size_t m, size_t n, size_t k, int tc
     // The workspace bounds the slice count (no allocation inside a call).
     const size_t per_slice = m * n * sizeof(float);
     if (slices > 1 && per_slice > 0) {
-        const size_t fit = h->workspace_bytes / per_slice;
+        const size_t fit = ws_bytes / per_slice;
         if (fit < 2) slices = 1;
         else if (static_cast<size_t>(slices) > fit) slices = static_cast<int>(fit);
     }
@@ -422,7 +435,7 @@ int shgemm_b200_set_config(shgemm_b200_handle_t h, int key, long long v) {
     if (!h) return SHGEMM_STATUS_INVALID_VALUE;
     switch (key) {
         case SHGEMM_CFG_CHUNK_K:
-            if (v < 64 || v % 64) return SHGEMM_STATUS_INVALID_VALUE;
+            if (v < 0 || v % 32) return SHGEMM_STATUS_INVALID_VALUE;
             h->chunk_k = v;
             return SHGEMM_STATUS_OK;
         case SHGEMM_CFG_SPLIT_K:
@@ -498,41 +511,12 @@ int shgemm_b200_selftest_wait_timeout(shgemm_b200_handle_t h, unsigned limit_us,
     return st;
 }
 
-int shgemm_b200_shgemm(shgemm_b200_handle_t h, int op_a, int op_b, size_t m, size_t n, size_t k,
-                       const float* alpha_ptr, const float* a, size_t lda, const void* b, size_t ldb,
-                       const float* beta_ptr, float* c, size_t ldc, int tc, int op_c, int* level_out) {
-    if (!h || !alpha_ptr || !beta_ptr) return SHGEMM_STATUS_INVALID_VALUE;
-    if ((op_a != kOpN && op_a != kOpT) || (op_b != kOpN && op_b != kOpT) || (op_c != kOpN && op_c != kOpT) ||
-        (tc != kFP16 && tc != kTF32))
-        return SHGEMM_STATUS_INVALID_VALUE;
-    if (m == 0 || n == 0) {
-        if (level_out) *level_out = SHGEMM_LEVEL_P0;
-        return SHGEMM_STATUS_OK;
-    }
-    const size_t a_rows = (op_a == kOpN) ? m : k;
-    const size_t b_rows = (op_b == kOpN) ? k : n;
-    const size_t c_rows = (op_c == kOpN) ? m : n;
-    if (!c || ldc < c_rows) return SHGEMM_STATUS_INVALID_VALUE;
-    if (k > 0 && (!a || !b || lda < std::max<size_t>(1, a_rows) || ldb < std::max<size_t>(1, b_rows)))
-        return SHGEMM_STATUS_INVALID_VALUE;
-    if (m >= (1u << 31) || n >= (1u << 31) || k >= (1u << 31)) return SHGEMM_STATUS_NOT_SUPPORTED;
-    const float alpha = *alpha_ptr, beta = *beta_ptr;
-    DeviceGuard g(h->device);
+}  // extern "C"
 
-    if (k == 0) {  // empty product: C = beta * C
-        const size_t rows = c_rows, cols = (op_c == kOpN) ? n : m;
-        const int blocks = static_cast<int>(std::min<size_t>((rows * cols + 255) / 256, 4096));
-        scale_c_kernel<<<blocks, 256, 0, h->stream>>>(c, ldc, static_cast<int>(rows), static_cast<int>(cols), beta);
-        h->launches++;
-        if (level_out) *level_out = SHGEMM_LEVEL_P0;
-        return launch_status();
-    }
-    // TMA needs 16-byte aligned bases and leading dimensions.
-    if ((reinterpret_cast<uintptr_t>(a) & 15) || (reinterpret_cast<uintptr_t>(b) & 15) || (lda * 4) % 16 ||
-        (ldb * 2) % 16)
-        return SHGEMM_STATUS_NOT_SUPPORTED;
-
-    const Plan pl = make_plan(h, m, n, k, tc);
+static int run_tiled(shgemm_b200_handle_t h, int op_a, int op_b, size_t m, size_t n, size_t k, float alpha,
+                     const float* a, size_t lda, const void* b, size_t ldb, float beta, float* c, size_t ldc, int tc,
+                     int op_c, int* level_out, float* splitk_ws, size_t splitk_bytes) {
+    const Plan pl = make_plan(h, m, n, k, tc, splitk_bytes);
     const bool a_kmajor = (op_a == kOpT);
     const bool b_kmajor = (op_b == kOpN);
     const int bk = (tc == kFP16) ? 64 : 32;
@@ -568,7 +552,7 @@ int shgemm_b200_shgemm(shgemm_b200_handle_t h, int op_a, int op_b, size_t m, siz
 
     P.c = c;
     P.ldc = ldc;
-    P.workspace = h->workspace;
+    P.workspace = splitk_ws;
     P.error_flag = h->error_word;
     P.wait_limit_ns = static_cast<uint64_t>(h->wait_limit_ms) * 1000000ull;
     P.m = static_cast<int>(m);
@@ -603,12 +587,117 @@ int shgemm_b200_shgemm(shgemm_b200_handle_t h, int op_a, int op_b, size_t m, siz
     if (pl.slices > 1) {
         const size_t mn = m * n;
         const int blocks = static_cast<int>(std::min<size_t>((mn + 255) / 256, size_t(h->num_sms) * 8));
-        splitk_reduce_kernel<<<blocks, 256, 0, h->stream>>>(h->workspace, pl.slices, P.m, P.n, c, ldc, op_c, alpha,
+        splitk_reduce_kernel<<<blocks, 256, 0, h->stream>>>(splitk_ws, pl.slices, P.m, P.n, c, ldc, op_c, alpha,
                                                             beta);
         h->launches++;
         if (launch_status() != SHGEMM_STATUS_OK) return SHGEMM_STATUS_LAUNCH_FAILED;
     }
     if (level_out) *level_out = (pl.slices > 1) ? SHGEMM_LEVEL_P0 : pl.level;
+    return SHGEMM_STATUS_OK;
+}
+
+static size_t round_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
+
+template <typename T>
+static void launch_pack(shgemm_b200_handle_t h, const T* src, size_t ld_src, T* dst, size_t ld_dst, size_t rows,
+                        size_t cols) {
+    const size_t total = rows * cols;
+    const int blocks = static_cast<int>(std::min<size_t>((total + 255) / 256, size_t(h->num_sms) * 16));
+    pack_kernel<T><<<blocks, 256, 0, h->stream>>>(src, ld_src, dst, ld_dst, static_cast<int>(rows),
+                                                  static_cast<int>(cols));
+    h->launches++;
+}
+
+extern "C" {
+
+int shgemm_b200_shgemm(shgemm_b200_handle_t h, int op_a, int op_b, size_t m, size_t n, size_t k,
+                       const float* alpha_ptr, const float* a, size_t lda, const void* b, size_t ldb,
+                       const float* beta_ptr, float* c, size_t ldc, int tc, int op_c, int* level_out) {
+    if (!h || !alpha_ptr || !beta_ptr) return SHGEMM_STATUS_INVALID_VALUE;
+    if ((op_a != kOpN && op_a != kOpT) || (op_b != kOpN && op_b != kOpT) || (op_c != kOpN && op_c != kOpT) ||
+        (tc != kFP16 && tc != kTF32))
+        return SHGEMM_STATUS_INVALID_VALUE;
+    if (m == 0 || n == 0) {
+        if (level_out) *level_out = SHGEMM_LEVEL_P0;
+        return SHGEMM_STATUS_OK;
+    }
+    const size_t a_rows = (op_a == kOpN) ? m : k;
+    const size_t b_rows = (op_b == kOpN) ? k : n;
+    const size_t c_rows = (op_c == kOpN) ? m : n;
+    if (!c || ldc < c_rows) return SHGEMM_STATUS_INVALID_VALUE;
+    if (k > 0 && (!a || !b || lda < std::max<size_t>(1, a_rows) || ldb < std::max<size_t>(1, b_rows)))
+        return SHGEMM_STATUS_INVALID_VALUE;
+    if (m >= (1u << 31) || n >= (1u << 31) || k >= (1u << 31)) return SHGEMM_STATUS_NOT_SUPPORTED;
+    const float alpha = *alpha_ptr, beta = *beta_ptr;
+    DeviceGuard g(h->device);
+
+    if (k == 0) {  // empty product: C = beta * C
+        const size_t rows = c_rows, cols = (op_c == kOpN) ? n : m;
+        const int blocks = static_cast<int>(std::min<size_t>((rows * cols + 255) / 256, 4096));
+        scale_c_kernel<<<blocks, 256, 0, h->stream>>>(c, ldc, static_cast<int>(rows), static_cast<int>(cols), beta);
+        h->launches++;
+        if (level_out) *level_out = SHGEMM_LEVEL_P0;
+        return launch_status();
+    }
+    // TMA addresses 16-byte aligned bases with 16-byte aligned leading dimensions.
+    const bool pack_a = (reinterpret_cast<uintptr_t>(a) & 15) || (lda * 4) % 16;
+    const bool pack_b = (reinterpret_cast<uintptr_t>(b) & 15) || (ldb * 2) % 16;
+    if (!pack_a && !pack_b)
+        return run_tiled(h, op_a, op_b, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc, tc, op_c, level_out,
+                         h->workspace, h->workspace_bytes);
+
+    // Staging path: copy the unaligned operand(s) slab by slab (k-slabs of a multiple
+    // of 64) into the handle's workspace with aligned leading dimensions, then run the
+    // tile kernel per slab, accumulating into C (beta for the first slab, 1 after).
+    auto a_bytes = [&](size_t kb) { return pack_a ? (op_a == kOpN ? round_up(m, 4) * kb : round_up(kb, 4) * m) * 4 : 0; };
+    auto b_bytes = [&](size_t kb) { return pack_b ? (op_b == kOpN ? round_up(kb, 8) * n : round_up(n, 8) * kb) * 2 : 0; };
+    size_t kb = k;
+    while (round_up(a_bytes(kb), 256) + round_up(b_bytes(kb), 256) > h->workspace_bytes) {
+        if (kb <= 64) return SHGEMM_STATUS_NOT_SUPPORTED;  // even one 64-deep slab does not fit
+        kb = std::max<size_t>(64, round_up(kb / 2, 64));
+    }
+    float* a_st = h->workspace;
+    __half* b_st = reinterpret_cast<__half*>(reinterpret_cast<char*>(h->workspace) + round_up(a_bytes(kb), 256));
+    int level = SHGEMM_LEVEL_P0;
+    for (size_t k0 = 0; k0 < k; k0 += kb) {
+        const size_t kk = std::min(kb, k - k0);
+        const float* as;
+        size_t lda_s;
+        if (pack_a) {
+            if (op_a == kOpN) {
+                lda_s = round_up(m, 4);
+                launch_pack<float>(h, a + k0 * lda, lda, a_st, lda_s, m, kk);
+            } else {
+                lda_s = round_up(kk, 4);
+                launch_pack<float>(h, a + k0, lda, a_st, lda_s, kk, m);
+            }
+            as = a_st;
+        } else {
+            as = (op_a == kOpN) ? a + k0 * lda : a + k0;
+            lda_s = lda;
+        }
+        const __half* bh = static_cast<const __half*>(b);
+        const __half* bs;
+        size_t ldb_s;
+        if (pack_b) {
+            if (op_b == kOpN) {
+                ldb_s = round_up(kk, 8);
+                launch_pack<__half>(h, bh + k0, ldb, b_st, ldb_s, kk, n);
+            } else {
+                ldb_s = round_up(n, 8);
+                launch_pack<__half>(h, bh + k0 * ldb, ldb, b_st, ldb_s, n, kk);
+            }
+            bs = b_st;
+        } else {
+            bs = (op_b == kOpN) ? bh + k0 : bh + k0 * ldb;
+            ldb_s = ldb;
+        }
+        if (launch_status() != SHGEMM_STATUS_OK) return SHGEMM_STATUS_LAUNCH_FAILED;
+        const int st = run_tiled(h, op_a, op_b, m, n, kk, alpha, as, lda_s, bs, ldb_s, k0 == 0 ? beta : 1.0f, c,
+                                 ldc, tc, op_c, &level, nullptr, 0);
+        if (st != SHGEMM_STATUS_OK) return st;
+    }
+    if (level_out) *level_out = level;
     return SHGEMM_STATUS_OK;
 }
 

@@ -187,18 +187,44 @@ def test_kernel_level_fixing(h, level):
     K.assert_parity(r)
 
 
-def test_unaligned_leading_dimension_is_rejected(h):
+@pytest.mark.parametrize("tc", [oracle.FP16, oracle.TF32])
+def test_unaligned_operands_go_through_staging(h, tc):
+    """Leading dimensions / base addresses TMA cannot address (the reference accepts
+    any ld, src/dmem_accessor.hpp:15-146) are staged into the workspace."""
     import torch
 
     import shgemm_b200 as sg
 
-    m, n, k = 33, 17, 35
-    A = torch.zeros(m * k + 8, device="cuda")
-    B = torch.zeros(k * n + 8, device="cuda", dtype=torch.float16)
-    C = torch.zeros(m * n + 8, device="cuda")
-    with pytest.raises(sg.ShgemmError) as ei:
-        sg.shgemm(h, 0, 0, m, n, k, 1.0, A, m, B, k, 0.0, C, m, sg.fp16)
-    assert ei.value.status == 2
+    rng = np.random.default_rng(41)
+    m, n, k = 75, 61, 333
+    inp = K.make_inputs(rng, m, n, k, 0, 0, 0, pad=3)  # lda = 78, ldb = 336: unaligned A
+    A = np.concatenate([[np.float32(0)], inp["A"]])  # shift the base by 4 bytes
+    B = np.concatenate([[np.float16(0)], inp["B"]])  # and B's by 2 bytes
+    dA = torch.from_numpy(A).cuda()
+    dB = torch.from_numpy(B.view(np.int16)).cuda().view(torch.float16)
+    dC = torch.from_numpy(inp["C"].copy()).cuda()
+    sg.shgemm(h, 0, 0, m, n, k, 1.0, dA.data_ptr() + 4, inp["lda"], dB.data_ptr() + 2, inp["ldb"], 0.25, dC,
+              inp["ldc"], tc)
+    torch.cuda.synchronize()
+    gpu_c = dC.cpu().numpy()
+    orc = K.run_oracle(tc, 0, 0, m, n, k, 1.0, inp, 0.25, 0, chunk=0)
+    ref = K.fp64(0, 0, m, n, k, 1.0, inp, 0.25, 0)
+    sgc = K.sgemm(0, 0, m, n, k, 1.0, inp, 0.25, 0)
+    K.assert_parity(K.parity_report(gpu_c, orc, ref, sgc, m, n, inp["ldc"], 0))
+
+
+def test_staging_in_k_slabs_with_small_workspace(cuda_device):
+    """With a workspace too small for the whole staged operand the product runs in
+    k-slabs accumulated into C."""
+    import shgemm_b200 as sg
+
+    hd = sg.Handle(0)
+    try:
+        hd.set_workspace_size(1 << 20)
+        r, _, _ = _parity(hd, oracle.FP16, 1, 0, 0, 301, 77, 3001, beta=0.5, seed=8)
+        K.assert_parity(r)
+    finally:
+        hd.close()
 
 
 def test_bounded_wait_times_out_and_context_survives(h):
