@@ -42,8 +42,6 @@ enum {
 /* Tunables for shgemm_b200_set_config (no reference counterpart; the
  * reference fixes these at compile time in its tile tables, src/shgemm.cu:429-488). */
 enum {
-    SHGEMM_CFG_CHUNK_K = 1,       /* k elements per hi-accumulator drain, rounded to whole k-steps
-                                     (64 fp16 / 32 tf32); 0 = one k-step (default) */
     SHGEMM_CFG_SPLIT_K = 2,       /* 0 = automatic, 1 = never split, s > 1 = force s slices */
     SHGEMM_CFG_WAIT_LIMIT_MS = 3, /* bound on every in-kernel wait (default 2000 ms) */
     SHGEMM_CFG_GROUP_M = 4        /* tile rasterisation group along m (default 8) */

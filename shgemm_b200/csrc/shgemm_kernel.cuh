@@ -3,27 +3,36 @@
 // C = alpha * op(A) * op(B) + beta * C, A FP32, B binary16, column-major.
 // The error-corrected method of the reference (src/wmmae_shgemm.hpp:11-125):
 // the FP32 operand is split on the fly into hi = T(a) and lo = T(2^11 (a - hi))
-// with T = binary16 or TF32; hi*B and lo*B are issued as two tcgen05 MMAs into
-// separate TMEM accumulators. The hi accumulator is restarted every k-chunk and
-// drained into registers, where chunks are summed with round-to-nearest FP32
-// adds (the reference adds every k-fragment's hi product the same way, which
-// avoids the tensor core's truncating accumulation); lo accumulates over the
-// whole k range and is folded in once at the end as hi + lo * 2^-11
-// (tcec store_matrix_sync, call site src/shgemm.cu:87-99). The epilogue applies
-// alpha/beta like src/dmem_accessor.hpp:187-356 (C is not read when beta == 0)
-// or, for split-K, writes the slice's partial to a workspace that a separate
-// kernel reduces in fixed slice order.
+// with T = binary16 or TF32, and hi*B and lo*B are issued as tensor-core MMAs.
+// The reference forms every k-fragment's hi product in a zeroed accumulator and
+// adds it to its FP32 running sum with a round-to-nearest add, avoiding the
+// tensor core's truncating accumulation; lo accumulates on the tensor core and
+// is folded in as hi + lo * 2^-11 (tcec store_matrix_sync, src/shgemm.cu:87-99).
 //
-// Warp roles (448 threads, one CTA per SM):
-//   warp 0      TMA producer: raw FP32 A tile + binary16 B tile per k-step
-//   warp 1      TMEM allocator + single-thread UMMA issuer
-//   warps 2-5   split warpgroup: thread t owns tile row t; writes hi/lo (and,
-//               for TF32, the widened B) as 128B-swizzled K-major UMMA tiles
-//   warps 6-13  epilogue: TMEM lane quadrant (warp % 4) x column half
-// Pipelines: load ring (TMA -> split/MMA), split ring (split -> MMA), two hi
-// TMEM buffers (MMA <-> epilogue ping-pong per k-chunk), two lo TMEM buffers
-// (alternating per tile). Every wait is bounded; on timeout the kernel records
-// an error code, drains its own in-flight copies and MMAs, frees TMEM and exits.
+// Here every k-step (one 128-byte swizzle row: 64 binary16 / 32 TF32 values of
+// k, four UMMA instructions per operand) is one drain chunk:
+//   D  = sum lo*B            (4 UMMAs into a fresh TMEM accumulator)
+//   D  = hi_0*B + D * 2^-11  (UMMA with scale-input-d = 11)
+//   D += hi_k*B              (3 more UMMAs)
+// so D holds the chunk's hi product plus its 2^-11-scaled lo product; the
+// epilogue warps drain D from TMEM every chunk and add it to FP32 registers
+// with round-to-nearest adds. D is double-buffered in TMEM (2 x BN columns),
+// so the next chunk's MMAs overlap the drain. The epilogue applies alpha/beta
+// like src/dmem_accessor.hpp:187-356 (C is not read when beta == 0) or, for
+// split-K, writes the slice's partial to a workspace that a separate kernel
+// reduces in fixed slice order.
+//
+// Warp roles (512 threads, one CTA per SM, registers rebalanced per warpgroup):
+//   warp 0       TMA producer: raw FP32 A tile and binary16 B tile per k-step
+//   warp 1       TMEM allocator + single-thread UMMA issuer
+//   warps 2-7    split: turn the raw FP32 tile into 128B-swizzled hi/lo UMMA
+//                tiles (K-major when A is K-contiguous, MN-major for binary16
+//                when it is M-contiguous) and, for TF32, widen B to TF32
+//   warps 8-15   epilogue: TMEM lane quadrant (warp % 4) x column half
+// Rings: A (TMA -> split), B (TMA -> MMA; TMA -> split for TF32), split tiles
+// (split -> MMA), D (MMA <-> epilogue). Every wait is bounded; on timeout the
+// kernel records an error code, drains its own in-flight copies and MMAs, frees
+// TMEM and exits.
 #pragma once
 #include "ptx.cuh"
 
@@ -57,7 +66,6 @@ struct alignas(64) TileGemmParams {
     int steps_per_slice;  // k-steps per slice
     int num_units;        // tiles_m * tiles_n * num_slices
     int group_m;          // rasterisation group along m
-    int chunk_steps;      // k-steps per hi-accumulator drain
 };
 
 template <int TC, int BN_, bool A_KMAJOR, bool B_KMAJOR>
@@ -67,26 +75,31 @@ struct TileCfg {
     static constexpr bool kTf32 = (TC == kTF32);
     static constexpr int BK = kTf32 ? 32 : 64;  // one 128-byte swizzle row of the compute type
     static constexpr int UMMA_K = kTf32 ? 8 : 16;
-    static constexpr int KSUB = BK / UMMA_K;  // MMAs per operand pair per k-step
+    static constexpr int KSUB = BK / UMMA_K;  // UMMAs per operand per k-step
     static constexpr int A_RAW = BM * BK * 4;
     static constexpr int B_RAW = BN * BK * 2;
-    static constexpr int LOAD_STAGE = A_RAW + B_RAW;
     static constexpr int HI_BYTES = BM * 128;  // BM rows of 128 bytes (both modes)
     static constexpr int BT_BYTES = kTf32 ? BN * 128 : 0;
+    // MN-major hi/lo tiles (binary16, M-contiguous A): 64-wide m atoms of BK k rows.
+    static constexpr int MN_ATOM_BYTES = BK * 128;
     static constexpr int SPLIT_STAGE = 2 * HI_BYTES + BT_BYTES;
-    static constexpr int SPLIT_STAGES = 2;
-    static constexpr int SMEM_BUDGET = 220 * 1024;
-    static constexpr int LS_FIT = (SMEM_BUDGET - SPLIT_STAGES * SPLIT_STAGE) / LOAD_STAGE;
-    static constexpr int LOAD_STAGES = LS_FIT > 6 ? 6 : LS_FIT;
-    static_assert(LOAD_STAGES >= 2, "shared memory budget");
-    static constexpr int NUM_THREADS = 448;
-    static constexpr int TMEM_COLS = 512;
-    static constexpr int HALF_N = BN / 2;  // columns per epilogue warp
+    static constexpr int SMEM_BUDGET = 224 * 1024;
+    static constexpr int SS = kTf32 ? 3 : (BN == 256 ? 2 : 3);
+    static constexpr int SA = kTf32 ? 3 : 2;
+    static constexpr int SB_FIT = (SMEM_BUDGET - SS * SPLIT_STAGE - SA * A_RAW) / B_RAW;
+    static constexpr int SB = SB_FIT > 6 ? 6 : SB_FIT;
+    static_assert(SB >= 2, "shared memory budget");
+    static constexpr int NUM_THREADS = 512;
+    static constexpr int SPLIT_WARPS = 6;
+    static constexpr int SPLIT_THREADS = 32 * SPLIT_WARPS;
+    static constexpr int EPI_WARP0 = 8;
+    static constexpr int TMEM_COLS = 2 * BN < 32 ? 32 : 2 * BN;  // D ping-pong
+    static constexpr int HALF_N = BN / 2;                        // columns per epilogue warp
     static constexpr int BAR_BYTES = 1024;
-    static constexpr int SMEM_BYTES =
-        LOAD_STAGES * LOAD_STAGE + SPLIT_STAGES * SPLIT_STAGE + BAR_BYTES + 1024 /*alignment slack*/;
-    static_assert(BN == 64 || BN == 128, "tile N");
-    static_assert(LOAD_STAGE % 1024 == 0 && SPLIT_STAGE % 1024 == 0, "1024B-aligned stages");
+    static constexpr int SMEM_BYTES = SA * A_RAW + SB * B_RAW + SS * SPLIT_STAGE + BAR_BYTES + 1024;
+    static_assert(BN == 64 || BN == 128 || (BN == 256 && !kTf32), "tile N");
+    static_assert(A_RAW % 1024 == 0 && B_RAW % 1024 == 0 && SPLIT_STAGE % 1024 == 0, "1024B-aligned stages");
+    static_assert(SMEM_BYTES <= 232448, "dynamic shared memory limit");
 };
 
 __device__ __forceinline__ void decode_unit(const TileGemmParams& p, int u, int& tm, int& tn, int& slice) {
@@ -107,29 +120,176 @@ __device__ __forceinline__ void step_range(const TileGemmParams& p, int slice, i
     s1 = min(s0 + p.steps_per_slice, total_steps);
 }
 
+// ---------------------------------------------------------------------------
+// Split helpers. hi = T(v), lo = T(2^11 (v - hi)), T = binary16 round-to-nearest-
+// even or TF32 round-to-nearest-away: the reference's split (src/wmmae_shgemm.hpp:30-31).
+__device__ __forceinline__ void split8_f16(const float (&v)[8], uint4& hi, uint4& lo) {
+    uint32_t h[4], l[4];
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+        const __half2 hh = __floats2half2_rn(v[2 * e], v[2 * e + 1]);
+        const float2 hf = __half22float2(hh);
+        const __half2 ll = __floats2half2_rn(__fmul_rn(__fsub_rn(v[2 * e], hf.x), 2048.0f),
+                                             __fmul_rn(__fsub_rn(v[2 * e + 1], hf.y), 2048.0f));
+        h[e] = *reinterpret_cast<const uint32_t*>(&hh);
+        l[e] = *reinterpret_cast<const uint32_t*>(&ll);
+    }
+    hi = make_uint4(h[0], h[1], h[2], h[3]);
+    lo = make_uint4(l[0], l[1], l[2], l[3]);
+}
+
+__device__ __forceinline__ void split4_tf32(const float4 x, float4& hi, float4& lo) {
+    hi.x = ptx::to_tf32_rna(x.x);
+    hi.y = ptx::to_tf32_rna(x.y);
+    hi.z = ptx::to_tf32_rna(x.z);
+    hi.w = ptx::to_tf32_rna(x.w);
+    lo.x = ptx::to_tf32_rna(__fmul_rn(__fsub_rn(x.x, hi.x), 2048.0f));
+    lo.y = ptx::to_tf32_rna(__fmul_rn(__fsub_rn(x.y, hi.y), 2048.0f));
+    lo.z = ptx::to_tf32_rna(__fmul_rn(__fsub_rn(x.z, hi.z), 2048.0f));
+    lo.w = ptx::to_tf32_rna(__fmul_rn(__fsub_rn(x.w, hi.w), 2048.0f));
+}
+
+// Split of one raw FP32 A tile (one k-step) by the split warps (thread sidx).
+template <class Cfg, bool A_KMAJOR>
+__device__ __forceinline__ void split_tile(const uint8_t* a_raw, uint8_t* hi_t, uint8_t* lo_t, int sidx) {
+    if constexpr (!Cfg::kTf32) {
+        if constexpr (A_KMAJOR) {
+            // raw: two [128 rows][32 floats] 128B-swizzled sub-tiles (k 0-31, 32-63);
+            // out: [128 rows][64 halves] K-major, 128B swizzle. Unit: (row, 16-byte chunk c).
+            for (int u = sidx; u < 1024; u += Cfg::SPLIT_THREADS) {
+                const int row = u & 127, c = u >> 7, sw = row & 7;
+                const uint8_t* rp = a_raw + (c >> 2) * (Cfg::BM * 128) + row * 128;
+                const int j0 = (c & 3) * 2;
+                const float4 x0 = *reinterpret_cast<const float4*>(rp + ((j0 ^ sw) << 4));
+                const float4 x1 = *reinterpret_cast<const float4*>(rp + (((j0 + 1) ^ sw) << 4));
+                const float v[8] = {x0.x, x0.y, x0.z, x0.w, x1.x, x1.y, x1.z, x1.w};
+                uint4 h, l;
+                split8_f16(v, h, l);
+                const int off = row * 128 + ((c ^ sw) << 4);
+                *reinterpret_cast<uint4*>(hi_t + off) = h;
+                *reinterpret_cast<uint4*>(lo_t + off) = l;
+            }
+        } else {
+            // raw: [64 k][128 m] floats (512-byte rows); out: MN-major, two atoms of
+            // [64 k rows][64 m halves], 128B swizzle. Unit: (k, group g of 8 consecutive m).
+            for (int u = sidx; u < 1024; u += Cfg::SPLIT_THREADS) {
+                const int g = u & 15, k = u >> 4;
+                const int first = (g >> 2) & 1;  // read order that keeps 8-thread phases conflict-free
+                const uint8_t* rp = a_raw + k * 512 + g * 32;
+                const float4 xa = *reinterpret_cast<const float4*>(rp + 16 * first);
+                const float4 xb = *reinterpret_cast<const float4*>(rp + 16 * (1 - first));
+                const float4 x0 = first ? xb : xa;
+                const float4 x1 = first ? xa : xb;
+                const float v[8] = {x0.x, x0.y, x0.z, x0.w, x1.x, x1.y, x1.z, x1.w};
+                uint4 h, l;
+                split8_f16(v, h, l);
+                const int off = (g >> 3) * Cfg::MN_ATOM_BYTES + k * 128 + (((g & 7) ^ (k & 7)) << 4);
+                *reinterpret_cast<uint4*>(hi_t + off) = h;
+                *reinterpret_cast<uint4*>(lo_t + off) = l;
+            }
+        }
+    } else {
+        if constexpr (A_KMAJOR) {
+            // raw: [128 rows][32 floats] 128B-swizzled; out: the same layout in TF32.
+            for (int u = sidx; u < 1024; u += Cfg::SPLIT_THREADS) {
+                const int row = u & 127, c = u >> 7;
+                const int off = row * 128 + ((c ^ (row & 7)) << 4);
+                float4 h, l;
+                split4_tf32(*reinterpret_cast<const float4*>(a_raw + off), h, l);
+                *reinterpret_cast<float4*>(hi_t + off) = h;
+                *reinterpret_cast<float4*>(lo_t + off) = l;
+            }
+        } else {
+            // raw: [32 k][128 m] floats; out: K-major [128 rows][32] TF32 (128B swizzle),
+            // transposed in registers 4 m x 4 k at a time. Unit: (m group g of 4, k group kq of 4).
+            for (int u = sidx; u < 256; u += Cfg::SPLIT_THREADS) {
+                const int g = u & 31, kq = u >> 5;
+                float4 h[4], l[4];  // h[j]: k = 4kq + j, m = 4g .. 4g+3
+#pragma unroll
+                for (int j = 0; j < 4; ++j)
+                    split4_tf32(*reinterpret_cast<const float4*>(a_raw + (kq * 4 + j) * 512 + g * 16), h[j], l[j]);
+                // rotate the row order so 8-thread store phases hit distinct 16-byte bank groups
+#pragma unroll
+                for (int r = 0; r < 4; ++r) {
+                    const int rr = (r + (g >> 1)) & 3;
+                    const int row = 4 * g + rr;
+                    const float4 hv = rr == 0   ? make_float4(h[0].x, h[1].x, h[2].x, h[3].x)
+                                      : rr == 1 ? make_float4(h[0].y, h[1].y, h[2].y, h[3].y)
+                                      : rr == 2 ? make_float4(h[0].z, h[1].z, h[2].z, h[3].z)
+                                                : make_float4(h[0].w, h[1].w, h[2].w, h[3].w);
+                    const float4 lv = rr == 0   ? make_float4(l[0].x, l[1].x, l[2].x, l[3].x)
+                                      : rr == 1 ? make_float4(l[0].y, l[1].y, l[2].y, l[3].y)
+                                      : rr == 2 ? make_float4(l[0].z, l[1].z, l[2].z, l[3].z)
+                                                : make_float4(l[0].w, l[1].w, l[2].w, l[3].w);
+                    const int off = row * 128 + ((kq ^ (row & 7)) << 4);
+                    *reinterpret_cast<float4*>(hi_t + off) = hv;
+                    *reinterpret_cast<float4*>(lo_t + off) = lv;
+                }
+            }
+        }
+    }
+}
+
+// TF32 mode: widen the binary16 B tile (exact in TF32) into a K-major [BN][32]
+// TF32 tile with a 128B swizzle. Unit: (row n, 16-byte chunk).
+template <class Cfg, bool B_KMAJOR>
+__device__ __forceinline__ void widen_b_tile(const uint8_t* b_raw, uint8_t* bt, int sidx) {
+    constexpr int BN = Cfg::BN;
+    if constexpr (B_KMAJOR) {
+        // raw: [BN][32] binary16, 64-byte rows, 64B swizzle; one raw 16-byte chunk
+        // (8 values) makes two output chunks.
+        for (int u = sidx; u < BN * 4; u += Cfg::SPLIT_THREADS) {
+            const int n = u % BN, rc = u / BN, sw = n & 7;
+            const uint4 hx = *reinterpret_cast<const uint4*>(b_raw + n * 64 + ((rc ^ ((n >> 1) & 3)) << 4));
+            const __half2* hp = reinterpret_cast<const __half2*>(&hx);
+            const float2 f0 = __half22float2(hp[0]);
+            const float2 f1 = __half22float2(hp[1]);
+            const float2 f2 = __half22float2(hp[2]);
+            const float2 f3 = __half22float2(hp[3]);
+            *reinterpret_cast<float4*>(bt + n * 128 + (((2 * rc) ^ sw) << 4)) = make_float4(f0.x, f0.y, f1.x, f1.y);
+            *reinterpret_cast<float4*>(bt + n * 128 + (((2 * rc + 1) ^ sw) << 4)) = make_float4(f2.x, f2.y, f3.x, f3.y);
+        }
+    } else {
+        // raw: [32 k][BN] binary16, no swizzle
+        const __half* bh = reinterpret_cast<const __half*>(b_raw);
+        for (int u = sidx; u < BN * 8; u += Cfg::SPLIT_THREADS) {
+            const int n = u % BN, c = u / BN;
+            float4 f;
+            f.x = __half2float(bh[(c * 4 + 0) * BN + n]);
+            f.y = __half2float(bh[(c * 4 + 1) * BN + n]);
+            f.z = __half2float(bh[(c * 4 + 2) * BN + n]);
+            f.w = __half2float(bh[(c * 4 + 3) * BN + n]);
+            *reinterpret_cast<float4*>(bt + n * 128 + ((c ^ (n & 7)) << 4)) = f;
+        }
+    }
+}
+
 template <int TC, int BN, bool A_KMAJOR, bool B_KMAJOR>
-__global__ void __launch_bounds__(448, 1) shgemm_tile_kernel(const __grid_constant__ TileGemmParams p) {
+__global__ void __launch_bounds__(512, 1) shgemm_tile_kernel(const __grid_constant__ TileGemmParams p) {
     using Cfg = TileCfg<TC, BN, A_KMAJOR, B_KMAJOR>;
-    constexpr int LS = Cfg::LOAD_STAGES;
-    constexpr int SS = Cfg::SPLIT_STAGES;
+    constexpr int SA = Cfg::SA;
+    constexpr int SB = Cfg::SB;
+    constexpr int SS = Cfg::SS;
     constexpr bool kTf32 = Cfg::kTf32;
+    constexpr int NSPLIT = Cfg::SPLIT_WARPS;
 
     extern __shared__ uint8_t smem_raw[];
     // 1024-byte alignment of the tile region (128B-swizzle atoms repeat every 1024 bytes).
     const uint32_t raw_s = ptx::smem_u32(smem_raw);
     uint8_t* smem = smem_raw + ((1024u - (raw_s & 1023u)) & 1023u);
-    uint8_t* load_base = smem;
-    uint8_t* split_base = load_base + LS * Cfg::LOAD_STAGE;
-    uint64_t* bars = reinterpret_cast<uint64_t*>(split_base + SS * Cfg::SPLIT_STAGE);
-    uint64_t* load_full = bars;
-    uint64_t* load_empty = load_full + LS;
-    uint64_t* split_full = load_empty + LS;
-    uint64_t* split_empty = split_full + SS;
-    uint64_t* hi_full = split_empty + SS;
-    uint64_t* hi_empty = hi_full + 2;
-    uint64_t* lo_full = hi_empty + 2;
-    uint64_t* lo_empty = lo_full + 2;
-    uint64_t* drain_bar = lo_empty + 2;
+    uint8_t* a_base = smem;
+    uint8_t* b_base = a_base + SA * Cfg::A_RAW;
+    uint8_t* s_base = b_base + SB * Cfg::B_RAW;
+    uint64_t* bars = reinterpret_cast<uint64_t*>(s_base + SS * Cfg::SPLIT_STAGE);
+    uint64_t* a_full = bars;
+    uint64_t* a_empty = a_full + SA;
+    uint64_t* b_full = a_empty + SA;
+    uint64_t* b_empty = b_full + SB;
+    uint64_t* s_full = b_empty + SB;
+    uint64_t* s_empty = s_full + SS;
+    uint64_t* d_full = s_empty + SS;
+    uint64_t* d_empty = d_full + 2;
+    uint64_t* drain_bar = d_empty + 2;
     uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(drain_bar + 1);
     volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
 
@@ -137,19 +297,21 @@ __global__ void __launch_bounds__(448, 1) shgemm_tile_kernel(const __grid_consta
     const int lane = threadIdx.x & 31;
 
     if (threadIdx.x == 0) {
-        for (int s = 0; s < LS; ++s) {
-            ptx::mbar_init(&load_full[s], 1);
-            ptx::mbar_init(&load_empty[s], kTf32 ? 4 : 1);
+        for (int s = 0; s < SA; ++s) {
+            ptx::mbar_init(&a_full[s], 1);
+            ptx::mbar_init(&a_empty[s], NSPLIT);
+        }
+        for (int s = 0; s < SB; ++s) {
+            ptx::mbar_init(&b_full[s], 1);
+            ptx::mbar_init(&b_empty[s], kTf32 ? NSPLIT : 1);
         }
         for (int s = 0; s < SS; ++s) {
-            ptx::mbar_init(&split_full[s], 4);
-            ptx::mbar_init(&split_empty[s], 1);
+            ptx::mbar_init(&s_full[s], NSPLIT);
+            ptx::mbar_init(&s_empty[s], 1);
         }
         for (int b = 0; b < 2; ++b) {
-            ptx::mbar_init(&hi_full[b], 1);
-            ptx::mbar_init(&hi_empty[b], 8);
-            ptx::mbar_init(&lo_full[b], 1);
-            ptx::mbar_init(&lo_empty[b], 8);
+            ptx::mbar_init(&d_full[b], 1);
+            ptx::mbar_init(&d_empty[b], 8);
         }
         ptx::mbar_init(drain_bar, 1);
         *abort_flag = 0;
@@ -175,61 +337,83 @@ __global__ void __launch_bounds__(448, 1) shgemm_tile_kernel(const __grid_consta
         atomicCAS(p.error_flag, 0, code);
     };
 
+    // Warpgroups 0-1 (producer, MMA, split) give registers to warpgroups 2-3 (epilogue):
+    // 2 x 128 x 80 + 2 x 128 x 176 = 65536.
+    if (warp < Cfg::EPI_WARP0) {
+    ptx::setmaxnreg_dec<80>();
     if (warp == 0) {
         // ------------------------------------------------------------ TMA producer
         if (lane == 0) {
-            int ls = 0;
-            uint32_t lph = 0;
-            uint32_t issued_mask = 0, issued_par = 0;  // per stage: a load is in flight / its phase parity
+            int as = 0, bs = 0;
+            uint32_t aph = 0, bph = 0;
+            uint32_t a_issued = 0, a_par = 0, b_issued = 0, b_par = 0;  // per stage: load in flight, its parity
             for (int u = blockIdx.x; u < p.num_units; u += gridDim.x) {
                 int tm, tn, slice, s0, s1;
                 decode_unit(p, u, tm, tn, slice);
                 step_range(p, slice, total_steps, s0, s1);
                 for (int st = s0; st < s1; ++st) {
-                    if (!ptx::mbar_wait(&load_empty[ls], lph ^ 1u, abort_flag, limit)) {
+                    const int kc = st * Cfg::BK;
+                    if (!ptx::mbar_wait(&a_empty[as], aph ^ 1u, abort_flag, limit)) {
                         fail(kErrProducerTimeout);
                         goto producer_done;
                     }
-                    uint8_t* a_dst = load_base + ls * Cfg::LOAD_STAGE;
-                    uint8_t* b_dst = a_dst + Cfg::A_RAW;
-                    ptx::mbar_arrive_expect_tx(&load_full[ls], Cfg::LOAD_STAGE);
-                    const int kc = st * Cfg::BK;
-                    if constexpr (A_KMAJOR) {
+                    {
+                        uint8_t* a_dst = a_base + as * Cfg::A_RAW;
+                        ptx::mbar_arrive_expect_tx(&a_full[as], Cfg::A_RAW);
+                        if constexpr (A_KMAJOR) {
 #pragma unroll
-                        for (int sub = 0; sub < Cfg::BK / 32; ++sub)
-                            ptx::tma_load_2d(a_dst + sub * (Cfg::BM * 128), &p.tmap_a, &load_full[ls], kc + 32 * sub,
-                                             tm * Cfg::BM);
-                    } else {
-                        ptx::tma_load_2d(a_dst, &p.tmap_a, &load_full[ls], tm * Cfg::BM, kc);
+                            for (int sub = 0; sub < Cfg::BK / 32; ++sub)
+                                ptx::tma_load_2d(a_dst + sub * (Cfg::BM * 128), &p.tmap_a, &a_full[as],
+                                                 kc + 32 * sub, tm * Cfg::BM);
+                        } else {
+                            ptx::tma_load_2d(a_dst, &p.tmap_a, &a_full[as], tm * Cfg::BM, kc);
+                        }
+                        a_issued |= 1u << as;
+                        a_par = (a_par & ~(1u << as)) | (aph << as);
                     }
-                    if constexpr (B_KMAJOR) {
-                        ptx::tma_load_2d(b_dst, &p.tmap_b, &load_full[ls], kc, tn * BN);
-                    } else if constexpr (!kTf32) {
+                    if (++as == SA) {
+                        as = 0;
+                        aph ^= 1u;
+                    }
+                    if (!ptx::mbar_wait(&b_empty[bs], bph ^ 1u, abort_flag, limit)) {
+                        fail(kErrProducerTimeout);
+                        goto producer_done;
+                    }
+                    {
+                        uint8_t* b_dst = b_base + bs * Cfg::B_RAW;
+                        ptx::mbar_arrive_expect_tx(&b_full[bs], Cfg::B_RAW);
+                        if constexpr (B_KMAJOR) {
+                            ptx::tma_load_2d(b_dst, &p.tmap_b, &b_full[bs], kc, tn * BN);
+                        } else if constexpr (!kTf32) {
 #pragma unroll
-                        for (int sub = 0; sub < BN / 64; ++sub)
-                            ptx::tma_load_2d(b_dst + sub * (Cfg::BK * 128), &p.tmap_b, &load_full[ls],
-                                             tn * BN + 64 * sub, kc);
-                    } else {
-                        ptx::tma_load_2d(b_dst, &p.tmap_b, &load_full[ls], tn * BN, kc);
+                            for (int sub = 0; sub < BN / 64; ++sub)
+                                ptx::tma_load_2d(b_dst + sub * (Cfg::BK * 128), &p.tmap_b, &b_full[bs],
+                                                 tn * BN + 64 * sub, kc);
+                        } else {
+                            ptx::tma_load_2d(b_dst, &p.tmap_b, &b_full[bs], tn * BN, kc);
+                        }
+                        b_issued |= 1u << bs;
+                        b_par = (b_par & ~(1u << bs)) | (bph << bs);
                     }
-                    issued_mask |= 1u << ls;
-                    issued_par = (issued_par & ~(1u << ls)) | (lph << ls);
-                    if (++ls == LS) {
-                        ls = 0;
-                        lph ^= 1u;
+                    if (++bs == SB) {
+                        bs = 0;
+                        bph ^= 1u;
                     }
                 }
             }
         producer_done:
             // Never leave with bulk copies in flight into this CTA's shared memory.
-            for (int s = 0; s < LS; ++s) {
-                if (issued_mask & (1u << s)) {
-                    const uint64_t t0 = ptx::globaltimer_ns();
-                    while (!ptx::mbar_try_wait(&load_full[s], (issued_par >> s) & 1u)) {
-                        if (ptx::globaltimer_ns() - t0 > limit) {
-                            fail(kErrDrainTimeout);
-                            break;
-                        }
+            for (int s = 0; s < SA + SB; ++s) {
+                const bool is_a = s < SA;
+                const int st = is_a ? s : s - SA;
+                if (!((is_a ? a_issued : b_issued) & (1u << st))) continue;
+                uint64_t* bar = is_a ? &a_full[st] : &b_full[st];
+                const uint32_t par = ((is_a ? a_par : b_par) >> st) & 1u;
+                const uint64_t t0 = ptx::globaltimer_ns();
+                while (!ptx::mbar_try_wait(bar, par)) {
+                    if (ptx::globaltimer_ns() - t0 > limit) {
+                        fail(kErrDrainTimeout);
+                        break;
                     }
                 }
             }
@@ -237,96 +421,91 @@ __global__ void __launch_bounds__(448, 1) shgemm_tile_kernel(const __grid_consta
     } else if (warp == 1) {
         // ------------------------------------------------------------ UMMA issuer
         if (lane == 0) {
-            constexpr uint32_t idesc = ptx::make_idesc(kTf32, !kTf32 && !B_KMAJOR, Cfg::BM, BN);
-            int ls = 0, ss = 0;
-            uint32_t lph = 0, sph = 0, gc = 0, t_iter = 0;
+            constexpr uint32_t idesc = ptx::make_idesc(kTf32, !A_KMAJOR && !kTf32, !kTf32 && !B_KMAJOR, Cfg::BM, BN);
+            int bs = 0, ss = 0;
+            uint32_t bph = 0, sph = 0, gc = 0;
             bool issued_any = false;
             for (int u = blockIdx.x; u < p.num_units; u += gridDim.x) {
                 int tm, tn, slice, s0, s1;
                 decode_unit(p, u, tm, tn, slice);
                 step_range(p, slice, total_steps, s0, s1);
                 const int nsteps = s1 - s0;
-                const uint32_t lb = t_iter & 1u;
-                if (!ptx::mbar_wait(&lo_empty[lb], ((t_iter >> 1) & 1u) ^ 1u, abort_flag, limit)) {
-                    fail(kErrMmaTimeout);
-                    goto mma_done;
-                }
-                ptx::tc_fence_after();
-                {
-                    const uint32_t d_lo = tmem_base + 256u + lb * 128u;
-                    for (int i = 0; i < nsteps; ++i) {
-                        const bool chunk_start = (i % p.chunk_steps) == 0;
-                        const uint32_t hb = gc & 1u;
-                        if (chunk_start) {
-                            if (!ptx::mbar_wait(&hi_empty[hb], ((gc >> 1) & 1u) ^ 1u, abort_flag, limit)) {
-                                fail(kErrMmaTimeout);
-                                goto mma_done;
-                            }
-                        }
-                        if constexpr (!kTf32) {
-                            if (!ptx::mbar_wait(&load_full[ls], lph, abort_flag, limit)) {
-                                fail(kErrMmaTimeout);
-                                goto mma_done;
-                            }
-                        }
-                        if (!ptx::mbar_wait(&split_full[ss], sph, abort_flag, limit)) {
+                for (int i = 0; i < nsteps; ++i) {
+                    const uint32_t db = gc & 1u;
+                    if (!ptx::mbar_wait(&d_empty[db], ((gc >> 1) & 1u) ^ 1u, abort_flag, limit)) {
+                        fail(kErrMmaTimeout);
+                        goto mma_done;
+                    }
+                    if constexpr (!kTf32) {
+                        if (!ptx::mbar_wait(&b_full[bs], bph, abort_flag, limit)) {
                             fail(kErrMmaTimeout);
                             goto mma_done;
                         }
-                        ptx::tc_fence_after();
-                        const uint32_t d_hi = tmem_base + hb * 128u;
-                        const uint32_t hi_s = ptx::smem_u32(split_base + ss * Cfg::SPLIT_STAGE);
+                    }
+                    if (!ptx::mbar_wait(&s_full[ss], sph, abort_flag, limit)) {
+                        fail(kErrMmaTimeout);
+                        goto mma_done;
+                    }
+                    ptx::tc_fence_after();
+                    {
+                        const uint32_t d = tmem_base + db * BN;
+                        const uint32_t hi_s = ptx::smem_u32(s_base + ss * Cfg::SPLIT_STAGE);
                         const uint32_t lo_s = hi_s + Cfg::HI_BYTES;
-                        uint32_t b_s;
-                        if constexpr (kTf32) {
-                            b_s = lo_s + Cfg::HI_BYTES;
-                        } else {
-                            b_s = ptx::smem_u32(load_base + ls * Cfg::LOAD_STAGE + Cfg::A_RAW);
-                        }
+                        const uint32_t b_s = kTf32 ? lo_s + Cfg::HI_BYTES : ptx::smem_u32(b_base + bs * Cfg::B_RAW);
+                        auto a_desc = [&](uint32_t base, int kk) -> uint64_t {
+                            if constexpr (A_KMAJOR || kTf32) {
+                                return ptx::make_smem_desc(base + kk * 32, 16, 1024, ptx::kLayoutSW128);
+                            } else {
+                                // MN-major: 64-wide m atoms MN_ATOM_BYTES apart, 8-row k groups 1024
+                                // bytes apart; one UMMA_K = 16 step is 16 rows of 128 bytes.
+                                return ptx::make_smem_desc(base + kk * 2048, Cfg::MN_ATOM_BYTES, 1024,
+                                                           ptx::kLayoutSW128);
+                            }
+                        };
+                        auto b_desc = [&](int kk) -> uint64_t {
+                            if constexpr (kTf32 || B_KMAJOR) {
+                                return ptx::make_smem_desc(b_s + kk * 32, 16, 1024, ptx::kLayoutSW128);
+                            } else {
+                                return ptx::make_smem_desc(b_s + kk * 2048, Cfg::BK * 128, 1024, ptx::kLayoutSW128);
+                            }
+                        };
+                        // lo products into a fresh accumulator ...
 #pragma unroll
                         for (int kk = 0; kk < Cfg::KSUB; ++kk) {
-                            const uint64_t a_hi = ptx::make_smem_desc(hi_s + kk * 32, 16, 1024, ptx::kLayoutSW128);
-                            const uint64_t a_lo = ptx::make_smem_desc(lo_s + kk * 32, 16, 1024, ptx::kLayoutSW128);
-                            uint64_t bd;
-                            if constexpr (kTf32 || B_KMAJOR) {
-                                bd = ptx::make_smem_desc(b_s + kk * 32, 16, 1024, ptx::kLayoutSW128);
-                            } else {
-                                // MN-major binary16 B: 64-wide MN atoms Cfg::BK*128 bytes apart, 8-row
-                                // k groups 1024 bytes apart; one UMMA_K=16 step = 16 rows of 128 bytes.
-                                bd = ptx::make_smem_desc(b_s + kk * 2048, Cfg::BK * 128, 1024, ptx::kLayoutSW128);
-                            }
-                            const uint32_t acc_hi = (!chunk_start || kk > 0) ? 1u : 0u;
-                            const uint32_t acc_lo = (i > 0 || kk > 0) ? 1u : 0u;
-                            if constexpr (kTf32) {
-                                ptx::umma_tf32_ss(d_hi, a_hi, bd, idesc, acc_hi);
-                                ptx::umma_tf32_ss(d_lo, a_lo, bd, idesc, acc_lo);
-                            } else {
-                                ptx::umma_f16_ss(d_hi, a_hi, bd, idesc, acc_hi);
-                                ptx::umma_f16_ss(d_lo, a_lo, bd, idesc, acc_lo);
-                            }
+                            if constexpr (kTf32)
+                                ptx::umma_tf32_ss(d, a_desc(lo_s, kk), b_desc(kk), idesc, kk > 0 ? 1u : 0u);
+                            else
+                                ptx::umma_f16_ss(d, a_desc(lo_s, kk), b_desc(kk), idesc, kk > 0 ? 1u : 0u);
                         }
-                        issued_any = true;
-                        ptx::umma_commit(&split_empty[ss]);
-                        if constexpr (!kTf32) {
-                            ptx::umma_commit(&load_empty[ls]);
-                            if (++ls == LS) {
-                                ls = 0;
-                                lph ^= 1u;
-                            }
-                        }
-                        if (++ss == SS) {
-                            ss = 0;
-                            sph ^= 1u;
-                        }
-                        const bool chunk_end = ((i + 1) % p.chunk_steps) == 0 || (i + 1) == nsteps;
-                        if (chunk_end) {
-                            ptx::umma_commit(&hi_full[hb]);
-                            ++gc;
+                        // ... scaled by 2^-11 under the first hi product, then the other hi products.
+                        if constexpr (kTf32)
+                            ptx::umma_tf32_ss_scale11(d, a_desc(hi_s, 0), b_desc(0), idesc);
+                        else
+                            ptx::umma_f16_ss_scale11(d, a_desc(hi_s, 0), b_desc(0), idesc);
+#pragma unroll
+                        for (int kk = 1; kk < Cfg::KSUB; ++kk) {
+                            if constexpr (kTf32)
+                                ptx::umma_tf32_ss(d, a_desc(hi_s, kk), b_desc(kk), idesc, 1u);
+                            else
+                                ptx::umma_f16_ss(d, a_desc(hi_s, kk), b_desc(kk), idesc, 1u);
                         }
                     }
+                    issued_any = true;
+                    ptx::umma_commit(&s_empty[ss]);
+                    if constexpr (!kTf32) {
+                        ptx::umma_commit(&b_empty[bs]);
+                        if (++bs == SB) {
+                            bs = 0;
+                            bph ^= 1u;
+                        }
+                    }
+                    if (++ss == SS) {
+                        ss = 0;
+                        sph ^= 1u;
+                    }
+                    ptx::umma_commit(&d_full[db]);
+                    ++gc;
                 }
-                ptx::umma_commit(&lo_full[lb]);
-                ++t_iter;
             }
         mma_done:
             // Wait for every MMA this thread issued before TMEM is released.
@@ -341,125 +520,46 @@ __global__ void __launch_bounds__(448, 1) shgemm_tile_kernel(const __grid_consta
                 }
             }
         }
-    } else if (warp < 6) {
-        // ------------------------------------------------------------ split warpgroup
-        const int t = (warp - 2) * 32 + lane;  // tile row (and B row in TF32 mode)
-        int ls = 0, ss = 0;
-        uint32_t lph = 0, sph = 0;
+    } else if (warp < Cfg::EPI_WARP0) {
+        // ------------------------------------------------------------ split warps
+        const int sidx = (warp - 2) * 32 + lane;
+        int as = 0, bs = 0, ss = 0;
+        uint32_t aph = 0, bph = 0, sph = 0;
         for (int u = blockIdx.x; u < p.num_units; u += gridDim.x) {
             int tm, tn, slice, s0, s1;
             decode_unit(p, u, tm, tn, slice);
             step_range(p, slice, total_steps, s0, s1);
             for (int st = s0; st < s1; ++st) {
-                if (!ptx::mbar_wait(&load_full[ls], lph, abort_flag, limit) ||
-                    !ptx::mbar_wait(&split_empty[ss], sph ^ 1u, abort_flag, limit)) {
+                if (!ptx::mbar_wait(&a_full[as], aph, abort_flag, limit) ||
+                    !ptx::mbar_wait(&s_empty[ss], sph ^ 1u, abort_flag, limit) ||
+                    (kTf32 && !ptx::mbar_wait(&b_full[bs], bph, abort_flag, limit))) {
                     fail(kErrSplitTimeout);
                     goto split_done;
                 }
                 {
-                    const uint8_t* a_raw = load_base + ls * Cfg::LOAD_STAGE;
-                    uint8_t* hi_t = split_base + ss * Cfg::SPLIT_STAGE;
+                    uint8_t* hi_t = s_base + ss * Cfg::SPLIT_STAGE;
                     uint8_t* lo_t = hi_t + Cfg::HI_BYTES;
-                    const int sw = t & 7;
-                    if constexpr (!kTf32) {
-#pragma unroll
-                        for (int c = 0; c < 8; ++c) {  // 16-byte output chunk = 8 k values
-                            float v[8];
-                            if constexpr (A_KMAJOR) {
-                                const uint8_t* row = a_raw + (c >> 2) * (Cfg::BM * 128) + t * 128;
-                                const int j0 = (c & 3) * 2;
-                                const float4 x0 = *reinterpret_cast<const float4*>(row + ((j0 ^ sw) << 4));
-                                const float4 x1 = *reinterpret_cast<const float4*>(row + (((j0 + 1) ^ sw) << 4));
-                                v[0] = x0.x; v[1] = x0.y; v[2] = x0.z; v[3] = x0.w;
-                                v[4] = x1.x; v[5] = x1.y; v[6] = x1.z; v[7] = x1.w;
-                            } else {
-                                const float* af = reinterpret_cast<const float*>(a_raw);
-#pragma unroll
-                                for (int e = 0; e < 8; ++e) v[e] = af[(c * 8 + e) * Cfg::BM + t];
-                            }
-                            uint32_t h[4], l[4];
-#pragma unroll
-                            for (int e = 0; e < 4; ++e) {
-                                const __half2 hh = __floats2half2_rn(v[2 * e], v[2 * e + 1]);
-                                const float2 hf = __half22float2(hh);
-                                const __half2 ll =
-                                    __floats2half2_rn(__fmul_rn(__fsub_rn(v[2 * e], hf.x), 2048.0f),
-                                                      __fmul_rn(__fsub_rn(v[2 * e + 1], hf.y), 2048.0f));
-                                h[e] = *reinterpret_cast<const uint32_t*>(&hh);
-                                l[e] = *reinterpret_cast<const uint32_t*>(&ll);
-                            }
-                            const int off = t * 128 + ((c ^ sw) << 4);
-                            *reinterpret_cast<uint4*>(hi_t + off) = make_uint4(h[0], h[1], h[2], h[3]);
-                            *reinterpret_cast<uint4*>(lo_t + off) = make_uint4(l[0], l[1], l[2], l[3]);
-                        }
-                    } else {
-#pragma unroll
-                        for (int c = 0; c < 8; ++c) {  // 16-byte output chunk = 4 k values
-                            float v[4];
-                            if constexpr (A_KMAJOR) {
-                                const float4 x = *reinterpret_cast<const float4*>(a_raw + t * 128 + ((c ^ sw) << 4));
-                                v[0] = x.x; v[1] = x.y; v[2] = x.z; v[3] = x.w;
-                            } else {
-                                const float* af = reinterpret_cast<const float*>(a_raw);
-#pragma unroll
-                                for (int e = 0; e < 4; ++e) v[e] = af[(c * 4 + e) * Cfg::BM + t];
-                            }
-                            float hv[4], lv[4];
-#pragma unroll
-                            for (int e = 0; e < 4; ++e) {
-                                hv[e] = ptx::to_tf32_rna(v[e]);
-                                lv[e] = ptx::to_tf32_rna(__fmul_rn(__fsub_rn(v[e], hv[e]), 2048.0f));
-                            }
-                            const int off = t * 128 + ((c ^ sw) << 4);
-                            *reinterpret_cast<float4*>(hi_t + off) = make_float4(hv[0], hv[1], hv[2], hv[3]);
-                            *reinterpret_cast<float4*>(lo_t + off) = make_float4(lv[0], lv[1], lv[2], lv[3]);
-                        }
-                        // Widen B (binary16 is exact in TF32): thread t writes K-major row n = t.
-                        if (t < BN) {
-                            const uint8_t* b_raw = a_raw + Cfg::A_RAW;
-                            uint8_t* bt = lo_t + Cfg::HI_BYTES;
-                            if constexpr (B_KMAJOR) {
-                                // raw tile [BN][32] binary16, 64-byte rows, 64B swizzle
-#pragma unroll
-                                for (int q = 0; q < 4; ++q) {
-                                    const uint4 hx = *reinterpret_cast<const uint4*>(
-                                        b_raw + t * 64 + ((q ^ ((t >> 1) & 3)) << 4));
-                                    const __half2* hp = reinterpret_cast<const __half2*>(&hx);
-                                    const float2 f0 = __half22float2(hp[0]);
-                                    const float2 f1 = __half22float2(hp[1]);
-                                    const float2 f2 = __half22float2(hp[2]);
-                                    const float2 f3 = __half22float2(hp[3]);
-                                    *reinterpret_cast<float4*>(bt + t * 128 + (((2 * q) ^ sw) << 4)) =
-                                        make_float4(f0.x, f0.y, f1.x, f1.y);
-                                    *reinterpret_cast<float4*>(bt + t * 128 + (((2 * q + 1) ^ sw) << 4)) =
-                                        make_float4(f2.x, f2.y, f3.x, f3.y);
-                                }
-                            } else {
-                                // raw tile [32 k][BN] binary16, no swizzle
-                                const __half* bh = reinterpret_cast<const __half*>(b_raw);
-#pragma unroll
-                                for (int c = 0; c < 8; ++c) {
-                                    float4 f;
-                                    f.x = __half2float(bh[(c * 4 + 0) * BN + t]);
-                                    f.y = __half2float(bh[(c * 4 + 1) * BN + t]);
-                                    f.z = __half2float(bh[(c * 4 + 2) * BN + t]);
-                                    f.w = __half2float(bh[(c * 4 + 3) * BN + t]);
-                                    *reinterpret_cast<float4*>(bt + t * 128 + ((c ^ sw) << 4)) = f;
-                                }
-                            }
-                        }
-                    }
+                    split_tile<Cfg, A_KMAJOR>(a_base + as * Cfg::A_RAW, hi_t, lo_t, sidx);
+                    if constexpr (kTf32)
+                        widen_b_tile<Cfg, B_KMAJOR>(b_base + bs * Cfg::B_RAW, lo_t + Cfg::HI_BYTES, sidx);
                 }
                 // Make the generic-proxy stores visible to the tensor core (async proxy).
                 ptx::fence_proxy_async_smem();
                 __syncwarp();
                 if (lane == 0) {
-                    ptx::mbar_arrive(&split_full[ss]);
-                    if constexpr (kTf32) ptx::mbar_arrive(&load_empty[ls]);
+                    ptx::mbar_arrive(&a_empty[as]);
+                    ptx::mbar_arrive(&s_full[ss]);
+                    if constexpr (kTf32) ptx::mbar_arrive(&b_empty[bs]);
                 }
-                if (++ls == LS) {
-                    ls = 0;
-                    lph ^= 1u;
+                if (++as == SA) {
+                    as = 0;
+                    aph ^= 1u;
+                }
+                if constexpr (kTf32) {
+                    if (++bs == SB) {
+                        bs = 0;
+                        bph ^= 1u;
+                    }
                 }
                 if (++ss == SS) {
                     ss = 0;
@@ -468,62 +568,48 @@ __global__ void __launch_bounds__(448, 1) shgemm_tile_kernel(const __grid_consta
             }
         }
     split_done:;
+    }
     } else {
         // ------------------------------------------------------------ epilogue
+        ptx::setmaxnreg_inc<176>();
         constexpr int HN = Cfg::HALF_N;
-        const int q = warp & 3;             // TMEM lane quadrant this warp may access
-        const int half = (warp - 6) >> 2;   // column half of the tile
+        const int q = warp & 3;                         // TMEM lane quadrant this warp may access
+        const int half = (warp - Cfg::EPI_WARP0) >> 2;  // column half of the tile
         const int row_in_tile = q * 32 + lane;
         const uint32_t lane_addr = static_cast<uint32_t>(q * 32) << 16;
-        uint32_t gc = 0, t_iter = 0;
+        uint32_t gc = 0;
         for (int u = blockIdx.x; u < p.num_units; u += gridDim.x) {
             int tm, tn, slice, s0, s1;
             decode_unit(p, u, tm, tn, slice);
             step_range(p, slice, total_steps, s0, s1);
             const int nsteps = s1 - s0;
-            const int nchunks = (nsteps + p.chunk_steps - 1) / p.chunk_steps;
             float acc[HN];
 #pragma unroll
             for (int j = 0; j < HN; ++j) acc[j] = 0.0f;
-            for (int c = 0; c < nchunks; ++c) {
-                const uint32_t hb = gc & 1u;
-                if (!ptx::mbar_wait(&hi_full[hb], (gc >> 1) & 1u, abort_flag, limit)) {
+            for (int i = 0; i < nsteps; ++i) {
+                const uint32_t db = gc & 1u;
+                if (!ptx::mbar_wait(&d_full[db], (gc >> 1) & 1u, abort_flag, limit)) {
                     fail(kErrEpilogueTimeout);
                     goto epi_done;
                 }
                 ptx::tc_fence_after();
 #pragma unroll
                 for (int j0 = 0; j0 < HN; j0 += 32) {
-                    uint32_t r[32];
-                    ptx::tmem_ld_32x32b_x32(tmem_base + lane_addr + hb * 128u + half * HN + j0, r);
+                    uint32_t r0[16], r1[16];
+                    const uint32_t ta = tmem_base + lane_addr + db * BN + half * HN + j0;
+                    ptx::tmem_ld_32x32b_x16(ta, r0);
+                    ptx::tmem_ld_32x32b_x16(ta + 16, r1);
                     ptx::tmem_ld_wait();
 #pragma unroll
-                    for (int e = 0; e < 32; ++e) acc[j0 + e] = __fadd_rn(acc[j0 + e], __uint_as_float(r[e]));
+                    for (int e = 0; e < 16; ++e) {
+                        acc[j0 + e] = __fadd_rn(acc[j0 + e], __uint_as_float(r0[e]));
+                        acc[j0 + 16 + e] = __fadd_rn(acc[j0 + 16 + e], __uint_as_float(r1[e]));
+                    }
                 }
                 ptx::tc_fence_before();
                 __syncwarp();
-                if (lane == 0) ptx::mbar_arrive(&hi_empty[hb]);
+                if (lane == 0) ptx::mbar_arrive(&d_empty[db]);
                 ++gc;
-            }
-            {
-                const uint32_t lb = t_iter & 1u;
-                if (!ptx::mbar_wait(&lo_full[lb], (t_iter >> 1) & 1u, abort_flag, limit)) {
-                    fail(kErrEpilogueTimeout);
-                    goto epi_done;
-                }
-                ptx::tc_fence_after();
-#pragma unroll
-                for (int j0 = 0; j0 < HN; j0 += 32) {
-                    uint32_t r[32];
-                    ptx::tmem_ld_32x32b_x32(tmem_base + lane_addr + 256u + lb * 128u + half * HN + j0, r);
-                    ptx::tmem_ld_wait();
-#pragma unroll
-                    for (int e = 0; e < 32; ++e)
-                        acc[j0 + e] = __fadd_rn(acc[j0 + e], __fmul_rn(__uint_as_float(r[e]), 0x1p-11f));
-                }
-                ptx::tc_fence_before();
-                __syncwarp();
-                if (lane == 0) ptx::mbar_arrive(&lo_empty[lb]);
             }
             {
                 const int row = tm * Cfg::BM + row_in_tile;
@@ -561,7 +647,6 @@ __global__ void __launch_bounds__(448, 1) shgemm_tile_kernel(const __grid_consta
                     }
                 }
             }
-            ++t_iter;
         }
     epi_done:;
     }

@@ -26,7 +26,6 @@ struct shgemm_b200_handle {
     cudaStream_t stream = nullptr;
     unsigned debug_mode = 0;
     int fixed_level = SHGEMM_LEVEL_AUTO;
-    long long chunk_k = 0;  // 0: one k-step (4 UMMA instructions) per hi drain
     long long split_k = 0;
     long long wait_limit_ms = 2000;
     long long group_m = 8;
@@ -88,14 +87,14 @@ struct KernelEntry {
     int smem;
 };
 
-// [tc][bn128][a_kmajor][b_kmajor]
-KernelEntry kernel_table(int tc, int bn128, int ak, int bk) {
+// Instantiated tile kernels: binary16 compute with tile N 64 / 128 / 256, TF32 with 64 / 128.
+KernelEntry kernel_table(int tc, int bn, int ak, int bk) {
 #define SHG_ENTRY(TC, BN, AK, BK) \
-    if (tc == TC && bn128 == (BN == 128) && ak == AK && bk == BK) return {tile_kernel_ptr<TC, BN, AK, BK>(), tile_smem<TC, BN, AK, BK>()};
-    SHG_ENTRY(kFP16, 128, 0, 0) SHG_ENTRY(kFP16, 128, 0, 1) SHG_ENTRY(kFP16, 128, 1, 0) SHG_ENTRY(kFP16, 128, 1, 1)
-    SHG_ENTRY(kFP16, 64, 0, 0) SHG_ENTRY(kFP16, 64, 0, 1) SHG_ENTRY(kFP16, 64, 1, 0) SHG_ENTRY(kFP16, 64, 1, 1)
-    SHG_ENTRY(kTF32, 128, 0, 0) SHG_ENTRY(kTF32, 128, 0, 1) SHG_ENTRY(kTF32, 128, 1, 0) SHG_ENTRY(kTF32, 128, 1, 1)
-    SHG_ENTRY(kTF32, 64, 0, 0) SHG_ENTRY(kTF32, 64, 0, 1) SHG_ENTRY(kTF32, 64, 1, 0) SHG_ENTRY(kTF32, 64, 1, 1)
+    if (tc == TC && bn == BN && ak == AK && bk == BK) return {tile_kernel_ptr<TC, BN, AK, BK>(), tile_smem<TC, BN, AK, BK>()};
+#define SHG_ENTRY4(TC, BN) SHG_ENTRY(TC, BN, 0, 0) SHG_ENTRY(TC, BN, 0, 1) SHG_ENTRY(TC, BN, 1, 0) SHG_ENTRY(TC, BN, 1, 1)
+    SHG_ENTRY4(kFP16, 64) SHG_ENTRY4(kFP16, 128) SHG_ENTRY4(kFP16, 256)
+    SHG_ENTRY4(kTF32, 64) SHG_ENTRY4(kTF32, 128)
+#undef SHG_ENTRY4
 #undef SHG_ENTRY
     return {nullptr, 0};
 }
@@ -277,13 +276,12 @@ int launch_status() {
 }
 
 struct Plan {
-    int level;  // 0: BN = 64, 1: BN = 128
+    int level;  // 0: the smaller tile N, 1: the larger one
     int bn;
     int tiles_m, tiles_n;
     int total_steps;
     int slices;
     int steps_per_slice;
-    int chunk_steps;
 };
 
 double wave_efficiency(long long units, int sms) {
@@ -291,20 +289,24 @@ double wave_efficiency(long long units, int sms) {
     return static_cast<double>(units) / static_cast<double>(waves * sms);
 }
 
+// Tile N per level: binary16 compute {128, 256}, TF32 {64, 128}; n <= 64 always
+// takes N = 64, which wastes no MMA columns.
+int level_bn(int tc, int level) { return tc == kFP16 ? (level ? 256 : 128) : (level ? 128 : 64); }
+
 Plan make_plan(const shgemm_b200_handle* h, size_t m, size_t n, size_t k, int tc, size_t ws_bytes) {
     Plan p{};
     const int bk = (tc == kFP16) ? 64 : 32;
     p.total_steps = static_cast<int>((k + bk - 1) / bk);
-    const long long chunk_k = h->chunk_k <= 0 ? bk : std::max<long long>(bk, h->chunk_k);
-    p.chunk_steps = static_cast<int>(std::max<long long>(1, chunk_k / bk));
     p.tiles_m = static_cast<int>((m + 127) / 128);
     // Level choice mirrors the reference (src/shgemm.cu:643-656): the large tile when it
     // still fills the machine, else the small one; a fixed level overrides.
-    const long long tiles128 = static_cast<long long>(p.tiles_m) * ((n + 127) / 128);
-    int level = (n <= 64 || tiles128 < h->num_sms) ? 0 : 1;
+    const int big = level_bn(tc, 1);
+    const long long tiles_big = static_cast<long long>(p.tiles_m) * ((n + big - 1) / big);
+    int level = (tiles_big >= h->num_sms && n > static_cast<size_t>(level_bn(tc, 0))) ? 1 : 0;
     if (h->fixed_level == SHGEMM_LEVEL_P0 || h->fixed_level == SHGEMM_LEVEL_P1) level = h->fixed_level;
     p.level = level;
-    p.bn = level ? 128 : 64;
+    p.bn = level_bn(tc, level);
+    if (n <= 64 && h->fixed_level == SHGEMM_LEVEL_AUTO) p.bn = 64;
     p.tiles_n = static_cast<int>((n + p.bn - 1) / p.bn);
     const long long tiles = static_cast<long long>(p.tiles_m) * p.tiles_n;
     // Split-K: deterministic slices when the tiles alone leave SMs idle and k is long.
@@ -314,7 +316,7 @@ Plan make_plan(const shgemm_b200_handle* h, size_t m, size_t n, size_t k, int tc
     } else if (h->split_k == 0 && tiles < h->num_sms && k >= 4096) {
         double best = wave_efficiency(tiles, h->num_sms);
         for (int s = 2; s <= 64; ++s) {
-            if (p.total_steps / s < 2 * p.chunk_steps) break;
+            if (p.total_steps / s < 8) break;
             const double e = wave_efficiency(tiles * s, h->num_sms);
             if (e > best + 0.02) {
                 best = e;
@@ -387,10 +389,11 @@ int shgemm_b200_create(shgemm_b200_handle_t* out, int device) {
         return SHGEMM_STATUS_ALLOC_FAILED;
     }
     for (int tc = 0; tc < 2; ++tc)
-        for (int b = 0; b < 2; ++b)
+        for (int bn : {64, 128, 256})
             for (int ak = 0; ak < 2; ++ak)
                 for (int bk = 0; bk < 2; ++bk) {
-                    KernelEntry e = kernel_table(tc, b, ak, bk);
+                    KernelEntry e = kernel_table(tc, bn, ak, bk);
+                    if (!e.fn) continue;
                     if (cudaFuncSetAttribute(e.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, e.smem) !=
                         cudaSuccess) {
                         cudaGetLastError();
@@ -434,10 +437,6 @@ int shgemm_b200_set_debug_mode(shgemm_b200_handle_t h, unsigned on) {
 int shgemm_b200_set_config(shgemm_b200_handle_t h, int key, long long v) {
     if (!h) return SHGEMM_STATUS_INVALID_VALUE;
     switch (key) {
-        case SHGEMM_CFG_CHUNK_K:
-            if (v < 0 || v % 32) return SHGEMM_STATUS_INVALID_VALUE;
-            h->chunk_k = v;
-            return SHGEMM_STATUS_OK;
         case SHGEMM_CFG_SPLIT_K:
             if (v < 0 || v > 1024) return SHGEMM_STATUS_INVALID_VALUE;
             h->split_k = v;
@@ -458,7 +457,6 @@ int shgemm_b200_set_config(shgemm_b200_handle_t h, int key, long long v) {
 int shgemm_b200_get_config(shgemm_b200_handle_t h, int key, long long* v) {
     if (!h || !v) return SHGEMM_STATUS_INVALID_VALUE;
     switch (key) {
-        case SHGEMM_CFG_CHUNK_K: *v = h->chunk_k; return SHGEMM_STATUS_OK;
         case SHGEMM_CFG_SPLIT_K: *v = h->split_k; return SHGEMM_STATUS_OK;
         case SHGEMM_CFG_WAIT_LIMIT_MS: *v = h->wait_limit_ms; return SHGEMM_STATUS_OK;
         case SHGEMM_CFG_GROUP_M: *v = h->group_m; return SHGEMM_STATUS_OK;
@@ -567,18 +565,18 @@ static int run_tiled(shgemm_b200_handle_t h, int op_a, int op_b, size_t m, size_
     P.steps_per_slice = pl.steps_per_slice;
     P.num_units = pl.tiles_m * pl.tiles_n * pl.slices;
     P.group_m = static_cast<int>(h->group_m);
-    P.chunk_steps = pl.chunk_steps;
 
-    const KernelEntry e = kernel_table(tc, pl.bn == 128, a_kmajor, b_kmajor);
+    const KernelEntry e = kernel_table(tc, pl.bn, a_kmajor, b_kmajor);
+    if (!e.fn) return SHGEMM_STATUS_NOT_SUPPORTED;
     const int grid = std::min(P.num_units, h->num_sms);
     if (h->debug_mode) {
         std::printf("[shape=(%zu,%zu,%zu),op_a=%s,op_b=%s,compute_type=%s] kernel_level = %d, tile = 128x%d, "
                     "k_slices = %d, chunk_k = %d, grid = %d\n",
                     m, n, k, op_a == kOpN ? "N" : "T", op_b == kOpN ? "N" : "T", tc == kTF32 ? "TF32" : "FP16",
-                    pl.level, pl.bn, pl.slices, pl.chunk_steps * bk, grid);
+                    pl.level, pl.bn, pl.slices, bk, grid);
     }
     void* args[] = {&P};
-    cudaError_t err = cudaLaunchKernel(e.fn, dim3(grid), dim3(448), args, e.smem, h->stream);
+    cudaError_t err = cudaLaunchKernel(e.fn, dim3(grid), dim3(512), args, e.smem, h->stream);
     h->launches++;
     if (err != cudaSuccess) {
         cudaGetLastError();
