@@ -25,14 +25,17 @@
 // Warp roles (512 threads, one CTA per SM, registers rebalanced per warpgroup):
 //   warp 0       TMA producer: raw FP32 A tile and binary16 B tile per k-step
 //   warp 1       TMEM allocator + single-thread UMMA issuer
-//   warps 2-7    split: turn the raw FP32 tile into 128B-swizzled hi/lo UMMA
-//                tiles (K-major when A is K-contiguous, MN-major for binary16
-//                when it is M-contiguous) and, for TF32, widen B to TF32
+//   warps 2-7    split: turn the raw FP32 tile, in place, into 128B-swizzled
+//                hi/lo UMMA tiles (K-major when A is K-contiguous, MN-major for
+//                binary16 when it is M-contiguous) and, for TF32, widen B in place
 //   warps 8-15   epilogue: TMEM lane quadrant (warp % 4) x column half
-// Rings: A (TMA -> split), B (TMA -> MMA; TMA -> split for TF32), split tiles
-// (split -> MMA), D (MMA <-> epilogue). Every wait is bounded; on timeout the
-// kernel records an error code, drains its own in-flight copies and MMAs, frees
-// TMEM and exits.
+// Rings: A stages (TMA -> split in place -> MMA), B stages (TMA -> MMA; for TF32
+// TMA -> widen in place -> MMA), D (MMA <-> epilogue). A stage is 32 KB: the raw
+// FP32 tile and the hi + lo tiles have the same size (binary16) or fit in it
+// (TF32), so the split reads its whole share into registers, waits until every
+// split thread has done so, then overwrites the stage. Every wait is bounded; on
+// timeout the kernel records an error code, drains its own in-flight copies and
+// MMAs, frees TMEM and exits.
 #pragma once
 #include "ptx.cuh"
 
@@ -79,26 +82,29 @@ struct TileCfg {
     static constexpr int A_RAW = BM * BK * 4;
     static constexpr int B_RAW = BN * BK * 2;
     static constexpr int HI_BYTES = BM * 128;  // BM rows of 128 bytes (both modes)
-    static constexpr int BT_BYTES = kTf32 ? BN * 128 : 0;
+    static constexpr int A_STAGE = 2 * HI_BYTES;  // raw FP32 tile, then hi + lo tiles
+    static constexpr int B_STAGE = BN * 128;      // binary16 tile; TF32: widened tile
     // MN-major hi/lo tiles (binary16, M-contiguous A): 64-wide m atoms of BK k rows.
     static constexpr int MN_ATOM_BYTES = BK * 128;
-    static constexpr int SPLIT_STAGE = 2 * HI_BYTES + BT_BYTES;
     static constexpr int SMEM_BUDGET = 224 * 1024;
-    static constexpr int SS = kTf32 ? 3 : (BN == 256 ? 2 : 3);
-    static constexpr int SA = kTf32 ? 3 : 2;
-    static constexpr int SB_FIT = (SMEM_BUDGET - SS * SPLIT_STAGE - SA * A_RAW) / B_RAW;
+    static constexpr int SA = 4;
+    static constexpr int SB_FIT = (SMEM_BUDGET - SA * A_STAGE) / B_STAGE;
     static constexpr int SB = SB_FIT > 6 ? 6 : SB_FIT;
-    static_assert(SB >= 2, "shared memory budget");
+    static_assert(SB >= 3, "shared memory budget");
     static constexpr int NUM_THREADS = 512;
     static constexpr int SPLIT_WARPS = 6;
     static constexpr int SPLIT_THREADS = 32 * SPLIT_WARPS;
     static constexpr int EPI_WARP0 = 8;
     static constexpr int TMEM_COLS = 2 * BN < 32 ? 32 : 2 * BN;  // D ping-pong
     static constexpr int HALF_N = BN / 2;                        // columns per epilogue warp
+    // Per-thread registers after setmaxnreg: warpgroups 0-1 (producer, MMA, split) and
+    // 2-3 (epilogue, which holds HALF_N running sums); 256 x (SPLIT_REGS + EPI_REGS) = 65536.
+    static constexpr int SPLIT_REGS = BN == 256 ? 80 : 112;
+    static constexpr int EPI_REGS = 256 - SPLIT_REGS;
     static constexpr int BAR_BYTES = 1024;
-    static constexpr int SMEM_BYTES = SA * A_RAW + SB * B_RAW + SS * SPLIT_STAGE + BAR_BYTES + 1024;
+    static constexpr int SMEM_BYTES = SA * A_STAGE + SB * B_STAGE + BAR_BYTES + 1024;
     static_assert(BN == 64 || BN == 128 || (BN == 256 && !kTf32), "tile N");
-    static_assert(A_RAW % 1024 == 0 && B_RAW % 1024 == 0 && SPLIT_STAGE % 1024 == 0, "1024B-aligned stages");
+    static_assert(A_STAGE % 1024 == 0 && B_STAGE % 1024 == 0 && A_RAW <= A_STAGE, "1024B-aligned stages");
     static_assert(SMEM_BYTES <= 232448, "dynamic shared memory limit");
 };
 
@@ -124,13 +130,16 @@ __device__ __forceinline__ void step_range(const TileGemmParams& p, int slice, i
 // Split helpers. hi = T(v), lo = T(2^11 (v - hi)), T = binary16 round-to-nearest-
 // even or TF32 round-to-nearest-away: the reference's split (src/wmmae_shgemm.hpp:30-31).
 __device__ __forceinline__ void split8_f16(const float (&v)[8], uint4& hi, uint4& lo) {
+    const uint64_t scale = ptx::f2_pack(2048.0f, 2048.0f);
     uint32_t h[4], l[4];
 #pragma unroll
     for (int e = 0; e < 4; ++e) {
         const __half2 hh = __floats2half2_rn(v[2 * e], v[2 * e + 1]);
         const float2 hf = __half22float2(hh);
-        const __half2 ll = __floats2half2_rn(__fmul_rn(__fsub_rn(v[2 * e], hf.x), 2048.0f),
-                                             __fmul_rn(__fsub_rn(v[2 * e + 1], hf.y), 2048.0f));
+        // (v - hi) is exact and the 2^11 scaling is exact: lo = T(2^11 (v - hi))
+        const uint64_t d = ptx::f2_mul(ptx::f2_sub(ptx::f2_pack(v[2 * e], v[2 * e + 1]), ptx::f2_pack(hf.x, hf.y)),
+                                       scale);
+        const __half2 ll = __floats2half2_rn(ptx::f2_lo(d), ptx::f2_hi(d));
         h[e] = *reinterpret_cast<const uint32_t*>(&hh);
         l[e] = *reinterpret_cast<const uint32_t*>(&ll);
     }
@@ -143,124 +152,193 @@ __device__ __forceinline__ void split4_tf32(const float4 x, float4& hi, float4& 
     hi.y = ptx::to_tf32_rna(x.y);
     hi.z = ptx::to_tf32_rna(x.z);
     hi.w = ptx::to_tf32_rna(x.w);
-    lo.x = ptx::to_tf32_rna(__fmul_rn(__fsub_rn(x.x, hi.x), 2048.0f));
-    lo.y = ptx::to_tf32_rna(__fmul_rn(__fsub_rn(x.y, hi.y), 2048.0f));
-    lo.z = ptx::to_tf32_rna(__fmul_rn(__fsub_rn(x.z, hi.z), 2048.0f));
-    lo.w = ptx::to_tf32_rna(__fmul_rn(__fsub_rn(x.w, hi.w), 2048.0f));
+    const uint64_t scale = ptx::f2_pack(2048.0f, 2048.0f);
+    const uint64_t d0 = ptx::f2_mul(ptx::f2_sub(ptx::f2_pack(x.x, x.y), ptx::f2_pack(hi.x, hi.y)), scale);
+    const uint64_t d1 = ptx::f2_mul(ptx::f2_sub(ptx::f2_pack(x.z, x.w), ptx::f2_pack(hi.z, hi.w)), scale);
+    lo.x = ptx::to_tf32_rna(ptx::f2_lo(d0));
+    lo.y = ptx::to_tf32_rna(ptx::f2_hi(d0));
+    lo.z = ptx::to_tf32_rna(ptx::f2_lo(d1));
+    lo.w = ptx::to_tf32_rna(ptx::f2_hi(d1));
 }
 
-// Split of one raw FP32 A tile (one k-step) by the split warps (thread sidx).
-template <class Cfg, bool A_KMAJOR>
-__device__ __forceinline__ void split_tile(const uint8_t* a_raw, uint8_t* hi_t, uint8_t* lo_t, int sidx) {
+// One k-step of the split warps (thread sidx of SPLIT_THREADS), in place:
+// phase 1 reads this thread's share of the raw tiles into registers;
+// `all_read()` returns once every split thread has done so (false on timeout);
+// phase 2 converts and overwrites the stages with the UMMA tiles:
+//   A stage: hi at [0, HI_BYTES), lo at [HI_BYTES, 2 HI_BYTES)
+//   B stage (TF32 only): the widened [BN][32] TF32 tile.
+template <class Cfg, bool A_KMAJOR, bool B_KMAJOR, class AllRead>
+__device__ __forceinline__ bool split_step(uint8_t* a_st, uint8_t* b_st, int sidx, AllRead&& all_read) {
+    constexpr int NT = Cfg::SPLIT_THREADS;
+    uint8_t* hi_t = a_st;
+    uint8_t* lo_t = a_st + Cfg::HI_BYTES;
     if constexpr (!Cfg::kTf32) {
-        if constexpr (A_KMAJOR) {
-            // raw: two [128 rows][32 floats] 128B-swizzled sub-tiles (k 0-31, 32-63);
-            // out: [128 rows][64 halves] K-major, 128B swizzle. Unit: (row, 16-byte chunk c).
-            for (int u = sidx; u < 1024; u += Cfg::SPLIT_THREADS) {
-                const int row = u & 127, c = u >> 7, sw = row & 7;
-                const uint8_t* rp = a_raw + (c >> 2) * (Cfg::BM * 128) + row * 128;
-                const int j0 = (c & 3) * 2;
-                const float4 x0 = *reinterpret_cast<const float4*>(rp + ((j0 ^ sw) << 4));
-                const float4 x1 = *reinterpret_cast<const float4*>(rp + (((j0 + 1) ^ sw) << 4));
-                const float v[8] = {x0.x, x0.y, x0.z, x0.w, x1.x, x1.y, x1.z, x1.w};
-                uint4 h, l;
-                split8_f16(v, h, l);
-                const int off = row * 128 + ((c ^ sw) << 4);
-                *reinterpret_cast<uint4*>(hi_t + off) = h;
-                *reinterpret_cast<uint4*>(lo_t + off) = l;
-            }
-        } else {
-            // raw: [64 k][128 m] floats (512-byte rows); out: MN-major, two atoms of
-            // [64 k rows][64 m halves], 128B swizzle. Unit: (k, group g of 8 consecutive m).
-            for (int u = sidx; u < 1024; u += Cfg::SPLIT_THREADS) {
-                const int g = u & 15, k = u >> 4;
-                const int first = (g >> 2) & 1;  // read order that keeps 8-thread phases conflict-free
-                const uint8_t* rp = a_raw + k * 512 + g * 32;
-                const float4 xa = *reinterpret_cast<const float4*>(rp + 16 * first);
-                const float4 xb = *reinterpret_cast<const float4*>(rp + 16 * (1 - first));
-                const float4 x0 = first ? xb : xa;
-                const float4 x1 = first ? xa : xb;
-                const float v[8] = {x0.x, x0.y, x0.z, x0.w, x1.x, x1.y, x1.z, x1.w};
-                uint4 h, l;
-                split8_f16(v, h, l);
-                const int off = (g >> 3) * Cfg::MN_ATOM_BYTES + k * 128 + (((g & 7) ^ (k & 7)) << 4);
-                *reinterpret_cast<uint4*>(hi_t + off) = h;
-                *reinterpret_cast<uint4*>(lo_t + off) = l;
-            }
-        }
-    } else {
-        if constexpr (A_KMAJOR) {
-            // raw: [128 rows][32 floats] 128B-swizzled; out: the same layout in TF32.
-            for (int u = sidx; u < 1024; u += Cfg::SPLIT_THREADS) {
-                const int row = u & 127, c = u >> 7;
-                const int off = row * 128 + ((c ^ (row & 7)) << 4);
-                float4 h, l;
-                split4_tf32(*reinterpret_cast<const float4*>(a_raw + off), h, l);
-                *reinterpret_cast<float4*>(hi_t + off) = h;
-                *reinterpret_cast<float4*>(lo_t + off) = l;
-            }
-        } else {
-            // raw: [32 k][128 m] floats; out: K-major [128 rows][32] TF32 (128B swizzle),
-            // transposed in registers 4 m x 4 k at a time. Unit: (m group g of 4, k group kq of 4).
-            for (int u = sidx; u < 256; u += Cfg::SPLIT_THREADS) {
-                const int g = u & 31, kq = u >> 5;
-                float4 h[4], l[4];  // h[j]: k = 4kq + j, m = 4g .. 4g+3
+        constexpr int U = (1024 + NT - 1) / NT;  // units of 8 values per thread
+        float4 x[U][2];
 #pragma unroll
-                for (int j = 0; j < 4; ++j)
-                    split4_tf32(*reinterpret_cast<const float4*>(a_raw + (kq * 4 + j) * 512 + g * 16), h[j], l[j]);
-                // rotate the row order so 8-thread store phases hit distinct 16-byte bank groups
-#pragma unroll
-                for (int r = 0; r < 4; ++r) {
-                    const int rr = (r + (g >> 1)) & 3;
-                    const int row = 4 * g + rr;
-                    const float4 hv = rr == 0   ? make_float4(h[0].x, h[1].x, h[2].x, h[3].x)
-                                      : rr == 1 ? make_float4(h[0].y, h[1].y, h[2].y, h[3].y)
-                                      : rr == 2 ? make_float4(h[0].z, h[1].z, h[2].z, h[3].z)
-                                                : make_float4(h[0].w, h[1].w, h[2].w, h[3].w);
-                    const float4 lv = rr == 0   ? make_float4(l[0].x, l[1].x, l[2].x, l[3].x)
-                                      : rr == 1 ? make_float4(l[0].y, l[1].y, l[2].y, l[3].y)
-                                      : rr == 2 ? make_float4(l[0].z, l[1].z, l[2].z, l[3].z)
-                                                : make_float4(l[0].w, l[1].w, l[2].w, l[3].w);
-                    const int off = row * 128 + ((kq ^ (row & 7)) << 4);
-                    *reinterpret_cast<float4*>(hi_t + off) = hv;
-                    *reinterpret_cast<float4*>(lo_t + off) = lv;
+        for (int j = 0; j < U; ++j) {
+            const int u = sidx + j * NT;
+            if (u < 1024) {
+                if constexpr (A_KMAJOR) {
+                    // raw: two [128 rows][32 floats] 128B-swizzled sub-tiles (k 0-31, 32-63).
+                    // Unit: (row, 16-byte output chunk c).
+                    const int row = u & 127, c = u >> 7, sw = row & 7, j0 = (c & 3) * 2;
+                    const uint8_t* rp = a_st + (c >> 2) * (Cfg::BM * 128) + row * 128;
+                    x[j][0] = *reinterpret_cast<const float4*>(rp + ((j0 ^ sw) << 4));
+                    x[j][1] = *reinterpret_cast<const float4*>(rp + (((j0 + 1) ^ sw) << 4));
+                } else {
+                    // raw: [64 k][128 m] floats (512-byte rows). Unit: (k, group g of 8
+                    // consecutive m); the read order keeps 8-thread phases conflict-free.
+                    const int g = u & 15, k = u >> 4, first = (g >> 2) & 1;
+                    const uint8_t* rp = a_st + k * 512 + g * 32;
+                    const float4 xa = *reinterpret_cast<const float4*>(rp + 16 * first);
+                    const float4 xb = *reinterpret_cast<const float4*>(rp + 16 * (1 - first));
+                    x[j][0] = first ? xb : xa;
+                    x[j][1] = first ? xa : xb;
                 }
             }
         }
-    }
-}
-
-// TF32 mode: widen the binary16 B tile (exact in TF32) into a K-major [BN][32]
-// TF32 tile with a 128B swizzle. Unit: (row n, 16-byte chunk).
-template <class Cfg, bool B_KMAJOR>
-__device__ __forceinline__ void widen_b_tile(const uint8_t* b_raw, uint8_t* bt, int sidx) {
-    constexpr int BN = Cfg::BN;
-    if constexpr (B_KMAJOR) {
-        // raw: [BN][32] binary16, 64-byte rows, 64B swizzle; one raw 16-byte chunk
-        // (8 values) makes two output chunks.
-        for (int u = sidx; u < BN * 4; u += Cfg::SPLIT_THREADS) {
-            const int n = u % BN, rc = u / BN, sw = n & 7;
-            const uint4 hx = *reinterpret_cast<const uint4*>(b_raw + n * 64 + ((rc ^ ((n >> 1) & 3)) << 4));
-            const __half2* hp = reinterpret_cast<const __half2*>(&hx);
-            const float2 f0 = __half22float2(hp[0]);
-            const float2 f1 = __half22float2(hp[1]);
-            const float2 f2 = __half22float2(hp[2]);
-            const float2 f3 = __half22float2(hp[3]);
-            *reinterpret_cast<float4*>(bt + n * 128 + (((2 * rc) ^ sw) << 4)) = make_float4(f0.x, f0.y, f1.x, f1.y);
-            *reinterpret_cast<float4*>(bt + n * 128 + (((2 * rc + 1) ^ sw) << 4)) = make_float4(f2.x, f2.y, f3.x, f3.y);
+        if (!all_read()) return false;
+#pragma unroll
+        for (int j = 0; j < U; ++j) {
+            const int u = sidx + j * NT;
+            if (u < 1024) {
+                const float v[8] = {x[j][0].x, x[j][0].y, x[j][0].z, x[j][0].w,
+                                    x[j][1].x, x[j][1].y, x[j][1].z, x[j][1].w};
+                uint4 h, l;
+                split8_f16(v, h, l);
+                int off;
+                if constexpr (A_KMAJOR) {
+                    // out: [128 rows][64 halves] K-major, 128B swizzle
+                    const int row = u & 127, c = u >> 7;
+                    off = row * 128 + ((c ^ (row & 7)) << 4);
+                } else {
+                    // out: MN-major, two atoms of [64 k rows][64 m halves], 128B swizzle
+                    const int g = u & 15, k = u >> 4;
+                    off = (g >> 3) * Cfg::MN_ATOM_BYTES + k * 128 + (((g & 7) ^ (k & 7)) << 4);
+                }
+                *reinterpret_cast<uint4*>(hi_t + off) = h;
+                *reinterpret_cast<uint4*>(lo_t + off) = l;
+            }
         }
+        return true;
     } else {
-        // raw: [32 k][BN] binary16, no swizzle
-        const __half* bh = reinterpret_cast<const __half*>(b_raw);
-        for (int u = sidx; u < BN * 8; u += Cfg::SPLIT_THREADS) {
-            const int n = u % BN, c = u / BN;
-            float4 f;
-            f.x = __half2float(bh[(c * 4 + 0) * BN + n]);
-            f.y = __half2float(bh[(c * 4 + 1) * BN + n]);
-            f.z = __half2float(bh[(c * 4 + 2) * BN + n]);
-            f.w = __half2float(bh[(c * 4 + 3) * BN + n]);
-            *reinterpret_cast<float4*>(bt + n * 128 + ((c ^ (n & 7)) << 4)) = f;
+        constexpr int BN = Cfg::BN;
+        // ---- phase 1: A
+        constexpr int UA = A_KMAJOR ? (1024 + NT - 1) / NT : (256 + NT - 1) / NT;
+        float4 xa[UA][A_KMAJOR ? 1 : 4];
+#pragma unroll
+        for (int j = 0; j < UA; ++j) {
+            const int u = sidx + j * NT;
+            if constexpr (A_KMAJOR) {
+                // raw: [128 rows][32 floats] 128B-swizzled. Unit: (row, 16-byte chunk c).
+                if (u < 1024) {
+                    const int row = u & 127, c = u >> 7;
+                    xa[j][0] = *reinterpret_cast<const float4*>(a_st + row * 128 + ((c ^ (row & 7)) << 4));
+                }
+            } else {
+                // raw: [32 k][128 m] floats. Unit: (m group g of 4, k group kq of 4).
+                if (u < 256) {
+                    const int g = u & 31, kq = u >> 5;
+#pragma unroll
+                    for (int r = 0; r < 4; ++r)
+                        xa[j][r] = *reinterpret_cast<const float4*>(a_st + (kq * 4 + r) * 512 + g * 16);
+                }
+            }
         }
+        // ---- phase 1: B (binary16, exact in TF32)
+        constexpr int UB = B_KMAJOR ? (BN * 4 + NT - 1) / NT : (BN * 8 + NT - 1) / NT;
+        uint4 xb_k[B_KMAJOR ? UB : 1];
+        uint2 xb_m[B_KMAJOR ? 1 : UB];
+#pragma unroll
+        for (int j = 0; j < UB; ++j) {
+            const int u = sidx + j * NT;
+            if constexpr (B_KMAJOR) {
+                // raw: [BN][32] binary16, 64-byte rows, 64B swizzle. Unit: (row n, raw chunk rc).
+                if (u < BN * 4) {
+                    const int n = u % BN, rc = u / BN;
+                    xb_k[j] = *reinterpret_cast<const uint4*>(b_st + n * 64 + ((rc ^ ((n >> 1) & 3)) << 4));
+                }
+            } else {
+                // raw: [32 k][BN] binary16. Unit: (column n, output chunk c = k 4c .. 4c+3).
+                if (u < BN * 8) {
+                    const int n = u % BN, c = u / BN;
+                    const uint16_t* bh = reinterpret_cast<const uint16_t*>(b_st);
+                    xb_m[j].x = uint32_t(bh[(c * 4 + 0) * BN + n]) | (uint32_t(bh[(c * 4 + 1) * BN + n]) << 16);
+                    xb_m[j].y = uint32_t(bh[(c * 4 + 2) * BN + n]) | (uint32_t(bh[(c * 4 + 3) * BN + n]) << 16);
+                }
+            }
+        }
+        if (!all_read()) return false;
+        // ---- phase 2: A -> hi/lo [128 rows][32] TF32, K-major, 128B swizzle
+#pragma unroll
+        for (int j = 0; j < UA; ++j) {
+            const int u = sidx + j * NT;
+            if constexpr (A_KMAJOR) {
+                if (u < 1024) {
+                    const int row = u & 127, c = u >> 7;
+                    const int off = row * 128 + ((c ^ (row & 7)) << 4);
+                    float4 h, l;
+                    split4_tf32(xa[j][0], h, l);
+                    *reinterpret_cast<float4*>(hi_t + off) = h;
+                    *reinterpret_cast<float4*>(lo_t + off) = l;
+                }
+            } else {
+                if (u < 256) {
+                    const int g = u & 31, kq = u >> 5;
+                    float4 h[4], l[4];  // h[r]: k = 4kq + r, m = 4g .. 4g+3
+#pragma unroll
+                    for (int r = 0; r < 4; ++r) split4_tf32(xa[j][r], h[r], l[r]);
+                    // transpose 4 x 4; rotate the row order so 8-thread store phases
+                    // hit distinct 16-byte bank groups
+#pragma unroll
+                    for (int r = 0; r < 4; ++r) {
+                        const int rr = (r + (g >> 1)) & 3;
+                        const int row = 4 * g + rr;
+                        const float4 hv = rr == 0   ? make_float4(h[0].x, h[1].x, h[2].x, h[3].x)
+                                          : rr == 1 ? make_float4(h[0].y, h[1].y, h[2].y, h[3].y)
+                                          : rr == 2 ? make_float4(h[0].z, h[1].z, h[2].z, h[3].z)
+                                                    : make_float4(h[0].w, h[1].w, h[2].w, h[3].w);
+                        const float4 lv = rr == 0   ? make_float4(l[0].x, l[1].x, l[2].x, l[3].x)
+                                          : rr == 1 ? make_float4(l[0].y, l[1].y, l[2].y, l[3].y)
+                                          : rr == 2 ? make_float4(l[0].z, l[1].z, l[2].z, l[3].z)
+                                                    : make_float4(l[0].w, l[1].w, l[2].w, l[3].w);
+                        const int off = row * 128 + ((kq ^ (row & 7)) << 4);
+                        *reinterpret_cast<float4*>(hi_t + off) = hv;
+                        *reinterpret_cast<float4*>(lo_t + off) = lv;
+                    }
+                }
+            }
+        }
+        // ---- phase 2: B -> [BN][32] TF32, K-major, 128B swizzle
+#pragma unroll
+        for (int j = 0; j < UB; ++j) {
+            const int u = sidx + j * NT;
+            if constexpr (B_KMAJOR) {
+                if (u < BN * 4) {
+                    const int n = u % BN, rc = u / BN, sw = n & 7;
+                    const __half2* hp = reinterpret_cast<const __half2*>(&xb_k[j]);
+                    const float2 f0 = __half22float2(hp[0]);
+                    const float2 f1 = __half22float2(hp[1]);
+                    const float2 f2 = __half22float2(hp[2]);
+                    const float2 f3 = __half22float2(hp[3]);
+                    *reinterpret_cast<float4*>(b_st + n * 128 + (((2 * rc) ^ sw) << 4)) =
+                        make_float4(f0.x, f0.y, f1.x, f1.y);
+                    *reinterpret_cast<float4*>(b_st + n * 128 + (((2 * rc + 1) ^ sw) << 4)) =
+                        make_float4(f2.x, f2.y, f3.x, f3.y);
+                }
+            } else {
+                if (u < BN * 8) {
+                    const int n = u % BN, c = u / BN;
+                    const __half2* hp = reinterpret_cast<const __half2*>(&xb_m[j]);
+                    const float2 f0 = __half22float2(hp[0]);
+                    const float2 f1 = __half22float2(hp[1]);
+                    *reinterpret_cast<float4*>(b_st + n * 128 + ((c ^ (n & 7)) << 4)) =
+                        make_float4(f0.x, f0.y, f1.x, f1.y);
+                }
+            }
+        }
+        return true;
     }
 }
 
@@ -269,7 +347,6 @@ __global__ void __launch_bounds__(512, 1) shgemm_tile_kernel(const __grid_consta
     using Cfg = TileCfg<TC, BN, A_KMAJOR, B_KMAJOR>;
     constexpr int SA = Cfg::SA;
     constexpr int SB = Cfg::SB;
-    constexpr int SS = Cfg::SS;
     constexpr bool kTf32 = Cfg::kTf32;
     constexpr int NSPLIT = Cfg::SPLIT_WARPS;
 
@@ -278,16 +355,15 @@ __global__ void __launch_bounds__(512, 1) shgemm_tile_kernel(const __grid_consta
     const uint32_t raw_s = ptx::smem_u32(smem_raw);
     uint8_t* smem = smem_raw + ((1024u - (raw_s & 1023u)) & 1023u);
     uint8_t* a_base = smem;
-    uint8_t* b_base = a_base + SA * Cfg::A_RAW;
-    uint8_t* s_base = b_base + SB * Cfg::B_RAW;
-    uint64_t* bars = reinterpret_cast<uint64_t*>(s_base + SS * Cfg::SPLIT_STAGE);
-    uint64_t* a_full = bars;
-    uint64_t* a_empty = a_full + SA;
+    uint8_t* b_base = a_base + SA * Cfg::A_STAGE;
+    uint64_t* bars = reinterpret_cast<uint64_t*>(b_base + SB * Cfg::B_STAGE);
+    uint64_t* a_full = bars;           // TMA landed the raw A tile
+    uint64_t* a_read = a_full + SA;    // every split warp holds its share in registers
+    uint64_t* a_split = a_read + SA;   // hi/lo tiles written (and, for TF32, B widened)
+    uint64_t* a_empty = a_split + SA;  // MMAs reading the stage completed
     uint64_t* b_full = a_empty + SA;
     uint64_t* b_empty = b_full + SB;
-    uint64_t* s_full = b_empty + SB;
-    uint64_t* s_empty = s_full + SS;
-    uint64_t* d_full = s_empty + SS;
+    uint64_t* d_full = b_empty + SB;
     uint64_t* d_empty = d_full + 2;
     uint64_t* drain_bar = d_empty + 2;
     uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(drain_bar + 1);
@@ -299,15 +375,13 @@ __global__ void __launch_bounds__(512, 1) shgemm_tile_kernel(const __grid_consta
     if (threadIdx.x == 0) {
         for (int s = 0; s < SA; ++s) {
             ptx::mbar_init(&a_full[s], 1);
-            ptx::mbar_init(&a_empty[s], NSPLIT);
+            ptx::mbar_init(&a_read[s], NSPLIT);
+            ptx::mbar_init(&a_split[s], NSPLIT);
+            ptx::mbar_init(&a_empty[s], 1);
         }
         for (int s = 0; s < SB; ++s) {
             ptx::mbar_init(&b_full[s], 1);
-            ptx::mbar_init(&b_empty[s], kTf32 ? NSPLIT : 1);
-        }
-        for (int s = 0; s < SS; ++s) {
-            ptx::mbar_init(&s_full[s], NSPLIT);
-            ptx::mbar_init(&s_empty[s], 1);
+            ptx::mbar_init(&b_empty[s], 1);
         }
         for (int b = 0; b < 2; ++b) {
             ptx::mbar_init(&d_full[b], 1);
@@ -337,10 +411,9 @@ __global__ void __launch_bounds__(512, 1) shgemm_tile_kernel(const __grid_consta
         atomicCAS(p.error_flag, 0, code);
     };
 
-    // Warpgroups 0-1 (producer, MMA, split) give registers to warpgroups 2-3 (epilogue):
-    // 2 x 128 x 80 + 2 x 128 x 176 = 65536.
+    // Warpgroups 0-1 (producer, MMA, split) give registers to warpgroups 2-3 (epilogue).
     if (warp < Cfg::EPI_WARP0) {
-    ptx::setmaxnreg_dec<80>();
+    ptx::setmaxnreg_dec<Cfg::SPLIT_REGS>();
     if (warp == 0) {
         // ------------------------------------------------------------ TMA producer
         if (lane == 0) {
@@ -358,7 +431,7 @@ __global__ void __launch_bounds__(512, 1) shgemm_tile_kernel(const __grid_consta
                         goto producer_done;
                     }
                     {
-                        uint8_t* a_dst = a_base + as * Cfg::A_RAW;
+                        uint8_t* a_dst = a_base + as * Cfg::A_STAGE;
                         ptx::mbar_arrive_expect_tx(&a_full[as], Cfg::A_RAW);
                         if constexpr (A_KMAJOR) {
 #pragma unroll
@@ -380,7 +453,7 @@ __global__ void __launch_bounds__(512, 1) shgemm_tile_kernel(const __grid_consta
                         goto producer_done;
                     }
                     {
-                        uint8_t* b_dst = b_base + bs * Cfg::B_RAW;
+                        uint8_t* b_dst = b_base + bs * Cfg::B_STAGE;
                         ptx::mbar_arrive_expect_tx(&b_full[bs], Cfg::B_RAW);
                         if constexpr (B_KMAJOR) {
                             ptx::tma_load_2d(b_dst, &p.tmap_b, &b_full[bs], kc, tn * BN);
@@ -422,8 +495,8 @@ __global__ void __launch_bounds__(512, 1) shgemm_tile_kernel(const __grid_consta
         // ------------------------------------------------------------ UMMA issuer
         if (lane == 0) {
             constexpr uint32_t idesc = ptx::make_idesc(kTf32, !A_KMAJOR && !kTf32, !kTf32 && !B_KMAJOR, Cfg::BM, BN);
-            int bs = 0, ss = 0;
-            uint32_t bph = 0, sph = 0, gc = 0;
+            int as = 0, bs = 0;
+            uint32_t aph = 0, bph = 0, gc = 0;
             bool issued_any = false;
             for (int u = blockIdx.x; u < p.num_units; u += gridDim.x) {
                 int tm, tn, slice, s0, s1;
@@ -442,16 +515,16 @@ __global__ void __launch_bounds__(512, 1) shgemm_tile_kernel(const __grid_consta
                             goto mma_done;
                         }
                     }
-                    if (!ptx::mbar_wait(&s_full[ss], sph, abort_flag, limit)) {
+                    if (!ptx::mbar_wait(&a_split[as], aph, abort_flag, limit)) {
                         fail(kErrMmaTimeout);
                         goto mma_done;
                     }
                     ptx::tc_fence_after();
                     {
                         const uint32_t d = tmem_base + db * BN;
-                        const uint32_t hi_s = ptx::smem_u32(s_base + ss * Cfg::SPLIT_STAGE);
+                        const uint32_t hi_s = ptx::smem_u32(a_base + as * Cfg::A_STAGE);
                         const uint32_t lo_s = hi_s + Cfg::HI_BYTES;
-                        const uint32_t b_s = kTf32 ? lo_s + Cfg::HI_BYTES : ptx::smem_u32(b_base + bs * Cfg::B_RAW);
+                        const uint32_t b_s = ptx::smem_u32(b_base + bs * Cfg::B_STAGE);
                         auto a_desc = [&](uint32_t base, int kk) -> uint64_t {
                             if constexpr (A_KMAJOR || kTf32) {
                                 return ptx::make_smem_desc(base + kk * 32, 16, 1024, ptx::kLayoutSW128);
@@ -491,17 +564,15 @@ __global__ void __launch_bounds__(512, 1) shgemm_tile_kernel(const __grid_consta
                         }
                     }
                     issued_any = true;
-                    ptx::umma_commit(&s_empty[ss]);
-                    if constexpr (!kTf32) {
-                        ptx::umma_commit(&b_empty[bs]);
-                        if (++bs == SB) {
-                            bs = 0;
-                            bph ^= 1u;
-                        }
+                    ptx::umma_commit(&a_empty[as]);
+                    ptx::umma_commit(&b_empty[bs]);
+                    if (++as == SA) {
+                        as = 0;
+                        aph ^= 1u;
                     }
-                    if (++ss == SS) {
-                        ss = 0;
-                        sph ^= 1u;
+                    if (++bs == SB) {
+                        bs = 0;
+                        bph ^= 1u;
                     }
                     ptx::umma_commit(&d_full[db]);
                     ++gc;
@@ -523,34 +594,34 @@ __global__ void __launch_bounds__(512, 1) shgemm_tile_kernel(const __grid_consta
     } else if (warp < Cfg::EPI_WARP0) {
         // ------------------------------------------------------------ split warps
         const int sidx = (warp - 2) * 32 + lane;
-        int as = 0, bs = 0, ss = 0;
-        uint32_t aph = 0, bph = 0, sph = 0;
+        int as = 0, bs = 0;
+        uint32_t aph = 0, bph = 0;
         for (int u = blockIdx.x; u < p.num_units; u += gridDim.x) {
             int tm, tn, slice, s0, s1;
             decode_unit(p, u, tm, tn, slice);
             step_range(p, slice, total_steps, s0, s1);
             for (int st = s0; st < s1; ++st) {
                 if (!ptx::mbar_wait(&a_full[as], aph, abort_flag, limit) ||
-                    !ptx::mbar_wait(&s_empty[ss], sph ^ 1u, abort_flag, limit) ||
                     (kTf32 && !ptx::mbar_wait(&b_full[bs], bph, abort_flag, limit))) {
                     fail(kErrSplitTimeout);
                     goto split_done;
                 }
                 {
-                    uint8_t* hi_t = s_base + ss * Cfg::SPLIT_STAGE;
-                    uint8_t* lo_t = hi_t + Cfg::HI_BYTES;
-                    split_tile<Cfg, A_KMAJOR>(a_base + as * Cfg::A_RAW, hi_t, lo_t, sidx);
-                    if constexpr (kTf32)
-                        widen_b_tile<Cfg, B_KMAJOR>(b_base + bs * Cfg::B_RAW, lo_t + Cfg::HI_BYTES, sidx);
+                    auto all_read = [&]() -> bool {
+                        __syncwarp();
+                        if (lane == 0) ptx::mbar_arrive(&a_read[as]);
+                        return ptx::mbar_wait(&a_read[as], aph, abort_flag, limit);
+                    };
+                    if (!split_step<Cfg, A_KMAJOR, B_KMAJOR>(a_base + as * Cfg::A_STAGE, b_base + bs * Cfg::B_STAGE,
+                                                              sidx, all_read)) {
+                        fail(kErrSplitTimeout);
+                        goto split_done;
+                    }
                 }
                 // Make the generic-proxy stores visible to the tensor core (async proxy).
                 ptx::fence_proxy_async_smem();
                 __syncwarp();
-                if (lane == 0) {
-                    ptx::mbar_arrive(&a_empty[as]);
-                    ptx::mbar_arrive(&s_full[ss]);
-                    if constexpr (kTf32) ptx::mbar_arrive(&b_empty[bs]);
-                }
+                if (lane == 0) ptx::mbar_arrive(&a_split[as]);
                 if (++as == SA) {
                     as = 0;
                     aph ^= 1u;
@@ -561,17 +632,13 @@ __global__ void __launch_bounds__(512, 1) shgemm_tile_kernel(const __grid_consta
                         bph ^= 1u;
                     }
                 }
-                if (++ss == SS) {
-                    ss = 0;
-                    sph ^= 1u;
-                }
             }
         }
     split_done:;
     }
     } else {
         // ------------------------------------------------------------ epilogue
-        ptx::setmaxnreg_inc<176>();
+        ptx::setmaxnreg_inc<Cfg::EPI_REGS>();
         constexpr int HN = Cfg::HALF_N;
         const int q = warp & 3;                         // TMEM lane quadrant this warp may access
         const int half = (warp - Cfg::EPI_WARP0) >> 2;  // column half of the tile
@@ -583,9 +650,9 @@ __global__ void __launch_bounds__(512, 1) shgemm_tile_kernel(const __grid_consta
             decode_unit(p, u, tm, tn, slice);
             step_range(p, slice, total_steps, s0, s1);
             const int nsteps = s1 - s0;
-            float acc[HN];
+            uint64_t acc2[HN / 2];  // running sums, packed in pairs of columns
 #pragma unroll
-            for (int j = 0; j < HN; ++j) acc[j] = 0.0f;
+            for (int j = 0; j < HN / 2; ++j) acc2[j] = 0ull;
             for (int i = 0; i < nsteps; ++i) {
                 const uint32_t db = gc & 1u;
                 if (!ptx::mbar_wait(&d_full[db], (gc >> 1) & 1u, abort_flag, limit)) {
@@ -601,9 +668,11 @@ __global__ void __launch_bounds__(512, 1) shgemm_tile_kernel(const __grid_consta
                     ptx::tmem_ld_32x32b_x16(ta + 16, r1);
                     ptx::tmem_ld_wait();
 #pragma unroll
-                    for (int e = 0; e < 16; ++e) {
-                        acc[j0 + e] = __fadd_rn(acc[j0 + e], __uint_as_float(r0[e]));
-                        acc[j0 + 16 + e] = __fadd_rn(acc[j0 + 16 + e], __uint_as_float(r1[e]));
+                    for (int e = 0; e < 8; ++e) {
+                        acc2[j0 / 2 + e] = ptx::f2_add(acc2[j0 / 2 + e],
+                                                       (static_cast<uint64_t>(r0[2 * e + 1]) << 32) | r0[2 * e]);
+                        acc2[j0 / 2 + 8 + e] = ptx::f2_add(acc2[j0 / 2 + 8 + e],
+                                                           (static_cast<uint64_t>(r1[2 * e + 1]) << 32) | r1[2 * e]);
                     }
                 }
                 ptx::tc_fence_before();
@@ -612,6 +681,7 @@ __global__ void __launch_bounds__(512, 1) shgemm_tile_kernel(const __grid_consta
                 ++gc;
             }
             {
+                auto acc = [&](int j) -> float { return (j & 1) ? ptx::f2_hi(acc2[j >> 1]) : ptx::f2_lo(acc2[j >> 1]); };
                 const int row = tm * Cfg::BM + row_in_tile;
                 const int col0 = tn * BN + half * HN;
                 if (row < p.m) {
@@ -620,7 +690,7 @@ __global__ void __launch_bounds__(512, 1) shgemm_tile_kernel(const __grid_consta
 #pragma unroll
                         for (int j = 0; j < HN; ++j) {
                             const int col = col0 + j;
-                            if (col < p.n) w[static_cast<size_t>(col) * p.m] = acc[j];
+                            if (col < p.n) w[static_cast<size_t>(col) * p.m] = acc(j);
                         }
                     } else if (p.op_c == kOpN) {
                         float* cp = p.c + row;
@@ -629,8 +699,8 @@ __global__ void __launch_bounds__(512, 1) shgemm_tile_kernel(const __grid_consta
                             const int col = col0 + j;
                             if (col < p.n) {
                                 float* dst = cp + static_cast<size_t>(col) * p.ldc;
-                                *dst = (p.beta == 0.0f) ? __fmul_rn(acc[j], p.alpha)
-                                                        : __fmaf_rn(acc[j], p.alpha, __fmul_rn(p.beta, *dst));
+                                *dst = (p.beta == 0.0f) ? __fmul_rn(acc(j), p.alpha)
+                                                        : __fmaf_rn(acc(j), p.alpha, __fmul_rn(p.beta, *dst));
                             }
                         }
                     } else {
@@ -640,8 +710,8 @@ __global__ void __launch_bounds__(512, 1) shgemm_tile_kernel(const __grid_consta
                             const int col = col0 + j;
                             if (col < p.n) {
                                 float* dst = cp + col;
-                                *dst = (p.beta == 0.0f) ? __fmul_rn(acc[j], p.alpha)
-                                                        : __fmaf_rn(acc[j], p.alpha, __fmul_rn(p.beta, *dst));
+                                *dst = (p.beta == 0.0f) ? __fmul_rn(acc(j), p.alpha)
+                                                        : __fmaf_rn(acc(j), p.alpha, __fmul_rn(p.beta, *dst));
                             }
                         }
                     }
