@@ -43,7 +43,7 @@ WORKLOADS = {
     # Y = Omega^T A as hsgemm(op_t, op_n) -> internal shgemm(op_t, op_n, 4096, 256, 2^20, op_c = t)
     "sketch": dict(m=4096, n=256, k=1 << 20, op_a=1, op_b=0, tc=0, alpha=1.0, beta=0.0, dist="sketch",
                    desc="left sketch Y = Omega^T A, A 2^20 x 4096 FP32 (low rank + noise), Omega 2^20 x 256 "
-                        "binary16 N(0,1/256), split-K, fp16 compute", op_c=1),
+                        "binary16 N(0,1/256), split-K, fp16 compute", op_c=1, bound="hbm"),
 }
 
 
@@ -374,11 +374,19 @@ def main():
 
     # ---- roofline of the tile kernel (its launches are the timed steps)
     peaks, peak_kind = load_peaks()
-    peak = peaks.get("bf16_tflops", 1590.0)
-    achieved = flops_issued / (ms_step * 1e-3) / 1e12
-    roofline = {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
-                "traffic": None, "peak_kind": f"{peak_kind} bf16 dense burst",
-                "work_per_launch": f"4mnk = {flops_issued:.4e} issued tensor flops (two MMAs per k: hi and lo)"}
+    bytes_min = 4.0 * m * k + 2.0 * k * n + 4.0 * m * n * (2 if wl["beta"] != 0 else 1)
+    if wl.get("bound", "tensor") == "hbm":
+        peak = peaks.get("hbm_gbs", 6650.0)
+        achieved = bytes_min / (ms_step * 1e-3) / 1e9
+        roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                    "traffic": None, "peak_kind": f"{peak_kind} HBM copy bandwidth",
+                    "work_per_launch": f"A + B + C = {bytes_min:.4e} bytes (each operand read once)"}
+    else:
+        peak = peaks.get("bf16_tflops", 1590.0)
+        achieved = flops_issued / (ms_step * 1e-3) / 1e12
+        roofline = {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                    "frac": achieved / peak, "traffic": None, "peak_kind": f"{peak_kind} bf16 dense burst",
+                    "work_per_launch": f"4mnk = {flops_issued:.4e} issued tensor flops (two MMAs per k: hi and lo)"}
     traffic_file = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(traffic_file):
         with open(traffic_file) as f:

@@ -293,48 +293,53 @@ double wave_efficiency(long long units, int sms) {
 // takes N = 64, which wastes no MMA columns.
 int level_bn(int tc, int level) { return tc == kFP16 ? (level ? 256 : 128) : (level ? 128 : 64); }
 
-Plan make_plan(const shgemm_b200_handle* h, size_t m, size_t n, size_t k, int tc, size_t ws_bytes) {
+// Tiling and split-K plan. `split_k`: 0 automatic, 1 never, s > 1 forced. Split-K
+// partials need slices * m * n floats of scratch, bounded by `ws_bytes`.
+Plan make_plan_for(int num_sms, int fixed_level, long long split_k, size_t m, size_t n, size_t k, int tc,
+                   size_t ws_bytes) {
     Plan p{};
     const int bk = (tc == kFP16) ? 64 : 32;
     p.total_steps = static_cast<int>((k + bk - 1) / bk);
     p.tiles_m = static_cast<int>((m + 127) / 128);
+    const size_t per_slice = m * n * sizeof(float);
+    const int fit = per_slice ? static_cast<int>(std::min<size_t>(ws_bytes / per_slice, 1024)) : 0;
+    const bool can_split = split_k != 1 && fit >= 2 && k >= 4096;
     // Level choice mirrors the reference (src/shgemm.cu:643-656): the large tile when it
-    // still fills the machine, else the small one; a fixed level overrides.
-    const int big = level_bn(tc, 1);
+    // fills the machine (or when split-K will), else the small one; a fixed level overrides.
+    const int small = level_bn(tc, 0), big = level_bn(tc, 1);
     const long long tiles_big = static_cast<long long>(p.tiles_m) * ((n + big - 1) / big);
-    int level = (tiles_big >= h->num_sms && n > static_cast<size_t>(level_bn(tc, 0))) ? 1 : 0;
-    if (h->fixed_level == SHGEMM_LEVEL_P0 || h->fixed_level == SHGEMM_LEVEL_P1) level = h->fixed_level;
+    int level = 0;
+    if (n > static_cast<size_t>(small) && (tiles_big >= num_sms || can_split)) level = 1;
+    if (fixed_level == SHGEMM_LEVEL_P0 || fixed_level == SHGEMM_LEVEL_P1) level = fixed_level;
     p.level = level;
     p.bn = level_bn(tc, level);
-    if (n <= 64 && h->fixed_level == SHGEMM_LEVEL_AUTO) p.bn = 64;
+    if (n <= 64 && fixed_level == SHGEMM_LEVEL_AUTO) p.bn = 64;
     p.tiles_n = static_cast<int>((n + p.bn - 1) / p.bn);
     const long long tiles = static_cast<long long>(p.tiles_m) * p.tiles_n;
-    // Split-K: deterministic slices when the tiles alone leave SMs idle and k is long.
+    // Split-K: deterministic slices when the tiles alone leave SMs idle and k is long;
+    // the slice count maximises the fraction of busy SMs over the waves.
     int slices = 1;
-    if (h->split_k > 1) {
-        slices = static_cast<int>(h->split_k);
-    } else if (h->split_k == 0 && tiles < h->num_sms && k >= 4096) {
-        double best = wave_efficiency(tiles, h->num_sms);
-        for (int s = 2; s <= 64; ++s) {
+    if (split_k > 1) {
+        slices = static_cast<int>(std::min<long long>(split_k, fit >= 2 ? fit : 1));
+    } else if (can_split && tiles < num_sms) {
+        double best = wave_efficiency(tiles, num_sms);
+        for (int s = 2; s <= std::min(fit, 64); ++s) {
             if (p.total_steps / s < 8) break;
-            const double e = wave_efficiency(tiles * s, h->num_sms);
+            const double e = wave_efficiency(tiles * s, num_sms);
             if (e > best + 0.02) {
                 best = e;
                 slices = s;
             }
         }
     }
-    // The workspace bounds the slice count (no allocation inside a call).
-    const size_t per_slice = m * n * sizeof(float);
-    if (slices > 1 && per_slice > 0) {
-        const size_t fit = ws_bytes / per_slice;
-        if (fit < 2) slices = 1;
-        else if (static_cast<size_t>(slices) > fit) slices = static_cast<int>(fit);
-    }
     slices = std::max(1, std::min(slices, p.total_steps));
     p.steps_per_slice = (p.total_steps + slices - 1) / slices;
     p.slices = (p.total_steps + p.steps_per_slice - 1) / p.steps_per_slice;
     return p;
+}
+
+Plan make_plan(const shgemm_b200_handle* h, size_t m, size_t n, size_t k, int tc, size_t ws_bytes) {
+    return make_plan_for(h->num_sms, h->fixed_level, h->split_k, m, n, k, tc, ws_bytes);
 }
 
 }  // namespace

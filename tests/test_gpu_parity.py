@@ -234,3 +234,31 @@ def test_launch_count_increments(h):
     before = h.launch_count()
     _parity(h, oracle.FP16, 0, 0, 0, 64, 64, 64)
     assert h.launch_count() > before
+
+
+@pytest.mark.parametrize("tc", [oracle.FP16, oracle.TF32])
+@pytest.mark.parametrize("op_a,op_b", [(1, 0), (0, 0)])
+def test_split_k_deterministic_and_matches(h, tc, op_a, op_b):
+    """Long-k, few-tile shapes take the deterministic split-K path (the reference's
+    k-slicing, src/shgemm.cu:532-609, which reduces with atomics): results are
+    bit-identical across runs and within the parity bar; beta != 0 is supported."""
+    import shgemm_b200 as sg
+
+    m, n, k = 256, 192, 16384
+    rng = np.random.default_rng(77)
+    inp = K.make_inputs(rng, m, n, k, op_a, op_b, 1)
+    c1, _ = K.run_gpu(h, tc, op_a, op_b, m, n, k, 1.0, inp, 0.5, 1)
+    c2, _ = K.run_gpu(h, tc, op_a, op_b, m, n, k, 1.0, inp, 0.5, 1)
+    assert np.array_equal(c1.view(np.uint32), c2.view(np.uint32))
+    orc = K.run_oracle(tc, op_a, op_b, m, n, k, 1.0, inp, 0.5, 1, chunk=0)
+    ref = K.fp64(op_a, op_b, m, n, k, 1.0, inp, 0.5, 1)
+    sgc = K.sgemm(op_a, op_b, m, n, k, 1.0, inp, 0.5, 1)
+    K.assert_parity(K.parity_report(c1, orc, ref, sgc, m, n, inp["ldc"], 1))
+    # forcing one slice (no split-K) gives a result within the same bar
+    h.set_config(sg.CFG_SPLIT_K, 1)
+    try:
+        c3, _ = K.run_gpu(h, tc, op_a, op_b, m, n, k, 1.0, inp, 0.5, 1)
+    finally:
+        h.set_config(sg.CFG_SPLIT_K, 0)
+    K.assert_parity(K.parity_report(c3, orc, ref, sgc, m, n, inp["ldc"], 1))
+    assert not np.array_equal(c1.view(np.uint32), c3.view(np.uint32))  # the split path really ran
