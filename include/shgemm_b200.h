@@ -36,7 +36,8 @@ enum {
     SHGEMM_STATUS_ALLOC_FAILED = 3,
     SHGEMM_STATUS_LAUNCH_FAILED = 4,
     SHGEMM_STATUS_TIMEOUT = 5,
-    SHGEMM_STATUS_CUDA_ERROR = 6
+    SHGEMM_STATUS_CUDA_ERROR = 6,
+    SHGEMM_STATUS_SCRATCH_TOO_SMALL = 7
 };
 
 /* Tunables for shgemm_b200_set_config (no reference counterpart; the
@@ -125,6 +126,38 @@ int shgemm_b200_eval_dgemm_hs(shgemm_b200_handle_t handle, int op_a, int op_b, s
  * out[3] = number of entries where C and ref disagree on being finite. */
 int shgemm_b200_eval_error(shgemm_b200_handle_t handle, size_t m, size_t n, const float* c, size_t ldc, int op_c,
                            const double* c64, double alpha, double beta, const float* c0, double* out);
+
+/* ------------------------------------------------------------------------
+ * Allocation-free entry point. No counterpart in the reference.
+ *
+ * For callers that cannot call cudaMalloc -- code running inside an allocator
+ * callback, a memory manager that owns all device memory, or a process that
+ * reserved its device memory up front -- and so cannot create a handle (whose
+ * workspace is allocated). It computes what shgemm_b200_shgemm computes (same
+ * kernels, same deterministic split-K), on the current device and the given
+ * stream, and allocates nothing: the split-K partials live in a 16 MiB
+ * file-scope device array of the library (held on every GPU that loads the
+ * library until the process exits) and the error word in another.
+ *  - Limit: m * n <= shgemm_b200_noalloc_scratch_bytes() / 8 (two slices of
+ *    FP32 partials); larger problems return SHGEMM_STATUS_SCRATCH_TOO_SMALL.
+ *    Operands must be 16-byte aligned with 16-byte aligned leading dimensions
+ *    (no staging), else SHGEMM_STATUS_NOT_SUPPORTED.
+ *  - The first call on a device sets that device up (resolves the arrays'
+ *    device addresses, raises kernel shared-memory limits); make it before any
+ *    stream capture.
+ *  - Every call shares the arrays: calls that overlap on the GPU (different
+ *    streams, or different host threads) race on the partials. Serialise them.
+ * ------------------------------------------------------------------------ */
+int shgemm_b200_shgemm_noalloc(void* cuda_stream, int op_a, int op_b, size_t m, size_t n, size_t k,
+                               const float* alpha, const float* a, size_t lda, const void* b, size_t ldb,
+                               const float* beta, float* c, size_t ldc, int compute_type, int op_c, int* level_out);
+
+/* Size of the allocation-free path's scratch array in bytes. No counterpart in the reference. */
+size_t shgemm_b200_noalloc_scratch_bytes(void);
+
+/* Synchronises `cuda_stream` and reports the allocation-free path's device error
+ * word (as shgemm_b200_check_error does for a handle). No counterpart in the reference. */
+int shgemm_b200_noalloc_check_error(void* cuda_stream, int* device_code);
 
 #ifdef __cplusplus
 }

@@ -27,7 +27,7 @@ P0, P1 = 0, 1              # detail::kernel_level (include/shgemm/shgemm.hpp:30-
 CFG_SPLIT_K, CFG_WAIT_LIMIT_MS, CFG_GROUP_M = 2, 3, 4
 
 STATUS = {0: "OK", 1: "INVALID_VALUE", 2: "NOT_SUPPORTED", 3: "ALLOC_FAILED", 4: "LAUNCH_FAILED",
-          5: "TIMEOUT", 6: "CUDA_ERROR"}
+          5: "TIMEOUT", 6: "CUDA_ERROR", 7: "SCRATCH_TOO_SMALL"}
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 _LIB_PATH = os.path.join(_HERE, "libshgemm_b200.so")
@@ -71,11 +71,15 @@ def lib() -> ctypes.CDLL:
         "shgemm_b200_eval_dgemm": [vp, i, i, sz, sz, sz, vp, sz, vp, sz, vp],
         "shgemm_b200_eval_dgemm_hs": [vp, i, i, sz, sz, sz, vp, sz, vp, sz, vp],
         "shgemm_b200_eval_error": [vp, sz, sz, vp, sz, i, vp, d, d, vp, pd],
+        "shgemm_b200_shgemm_noalloc": [vp, i, i, sz, sz, sz, pf, vp, sz, vp, sz, pf, vp, sz, i, i, pi],
+        "shgemm_b200_noalloc_check_error": [vp, pi],
     }
     for name, args in sig.items():
         fn = getattr(L, name)
         fn.argtypes = args
         fn.restype = i
+    L.shgemm_b200_noalloc_scratch_bytes.argtypes = []
+    L.shgemm_b200_noalloc_scratch_bytes.restype = sz
     L.shgemm_b200_status_string.argtypes = [i]
     L.shgemm_b200_status_string.restype = ctypes.c_char_p
     _lib = L
@@ -227,3 +231,35 @@ def hsgemm(handle: Handle, op_a: int, op_b: int, m: int, n: int, k: int, alpha: 
                                   ctypes.byref(be), _addr(c), ldc, compute_type, op_c, ctypes.byref(lv))
     _check(st, "hsgemm")
     return lv.value
+
+
+# ---------------------------------------------------------------- allocation-free path
+def shgemm_noalloc(stream, op_a: int, op_b: int, m: int, n: int, k: int, alpha: float, a, lda: int, b, ldb: int,
+                   beta: float, c, ldc: int, compute_type: int, op_c: int = op_n) -> int:
+    """SHGEMM that allocates nothing: no handle, scratch in a fixed device array.
+
+    For callers that cannot call cudaMalloc (an allocator callback, a memory
+    manager that owns all device memory). Runs on the current device and
+    `stream`; m * n is limited by noalloc_scratch_bytes() / 8. Concurrent calls
+    share the scratch and must not overlap on the GPU. The first call on a device
+    does its one-time set-up and should come before any stream capture.
+    """
+    al, be, lv = ctypes.c_float(alpha), ctypes.c_float(beta), ctypes.c_int(0)
+    st = lib().shgemm_b200_shgemm_noalloc(ctypes.c_void_p(_stream_addr(stream)), op_a, op_b, m, n, k,
+                                          ctypes.byref(al), _addr(a), lda, _addr(b), ldb, ctypes.byref(be), _addr(c),
+                                          ldc, compute_type, op_c, ctypes.byref(lv))
+    _check(st, "shgemm_noalloc")
+    return lv.value
+
+
+def noalloc_scratch_bytes() -> int:
+    return lib().shgemm_b200_noalloc_scratch_bytes()
+
+
+def noalloc_check_error(stream) -> int:
+    """Synchronises `stream`; returns the allocation-free path's device error code."""
+    code = ctypes.c_int()
+    st = lib().shgemm_b200_noalloc_check_error(ctypes.c_void_p(_stream_addr(stream)), ctypes.byref(code))
+    if st not in (0, 5):
+        raise ShgemmError(st, "noalloc_check_error")
+    return code.value

@@ -355,6 +355,7 @@ const char* shgemm_b200_status_string(int s) {
         case SHGEMM_STATUS_LAUNCH_FAILED: return "SHGEMM_STATUS_LAUNCH_FAILED";
         case SHGEMM_STATUS_TIMEOUT: return "SHGEMM_STATUS_TIMEOUT";
         case SHGEMM_STATUS_CUDA_ERROR: return "SHGEMM_STATUS_CUDA_ERROR";
+        case SHGEMM_STATUS_SCRATCH_TOO_SMALL: return "SHGEMM_STATUS_SCRATCH_TOO_SMALL";
         default: return "SHGEMM_STATUS_UNKNOWN";
     }
 }
@@ -773,6 +774,123 @@ int shgemm_b200_eval_error(shgemm_b200_handle_t h, size_t m, size_t n, const flo
     out[2] = mx;
     out[3] = mm;
     return SHGEMM_STATUS_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Allocation-free split-K entry point.
+//
+// For callers that cannot call cudaMalloc (for example code running inside an
+// allocator callback, a custom memory manager that forbids other allocations, or
+// a process whose device memory is fully reserved up front). It runs the same
+// tile kernel and split-K reduction as shgemm_b200_shgemm, but keeps the split-K
+// partials and the error word in file-scope device arrays instead of a handle's
+// workspace, so it needs no handle and allocates nothing.
+//
+// The scratch array below is part of the library image: every GPU that loads
+// the library holds it (16 MiB) until the process exits.
+namespace {
+constexpr size_t kNoAllocScratchBytes = size_t(16) << 20;
+static __device__ __align__(256) float g_noalloc_scratch[kNoAllocScratchBytes / sizeof(float)];
+static __device__ __align__(256) int g_noalloc_error;
+
+struct NoAllocDevice {
+    bool ready = false;
+    int num_sms = 0;
+    float* scratch = nullptr;  // device address of g_noalloc_scratch on this device
+    int* error_word = nullptr; // device address of g_noalloc_error on this device
+};
+constexpr int kNoAllocMaxDevices = 64;
+NoAllocDevice g_noalloc_dev[kNoAllocMaxDevices];
+std::mutex g_noalloc_mutex;
+
+// One-time set-up on the current device: resolve the device addresses of the
+// file-scope arrays (their names are host-side stand-ins in host code) and raise
+// the dynamic shared memory limit of every tile kernel. Allocates nothing.
+int noalloc_setup(int dev, NoAllocDevice*& out) {
+    if (dev < 0 || dev >= kNoAllocMaxDevices) return SHGEMM_STATUS_NOT_SUPPORTED;
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    NoAllocDevice& d = g_noalloc_dev[dev];
+    if (!d.ready) {
+        int major = 0, minor = 0, sms = 0;
+        cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev);
+        cudaDeviceGetAttribute(&minor, cudaDevAttrComputeCapabilityMinor, dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        if (major != 10 || minor != 0 || !encode_fn()) return SHGEMM_STATUS_NOT_SUPPORTED;
+        void* sp = nullptr;
+        void* ep = nullptr;
+        if (cudaGetSymbolAddress(&sp, g_noalloc_scratch) != cudaSuccess ||
+            cudaGetSymbolAddress(&ep, g_noalloc_error) != cudaSuccess) {
+            cudaGetLastError();
+            return SHGEMM_STATUS_CUDA_ERROR;
+        }
+        for (int tc = 0; tc < 2; ++tc)
+            for (int bn : {64, 128, 256})
+                for (int ak = 0; ak < 2; ++ak)
+                    for (int bk = 0; bk < 2; ++bk) {
+                        KernelEntry e = kernel_table(tc, bn, ak, bk);
+                        if (!e.fn) continue;
+                        if (cudaFuncSetAttribute(e.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, e.smem) !=
+                            cudaSuccess) {
+                            cudaGetLastError();
+                            return SHGEMM_STATUS_NOT_SUPPORTED;
+                        }
+                    }
+        d.num_sms = sms;
+        d.scratch = static_cast<float*>(sp);
+        d.error_word = static_cast<int*>(ep);
+        d.ready = true;
+    }
+    out = &d;
+    return SHGEMM_STATUS_OK;
+}
+}  // namespace
+
+extern "C" {
+
+size_t shgemm_b200_noalloc_scratch_bytes(void) { return kNoAllocScratchBytes; }
+
+int shgemm_b200_shgemm_noalloc(void* cuda_stream, int op_a, int op_b, size_t m, size_t n, size_t k,
+                               const float* alpha, const float* a, size_t lda, const void* b, size_t ldb,
+                               const float* beta, float* c, size_t ldc, int compute_type, int op_c, int* level_out) {
+    if (!alpha || !beta) return SHGEMM_STATUS_INVALID_VALUE;
+    // The split-K partials need at least two slices of m x n floats in the scratch.
+    if (m * n > kNoAllocScratchBytes / sizeof(float) / 2) return SHGEMM_STATUS_SCRATCH_TOO_SMALL;
+    if (k > 0 && ((reinterpret_cast<uintptr_t>(a) & 15) || (reinterpret_cast<uintptr_t>(b) & 15) || (lda * 4) % 16 ||
+                  (ldb * 2) % 16))
+        return SHGEMM_STATUS_NOT_SUPPORTED;  // the staging path would need more scratch
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return SHGEMM_STATUS_CUDA_ERROR;
+    NoAllocDevice* d = nullptr;
+    const int st = noalloc_setup(dev, d);
+    if (st != SHGEMM_STATUS_OK) return st;
+    // A stack-resident handle: the existing dispatch path, pointed at the static arrays.
+    shgemm_b200_handle h;
+    h.device = dev;
+    h.num_sms = d->num_sms;
+    h.stream = static_cast<cudaStream_t>(cuda_stream);
+    h.workspace = d->scratch;
+    h.workspace_bytes = kNoAllocScratchBytes;
+    h.error_word = d->error_word;
+    // The error word keeps the previous call's value: clear it first.
+    if (cudaMemsetAsync(d->error_word, 0, sizeof(int), h.stream) != cudaSuccess) return SHGEMM_STATUS_CUDA_ERROR;
+    return shgemm_b200_shgemm(&h, op_a, op_b, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc, compute_type, op_c,
+                              level_out);
+}
+
+int shgemm_b200_noalloc_check_error(void* cuda_stream, int* device_code) {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return SHGEMM_STATUS_CUDA_ERROR;
+    NoAllocDevice* d = nullptr;
+    const int st = noalloc_setup(dev, d);
+    if (st != SHGEMM_STATUS_OK) return st;
+    if (cudaStreamSynchronize(static_cast<cudaStream_t>(cuda_stream)) != cudaSuccess) return SHGEMM_STATUS_CUDA_ERROR;
+    int code = 0;
+    if (cudaMemcpy(&code, d->error_word, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess)
+        return SHGEMM_STATUS_CUDA_ERROR;
+    if (device_code) *device_code = code;
+    return code ? SHGEMM_STATUS_TIMEOUT : SHGEMM_STATUS_OK;
 }
 
 }  // extern "C"
