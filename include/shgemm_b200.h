@@ -81,6 +81,42 @@ int shgemm_b200_hsgemm(shgemm_b200_handle_t handle, int op_a, int op_b, size_t m
                        const float* alpha, const void* a, size_t lda, const float* b, size_t ldb,
                        const float* beta, float* c, size_t ldc, int compute_type, int op_c, int* level_out);
 
+/* ------------------------------------------------------------------------
+ * Grouped launches (no reference counterpart; the reference's equivalent is a
+ * host loop of shgemm calls, one launch each). Many independent problems
+ * C_i = alpha_i op(A_i) op(B_i) + beta_i C_i in ONE persistent launch: a
+ * per-problem table of TMA descriptors and a unit list (tiles, longest first)
+ * in device memory, built on the host. All problems share op_a, op_b (op_n
+ * only), op_c and the compute type; operands must be TMA-addressable (16-byte
+ * aligned bases and leading dimensions). Tile N per problem: the smallest of
+ * 32/64/128/256 (TF32: up to 128) covering n_i.
+ * ------------------------------------------------------------------------ */
+typedef struct shgemm_b200_problem {
+    size_t m, n, k;
+    const float* a;
+    size_t lda;
+    const void* b; /* binary16 */
+    size_t ldb;
+    float* c;
+    size_t ldc;
+    float alpha, beta;
+} shgemm_b200_problem;
+
+/* Enqueues (on the handle's stream) the copy of the batch's tables from the
+ * handle's pinned host staging to the device and one grouped kernel launch.
+ * Can be captured in a CUDA graph: replaying the graph copies whatever the
+ * staging holds, so shgemm_b200_grouped_update + cudaGraphLaunch runs a new
+ * batch with the captured launch (up to the captured number of problems).
+ * At most 8192 problems and 65536 tiles per batch. */
+int shgemm_b200_shgemm_grouped(shgemm_b200_handle_t handle, int op_a, int op_b, int compute_type, int op_c,
+                               const shgemm_b200_problem* problems, int count);
+
+/* Rewrites the pinned host staging with a new batch without enqueueing anything
+ * (for replaying a captured grouped launch). The batch must use the op_a,
+ * compute type and op_c the launch was captured with. */
+int shgemm_b200_grouped_update(shgemm_b200_handle_t handle, int op_a, int op_b, int compute_type, int op_c,
+                               const shgemm_b200_problem* problems, int count);
+
 /* Tunables (no reference counterpart). */
 int shgemm_b200_set_config(shgemm_b200_handle_t handle, int key, long long value);
 int shgemm_b200_get_config(shgemm_b200_handle_t handle, int key, long long* value);

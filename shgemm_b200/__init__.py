@@ -34,6 +34,14 @@ _LIB_PATH = os.path.join(_HERE, "libshgemm_b200.so")
 _lib = None
 
 
+class Problem(ctypes.Structure):
+    """shgemm_b200_problem: one problem of a grouped launch (include/shgemm_b200.h)."""
+
+    _fields_ = [("m", ctypes.c_size_t), ("n", ctypes.c_size_t), ("k", ctypes.c_size_t), ("a", ctypes.c_void_p),
+                ("lda", ctypes.c_size_t), ("b", ctypes.c_void_p), ("ldb", ctypes.c_size_t), ("c", ctypes.c_void_p),
+                ("ldc", ctypes.c_size_t), ("alpha", ctypes.c_float), ("beta", ctypes.c_float)]
+
+
 class ShgemmError(RuntimeError):
     def __init__(self, status: int, what: str):
         self.status = status
@@ -72,6 +80,8 @@ def lib() -> ctypes.CDLL:
         "shgemm_b200_eval_dgemm_hs": [vp, i, i, sz, sz, sz, vp, sz, vp, sz, vp],
         "shgemm_b200_eval_error": [vp, sz, sz, vp, sz, i, vp, d, d, vp, pd],
         "shgemm_b200_shgemm_noalloc": [vp, i, i, sz, sz, sz, pf, vp, sz, vp, sz, pf, vp, sz, i, i, pi],
+        "shgemm_b200_shgemm_grouped": [vp, i, i, i, i, ctypes.POINTER(Problem), i],
+        "shgemm_b200_grouped_update": [vp, i, i, i, i, ctypes.POINTER(Problem), i],
         "shgemm_b200_noalloc_check_error": [vp, pi],
     }
     for name, args in sig.items():
@@ -263,3 +273,38 @@ def noalloc_check_error(stream) -> int:
     if st not in (0, 5):
         raise ShgemmError(st, "noalloc_check_error")
     return code.value
+
+
+# ---------------------------------------------------------------- grouped launches
+def _problem_array(problems):
+    arr = (Problem * max(1, len(problems)))()
+    for i, q in enumerate(problems):
+        if isinstance(q, Problem):
+            arr[i] = q
+            continue
+        m, n, k, a, lda, b, ldb, c, ldc = q[:9]
+        alpha = q[9] if len(q) > 9 else 1.0
+        beta = q[10] if len(q) > 10 else 0.0
+        arr[i] = Problem(m, n, k, _addr(a), lda, _addr(b), ldb, _addr(c), ldc, alpha, beta)
+    return arr
+
+
+def shgemm_grouped(handle: Handle, problems, compute_type: int, op_a: int = op_n, op_b: int = op_n,
+                   op_c: int = op_n) -> None:
+    """Many SHGEMMs in one persistent launch.
+
+    ``problems``: sequence of ``(m, n, k, A, lda, B, ldb, C, ldc[, alpha[, beta]])`` (tensors or
+    device addresses) or :class:`Problem`. Enqueued on the handle's stream; can be captured in a
+    CUDA graph and replayed after :func:`grouped_update`.
+    """
+    arr = _problem_array(problems)
+    _check(lib().shgemm_b200_shgemm_grouped(handle.ptr, op_a, op_b, compute_type, op_c, arr, len(problems)),
+           "shgemm_grouped")
+
+
+def grouped_update(handle: Handle, problems, compute_type: int, op_a: int = op_n, op_b: int = op_n,
+                   op_c: int = op_n) -> None:
+    """Rewrites the staged tables (no launch): the next replay of a captured grouped launch runs this batch."""
+    arr = _problem_array(problems)
+    _check(lib().shgemm_b200_grouped_update(handle.ptr, op_a, op_b, compute_type, op_c, arr, len(problems)),
+           "grouped_update")

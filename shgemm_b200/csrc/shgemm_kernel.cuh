@@ -126,6 +126,98 @@ __device__ __forceinline__ void step_range(const TileGemmParams& p, int slice, i
     s1 = min(s0 + p.steps_per_slice, total_steps);
 }
 
+// One grouped problem: C (m x n) = alpha * op(A) * op(B) + beta * C, with its TMA
+// descriptors; built on the host and copied to device memory before the launch.
+struct alignas(64) GroupedProblem {
+    CUtensorMap tmap_a;
+    CUtensorMap tmap_b;
+    float* c;
+    uint64_t ldc;
+    int m, n, k;
+    int bn;     // tile N of this problem (<= the kernel's BN; 16-multiple)
+    int steps;  // k-steps
+    float alpha, beta;
+    int pad[3];
+};
+static_assert(sizeof(GroupedProblem) % 64 == 0, "GroupedProblem alignment");
+
+struct alignas(64) GroupedParams {
+    const GroupedProblem* problems;
+    const int2* units;      // {problem, tm | tn << 16}, longest first
+    const int* num_units;   // in device memory: a captured graph relaunches with new tables
+    int* error_flag;
+    uint64_t wait_limit_ns;
+    int op_c;
+};
+
+// What one work unit (a 128 x bn tile of one problem over a range of k-steps) needs.
+struct UnitDesc {
+    const CUtensorMap* tmap_a;
+    const CUtensorMap* tmap_b;
+    float* c;
+    uint64_t ldc;
+    float* partial;  // split-K: this slice's partial buffer [n][m]; null: write C
+    int m, n;
+    int tm, tn;
+    int s0, s1;  // k-step range
+    int bn;      // tile N
+    float alpha, beta;
+    bool maps_in_global;  // descriptors written by a copy before the launch
+};
+
+template <class Cfg>
+__device__ __forceinline__ void get_unit(const TileGemmParams& p, int u, UnitDesc& d) {
+    int tm, tn, slice, s0, s1;
+    decode_unit(p, u, tm, tn, slice);
+    step_range(p, slice, (p.k + Cfg::BK - 1) / Cfg::BK, s0, s1);
+    d.tmap_a = &p.tmap_a;
+    d.tmap_b = &p.tmap_b;
+    d.c = p.c;
+    d.ldc = p.ldc;
+    d.partial = p.num_slices > 1 ? p.workspace + static_cast<size_t>(slice) * p.n * p.m : nullptr;
+    d.m = p.m;
+    d.n = p.n;
+    d.tm = tm;
+    d.tn = tn;
+    d.s0 = s0;
+    d.s1 = s1;
+    d.bn = Cfg::BN;
+    d.alpha = p.alpha;
+    d.beta = p.beta;
+    d.maps_in_global = false;
+}
+
+template <class Cfg>
+__device__ __forceinline__ void get_unit(const GroupedParams& p, int u, UnitDesc& d) {
+    const int2 e = p.units[u];
+    const GroupedProblem& q = p.problems[e.x];
+    d.tmap_a = &q.tmap_a;
+    d.tmap_b = &q.tmap_b;
+    d.c = q.c;
+    d.ldc = q.ldc;
+    d.partial = nullptr;
+    d.m = q.m;
+    d.n = q.n;
+    d.tm = e.y & 0xFFFF;
+    d.tn = e.y >> 16;
+    d.s0 = 0;
+    d.s1 = q.steps;
+    d.bn = q.bn;
+    d.alpha = q.alpha;
+    d.beta = q.beta;
+    d.maps_in_global = true;
+}
+
+__device__ __forceinline__ int unit_count(const TileGemmParams& p) { return p.num_units; }
+__device__ __forceinline__ int unit_count(const GroupedParams& p) { return *p.num_units; }
+__device__ __forceinline__ int output_op(const TileGemmParams& p) { return p.op_c; }
+__device__ __forceinline__ int output_op(const GroupedParams& p) { return p.op_c; }
+__device__ __forceinline__ void prefetch_params_maps(const TileGemmParams& p) {
+    ptx::tma_prefetch_desc(&p.tmap_a);
+    ptx::tma_prefetch_desc(&p.tmap_b);
+}
+__device__ __forceinline__ void prefetch_params_maps(const GroupedParams&) {}
+
 // ---------------------------------------------------------------------------
 // Split helpers. hi = T(v), lo = T(2^11 (v - hi)), T = binary16 round-to-nearest-
 // even or TF32 round-to-nearest-away: the reference's split (src/wmmae_shgemm.hpp:30-31).
@@ -342,8 +434,8 @@ __device__ __forceinline__ bool split_step(uint8_t* a_st, uint8_t* b_st, int sid
     }
 }
 
-template <int TC, int BN, bool A_KMAJOR, bool B_KMAJOR>
-__global__ void __launch_bounds__(512, 1) shgemm_tile_kernel(const __grid_constant__ TileGemmParams p) {
+template <int TC, int BN, bool A_KMAJOR, bool B_KMAJOR, class Params>
+__device__ __forceinline__ void tile_kernel_body(const Params& p) {
     using Cfg = TileCfg<TC, BN, A_KMAJOR, B_KMAJOR>;
     constexpr int SA = Cfg::SA;
     constexpr int SB = Cfg::SB;
@@ -391,10 +483,7 @@ __global__ void __launch_bounds__(512, 1) shgemm_tile_kernel(const __grid_consta
         *abort_flag = 0;
         ptx::fence_mbarrier_init();
     }
-    if (warp == 0 && lane == 0) {
-        ptx::tma_prefetch_desc(&p.tmap_a);
-        ptx::tma_prefetch_desc(&p.tmap_b);
-    }
+    if (warp == 0 && lane == 0) prefetch_params_maps(p);
     if (warp == 1) {
         ptx::tmem_alloc(tmem_slot, Cfg::TMEM_COLS);
     }
@@ -403,7 +492,7 @@ __global__ void __launch_bounds__(512, 1) shgemm_tile_kernel(const __grid_consta
     ptx::tc_fence_after();
     const uint32_t tmem_base = *tmem_slot;
 
-    const int total_steps = (p.k + Cfg::BK - 1) / Cfg::BK;
+    const int num_units = unit_count(p);
     const uint64_t limit = p.wait_limit_ns;
 
     auto fail = [&](int code) {
@@ -420,10 +509,14 @@ __global__ void __launch_bounds__(512, 1) shgemm_tile_kernel(const __grid_consta
             int as = 0, bs = 0;
             uint32_t aph = 0, bph = 0;
             uint32_t a_issued = 0, a_par = 0, b_issued = 0, b_par = 0;  // per stage: load in flight, its parity
-            for (int u = blockIdx.x; u < p.num_units; u += gridDim.x) {
-                int tm, tn, slice, s0, s1;
-                decode_unit(p, u, tm, tn, slice);
-                step_range(p, slice, total_steps, s0, s1);
+            for (int u = blockIdx.x; u < num_units; u += gridDim.x) {
+                UnitDesc ud;
+                get_unit<Cfg>(p, u, ud);
+                const int tm = ud.tm, tn = ud.tn, s0 = ud.s0, s1 = ud.s1;
+                if (ud.maps_in_global) {
+                    ptx::fence_tensormap_acquire(ud.tmap_a);
+                    ptx::fence_tensormap_acquire(ud.tmap_b);
+                }
                 for (int st = s0; st < s1; ++st) {
                     const int kc = st * Cfg::BK;
                     if (!ptx::mbar_wait(&a_empty[as], aph ^ 1u, abort_flag, limit)) {
@@ -436,10 +529,10 @@ __global__ void __launch_bounds__(512, 1) shgemm_tile_kernel(const __grid_consta
                         if constexpr (A_KMAJOR) {
 #pragma unroll
                             for (int sub = 0; sub < Cfg::BK / 32; ++sub)
-                                ptx::tma_load_2d(a_dst + sub * (Cfg::BM * 128), &p.tmap_a, &a_full[as],
+                                ptx::tma_load_2d(a_dst + sub * (Cfg::BM * 128), ud.tmap_a, &a_full[as],
                                                  kc + 32 * sub, tm * Cfg::BM);
                         } else {
-                            ptx::tma_load_2d(a_dst, &p.tmap_a, &a_full[as], tm * Cfg::BM, kc);
+                            ptx::tma_load_2d(a_dst, ud.tmap_a, &a_full[as], tm * Cfg::BM, kc);
                         }
                         a_issued |= 1u << as;
                         a_par = (a_par & ~(1u << as)) | (aph << as);
@@ -454,16 +547,16 @@ __global__ void __launch_bounds__(512, 1) shgemm_tile_kernel(const __grid_consta
                     }
                     {
                         uint8_t* b_dst = b_base + bs * Cfg::B_STAGE;
-                        ptx::mbar_arrive_expect_tx(&b_full[bs], Cfg::B_RAW);
+                        ptx::mbar_arrive_expect_tx(&b_full[bs], ud.bn * Cfg::BK * 2);
                         if constexpr (B_KMAJOR) {
-                            ptx::tma_load_2d(b_dst, &p.tmap_b, &b_full[bs], kc, tn * BN);
+                            ptx::tma_load_2d(b_dst, ud.tmap_b, &b_full[bs], kc, tn * ud.bn);
                         } else if constexpr (!kTf32) {
 #pragma unroll
                             for (int sub = 0; sub < BN / 64; ++sub)
-                                ptx::tma_load_2d(b_dst + sub * (Cfg::BK * 128), &p.tmap_b, &b_full[bs],
+                                ptx::tma_load_2d(b_dst + sub * (Cfg::BK * 128), ud.tmap_b, &b_full[bs],
                                                  tn * BN + 64 * sub, kc);
                         } else {
-                            ptx::tma_load_2d(b_dst, &p.tmap_b, &b_full[bs], tn * BN, kc);
+                            ptx::tma_load_2d(b_dst, ud.tmap_b, &b_full[bs], tn * BN, kc);
                         }
                         b_issued |= 1u << bs;
                         b_par = (b_par & ~(1u << bs)) | (bph << bs);
@@ -494,15 +587,14 @@ __global__ void __launch_bounds__(512, 1) shgemm_tile_kernel(const __grid_consta
     } else if (warp == 1) {
         // ------------------------------------------------------------ UMMA issuer
         if (lane == 0) {
-            constexpr uint32_t idesc = ptx::make_idesc(kTf32, !A_KMAJOR && !kTf32, !kTf32 && !B_KMAJOR, Cfg::BM, BN);
             int as = 0, bs = 0;
             uint32_t aph = 0, bph = 0, gc = 0;
             bool issued_any = false;
-            for (int u = blockIdx.x; u < p.num_units; u += gridDim.x) {
-                int tm, tn, slice, s0, s1;
-                decode_unit(p, u, tm, tn, slice);
-                step_range(p, slice, total_steps, s0, s1);
-                const int nsteps = s1 - s0;
+            for (int u = blockIdx.x; u < num_units; u += gridDim.x) {
+                UnitDesc ud;
+                get_unit<Cfg>(p, u, ud);
+                const int nsteps = ud.s1 - ud.s0;
+                const uint32_t idesc = ptx::make_idesc(kTf32, !A_KMAJOR && !kTf32, !kTf32 && !B_KMAJOR, Cfg::BM, ud.bn);
                 for (int i = 0; i < nsteps; ++i) {
                     const uint32_t db = gc & 1u;
                     if (!ptx::mbar_wait(&d_empty[db], ((gc >> 1) & 1u) ^ 1u, abort_flag, limit)) {
@@ -596,11 +688,10 @@ __global__ void __launch_bounds__(512, 1) shgemm_tile_kernel(const __grid_consta
         const int sidx = (warp - 2) * 32 + lane;
         int as = 0, bs = 0;
         uint32_t aph = 0, bph = 0;
-        for (int u = blockIdx.x; u < p.num_units; u += gridDim.x) {
-            int tm, tn, slice, s0, s1;
-            decode_unit(p, u, tm, tn, slice);
-            step_range(p, slice, total_steps, s0, s1);
-            for (int st = s0; st < s1; ++st) {
+        for (int u = blockIdx.x; u < num_units; u += gridDim.x) {
+            UnitDesc ud;
+            get_unit<Cfg>(p, u, ud);
+            for (int st = ud.s0; st < ud.s1; ++st) {
                 if (!ptx::mbar_wait(&a_full[as], aph, abort_flag, limit) ||
                     (kTf32 && !ptx::mbar_wait(&b_full[bs], bph, abort_flag, limit))) {
                     fail(kErrSplitTimeout);
@@ -645,11 +736,12 @@ __global__ void __launch_bounds__(512, 1) shgemm_tile_kernel(const __grid_consta
         const int row_in_tile = q * 32 + lane;
         const uint32_t lane_addr = static_cast<uint32_t>(q * 32) << 16;
         uint32_t gc = 0;
-        for (int u = blockIdx.x; u < p.num_units; u += gridDim.x) {
-            int tm, tn, slice, s0, s1;
-            decode_unit(p, u, tm, tn, slice);
-            step_range(p, slice, total_steps, s0, s1);
+        for (int u = blockIdx.x; u < num_units; u += gridDim.x) {
+            UnitDesc ud;
+            get_unit<Cfg>(p, u, ud);
+            const int tm = ud.tm, tn = ud.tn, s0 = ud.s0, s1 = ud.s1;
             const int nsteps = s1 - s0;
+            const int hn = ud.bn / 2;  // columns of this warp's half (<= HN)
             uint64_t acc2[HN / 2];  // running sums, packed in pairs of columns
 #pragma unroll
             for (int j = 0; j < HN / 2; ++j) acc2[j] = 0ull;
@@ -662,8 +754,9 @@ __global__ void __launch_bounds__(512, 1) shgemm_tile_kernel(const __grid_consta
                 ptx::tc_fence_after();
 #pragma unroll
                 for (int j0 = 0; j0 < HN; j0 += 32) {
+                    if (j0 >= hn) break;
                     uint32_t r0[16], r1[16];
-                    const uint32_t ta = tmem_base + lane_addr + db * BN + half * HN + j0;
+                    const uint32_t ta = tmem_base + lane_addr + db * BN + half * hn + j0;
                     ptx::tmem_ld_32x32b_x16(ta, r0);
                     ptx::tmem_ld_32x32b_x16(ta + 16, r1);
                     ptx::tmem_ld_wait();
@@ -683,35 +776,35 @@ __global__ void __launch_bounds__(512, 1) shgemm_tile_kernel(const __grid_consta
             {
                 auto acc = [&](int j) -> float { return (j & 1) ? ptx::f2_hi(acc2[j >> 1]) : ptx::f2_lo(acc2[j >> 1]); };
                 const int row = tm * Cfg::BM + row_in_tile;
-                const int col0 = tn * BN + half * HN;
-                if (row < p.m) {
-                    if (p.num_slices > 1) {
-                        float* w = p.workspace + static_cast<size_t>(slice) * p.n * p.m + row;
+                const int col0 = tn * ud.bn + half * hn;
+                if (row < ud.m) {
+                    if (ud.partial) {
+                        float* w = ud.partial + row;
 #pragma unroll
                         for (int j = 0; j < HN; ++j) {
                             const int col = col0 + j;
-                            if (col < p.n) w[static_cast<size_t>(col) * p.m] = acc(j);
+                            if (j < hn && col < ud.n) w[static_cast<size_t>(col) * ud.m] = acc(j);
                         }
-                    } else if (p.op_c == kOpN) {
-                        float* cp = p.c + row;
+                    } else if (output_op(p) == kOpN) {
+                        float* cp = ud.c + row;
 #pragma unroll
                         for (int j = 0; j < HN; ++j) {
                             const int col = col0 + j;
-                            if (col < p.n) {
-                                float* dst = cp + static_cast<size_t>(col) * p.ldc;
-                                *dst = (p.beta == 0.0f) ? __fmul_rn(acc(j), p.alpha)
-                                                        : __fmaf_rn(acc(j), p.alpha, __fmul_rn(p.beta, *dst));
+                            if (j < hn && col < ud.n) {
+                                float* dst = cp + static_cast<size_t>(col) * ud.ldc;
+                                *dst = (ud.beta == 0.0f) ? __fmul_rn(acc(j), ud.alpha)
+                                                         : __fmaf_rn(acc(j), ud.alpha, __fmul_rn(ud.beta, *dst));
                             }
                         }
                     } else {
-                        float* cp = p.c + static_cast<size_t>(row) * p.ldc;
+                        float* cp = ud.c + static_cast<size_t>(row) * ud.ldc;
 #pragma unroll
                         for (int j = 0; j < HN; ++j) {
                             const int col = col0 + j;
-                            if (col < p.n) {
+                            if (j < hn && col < ud.n) {
                                 float* dst = cp + col;
-                                *dst = (p.beta == 0.0f) ? __fmul_rn(acc(j), p.alpha)
-                                                        : __fmaf_rn(acc(j), p.alpha, __fmul_rn(p.beta, *dst));
+                                *dst = (ud.beta == 0.0f) ? __fmul_rn(acc(j), ud.alpha)
+                                                         : __fmaf_rn(acc(j), ud.alpha, __fmul_rn(ud.beta, *dst));
                             }
                         }
                     }
@@ -727,6 +820,18 @@ __global__ void __launch_bounds__(512, 1) shgemm_tile_kernel(const __grid_consta
     if (warp == 1) {
         ptx::tmem_dealloc(tmem_base, Cfg::TMEM_COLS);
     }
+}
+
+// Single problem (optionally split-K): descriptors in the kernel's parameter space.
+template <int TC, int BN, bool A_KMAJOR, bool B_KMAJOR>
+__global__ void __launch_bounds__(512, 1) shgemm_tile_kernel(const __grid_constant__ TileGemmParams p) {
+    tile_kernel_body<TC, BN, A_KMAJOR, B_KMAJOR>(p);
+}
+
+// Many problems in one launch: per-problem descriptors and a unit list in device memory.
+template <int TC, int BN, bool A_KMAJOR, bool B_KMAJOR>
+__global__ void __launch_bounds__(512, 1) shgemm_grouped_kernel(const __grid_constant__ GroupedParams p) {
+    tile_kernel_body<TC, BN, A_KMAJOR, B_KMAJOR>(p);
 }
 
 }  // namespace shgemm_b200

@@ -33,6 +33,13 @@ struct shgemm_b200_handle {
     size_t workspace_bytes = 0;
     int* error_word = nullptr;
     std::atomic<long long> launches{0};
+    // grouped launches: problem table + unit list, device copy and pinned host staging
+    void* grouped_dev = nullptr;
+    void* grouped_host = nullptr;
+    cudaEvent_t grouped_copied = nullptr;
+    int grouped_tc = -1, grouped_op_a = -1, grouped_op_b = -1, grouped_op_c = -1;
+    int grouped_units = 0;
+    int grouped_copied_count = 0;  // problem slots the last enqueued copy covers
 };
 
 namespace {
@@ -98,6 +105,28 @@ KernelEntry kernel_table(int tc, int bn, int ak, int bk) {
 #undef SHG_ENTRY
     return {nullptr, 0};
 }
+
+template <int TC, int BN, bool AK>
+void* grouped_kernel_ptr() {
+    return reinterpret_cast<void*>(&shgemm_grouped_kernel<TC, BN, AK, true>);
+}
+
+// Grouped kernels: binary16 compute with tile N up to 256, TF32 up to 128; B K-major.
+constexpr int kGroupedMaxBnF16 = 256, kGroupedMaxBnTf32 = 128;
+KernelEntry grouped_table(int tc, int ak) {
+    if (tc == kFP16)
+        return ak ? KernelEntry{grouped_kernel_ptr<kFP16, kGroupedMaxBnF16, true>(), tile_smem<kFP16, kGroupedMaxBnF16, true, true>()}
+                  : KernelEntry{grouped_kernel_ptr<kFP16, kGroupedMaxBnF16, false>(), tile_smem<kFP16, kGroupedMaxBnF16, false, true>()};
+    return ak ? KernelEntry{grouped_kernel_ptr<kTF32, kGroupedMaxBnTf32, true>(), tile_smem<kTF32, kGroupedMaxBnTf32, true, true>()}
+              : KernelEntry{grouped_kernel_ptr<kTF32, kGroupedMaxBnTf32, false>(), tile_smem<kTF32, kGroupedMaxBnTf32, false, true>()};
+}
+
+// Table layout (device copy and host staging): problems, then units, then the unit count.
+constexpr int kGroupedMaxProblems = 8192;
+constexpr int kGroupedMaxUnits = 1 << 16;
+constexpr size_t kGroupedUnitsOff = sizeof(GroupedProblem) * kGroupedMaxProblems;
+constexpr size_t kGroupedCountOff = kGroupedUnitsOff + sizeof(int2) * kGroupedMaxUnits;
+constexpr size_t kGroupedBytes = kGroupedCountOff + 256;
 
 // ------------------------------------------------------------------ small kernels
 // C = beta * C (k == 0: the product is empty).
@@ -409,6 +438,22 @@ int shgemm_b200_create(shgemm_b200_handle_t* out, int device) {
                         return SHGEMM_STATUS_NOT_SUPPORTED;
                     }
                 }
+    for (int tc = 0; tc < 2; ++tc)
+        for (int ak = 0; ak < 2; ++ak) {
+            KernelEntry e = grouped_table(tc, ak);
+            cudaFuncSetAttribute(e.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, e.smem);
+        }
+    if (cudaGetLastError() != cudaSuccess || cudaMalloc(&h->grouped_dev, kGroupedBytes) != cudaSuccess ||
+        cudaMallocHost(&h->grouped_host, kGroupedBytes) != cudaSuccess ||
+        cudaEventCreateWithFlags(&h->grouped_copied, cudaEventDisableTiming) != cudaSuccess) {
+        cudaGetLastError();
+        cudaFree(h->grouped_dev);
+        cudaFreeHost(h->grouped_host);
+        cudaFree(h->workspace);
+        cudaFree(h->error_word);
+        delete h;
+        return SHGEMM_STATUS_ALLOC_FAILED;
+    }
     *out = h;
     return SHGEMM_STATUS_OK;
 }
@@ -416,6 +461,12 @@ int shgemm_b200_create(shgemm_b200_handle_t* out, int device) {
 int shgemm_b200_destroy(shgemm_b200_handle_t h) {
     if (!h) return SHGEMM_STATUS_INVALID_VALUE;
     DeviceGuard g(h->device);
+    if (h->grouped_copied) {
+        cudaEventSynchronize(h->grouped_copied);
+        cudaEventDestroy(h->grouped_copied);
+    }
+    cudaFree(h->grouped_dev);
+    cudaFreeHost(h->grouped_host);
     cudaFree(h->workspace);
     cudaFree(h->error_word);
     delete h;
@@ -773,6 +824,156 @@ int shgemm_b200_eval_error(shgemm_b200_handle_t h, size_t m, size_t n, const flo
     out[1] = std::sqrt(r);
     out[2] = mx;
     out[3] = mm;
+    return SHGEMM_STATUS_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Grouped launches: many problems, one persistent kernel.
+namespace {
+
+int grouped_tile_n(int tc, size_t n) {
+    const int cap = tc == kFP16 ? kGroupedMaxBnF16 : kGroupedMaxBnTf32;
+    int bn = 32;
+    while (bn < cap && static_cast<size_t>(bn) < n) bn *= 2;
+    return bn;
+}
+
+// Writes the problem table and the unit list of a batch into the pinned host staging.
+int grouped_stage(shgemm_b200_handle_t h, int op_a, int op_b, int tc, int op_c, const shgemm_b200_problem* probs,
+                  int count) {
+    if (!h || count < 0 || (count > 0 && !probs)) return SHGEMM_STATUS_INVALID_VALUE;
+    if ((op_a != kOpN && op_a != kOpT) || op_b != kOpN || (op_c != kOpN && op_c != kOpT) ||
+        (tc != kFP16 && tc != kTF32))
+        return op_b == kOpT ? SHGEMM_STATUS_NOT_SUPPORTED : SHGEMM_STATUS_INVALID_VALUE;
+    if (count > kGroupedMaxProblems) return SHGEMM_STATUS_NOT_SUPPORTED;
+    // The staging buffer may still be the source of a pending copy: wait for it.
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    cudaStreamIsCapturing(h->stream, &cap);
+    if (cap == cudaStreamCaptureStatusNone && cudaEventSynchronize(h->grouped_copied) != cudaSuccess)
+        return SHGEMM_STATUS_CUDA_ERROR;
+    auto* host = static_cast<uint8_t*>(h->grouped_host);
+    auto* gp = reinterpret_cast<GroupedProblem*>(host);
+    auto* units = reinterpret_cast<int2*>(host + kGroupedUnitsOff);
+    const int bk = tc == kFP16 ? 64 : 32;
+    struct Cost {
+        long long cost;
+        int2 unit;
+    };
+    std::vector<Cost> list;
+    list.reserve(static_cast<size_t>(count) * 4);
+    for (int i = 0; i < count; ++i) {
+        const shgemm_b200_problem& q = probs[i];
+        GroupedProblem& g = gp[i];
+        std::memset(&g, 0, sizeof(g));
+        if (q.m == 0 || q.n == 0) continue;
+        const size_t a_rows = op_a == kOpN ? q.m : q.k, b_rows = q.k, c_rows = op_c == kOpN ? q.m : q.n;
+        if (!q.c || q.ldc < c_rows) return SHGEMM_STATUS_INVALID_VALUE;
+        if (q.m >= (1u << 31) || q.n >= (1u << 31) || q.k >= (1u << 31) || (q.m + 127) / 128 > 0xFFFF)
+            return SHGEMM_STATUS_NOT_SUPPORTED;
+        const int bn = grouped_tile_n(tc, q.n);
+        const long long tiles_n = static_cast<long long>((q.n + bn - 1) / bn);
+        if (tiles_n > 0x7FFF) return SHGEMM_STATUS_NOT_SUPPORTED;
+        if (q.k > 0) {
+            if (!q.a || !q.b || q.lda < std::max<size_t>(1, a_rows) || q.ldb < std::max<size_t>(1, b_rows))
+                return SHGEMM_STATUS_INVALID_VALUE;
+            if ((reinterpret_cast<uintptr_t>(q.a) & 15) || (reinterpret_cast<uintptr_t>(q.b) & 15) ||
+                (q.lda * 4) % 16 || (q.ldb * 2) % 16)
+                return SHGEMM_STATUS_NOT_SUPPORTED;  // grouped launches take TMA-addressable operands only
+            bool ok = op_a == kOpT ? make_tmap(&g.tmap_a, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, q.a, q.k, q.m, q.lda * 4, 32,
+                                               128, CU_TENSOR_MAP_SWIZZLE_128B)
+                                   : make_tmap(&g.tmap_a, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, q.a, q.m, q.k, q.lda * 4,
+                                               128, bk, CU_TENSOR_MAP_SWIZZLE_NONE);
+            ok = ok && (tc == kFP16 ? make_tmap(&g.tmap_b, CU_TENSOR_MAP_DATA_TYPE_FLOAT16, q.b, q.k, q.n, q.ldb * 2,
+                                                64, bn, CU_TENSOR_MAP_SWIZZLE_128B)
+                                    : make_tmap(&g.tmap_b, CU_TENSOR_MAP_DATA_TYPE_FLOAT16, q.b, q.k, q.n, q.ldb * 2,
+                                                32, bn, CU_TENSOR_MAP_SWIZZLE_64B));
+            if (!ok) return SHGEMM_STATUS_NOT_SUPPORTED;
+        }
+        g.c = q.c;
+        g.ldc = q.ldc;
+        g.m = static_cast<int>(q.m);
+        g.n = static_cast<int>(q.n);
+        g.k = static_cast<int>(q.k);
+        g.bn = bn;
+        g.steps = static_cast<int>((q.k + bk - 1) / bk);
+        g.alpha = q.alpha;
+        g.beta = q.beta;
+        const int tiles_m = static_cast<int>((q.m + 127) / 128);
+        for (int tn = 0; tn < tiles_n; ++tn)
+            for (int tm = 0; tm < tiles_m; ++tm)
+                list.push_back({static_cast<long long>(g.steps + 1) * (bn + 64), make_int2(i, tm | (tn << 16))});
+    }
+    if (list.size() > static_cast<size_t>(kGroupedMaxUnits)) return SHGEMM_STATUS_NOT_SUPPORTED;
+    // Longest units first: the persistent CTAs take them round-robin, which balances
+    // uneven k (greedy longest-processing-time order).
+    std::stable_sort(list.begin(), list.end(), [](const Cost& x, const Cost& y) { return x.cost > y.cost; });
+    for (size_t u = 0; u < list.size(); ++u) units[u] = list[u].unit;
+    *reinterpret_cast<int*>(host + kGroupedCountOff) = static_cast<int>(list.size());
+    h->grouped_tc = tc;
+    h->grouped_op_a = op_a;
+    h->grouped_op_b = op_b;
+    h->grouped_op_c = op_c;
+    h->grouped_units = static_cast<int>(list.size());
+    return SHGEMM_STATUS_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int shgemm_b200_grouped_update(shgemm_b200_handle_t h, int op_a, int op_b, int compute_type, int op_c,
+                               const shgemm_b200_problem* problems, int count) {
+    if (!h) return SHGEMM_STATUS_INVALID_VALUE;
+    DeviceGuard g(h->device);
+    const int prev_tc = h->grouped_tc, prev_a = h->grouped_op_a, prev_c = h->grouped_op_c;
+    const int st = grouped_stage(h, op_a, op_b, compute_type, op_c, problems, count);
+    if (st != SHGEMM_STATUS_OK) return st;
+    // A captured launch was built for one kernel variant and copies a fixed number of
+    // problem slots: the batch must keep the variant and fit those slots.
+    if (prev_tc >= 0 && (prev_tc != compute_type || prev_a != op_a || prev_c != op_c)) return SHGEMM_STATUS_INVALID_VALUE;
+    if (count > h->grouped_copied_count) return SHGEMM_STATUS_INVALID_VALUE;
+    return SHGEMM_STATUS_OK;
+}
+
+int shgemm_b200_shgemm_grouped(shgemm_b200_handle_t h, int op_a, int op_b, int compute_type, int op_c,
+                               const shgemm_b200_problem* problems, int count) {
+    if (!h) return SHGEMM_STATUS_INVALID_VALUE;
+    DeviceGuard g(h->device);
+    const int st = grouped_stage(h, op_a, op_b, compute_type, op_c, problems, count);
+    if (st != SHGEMM_STATUS_OK) return st;
+    // problems, units and count in two copies from the pinned staging (the tables are
+    // fixed-offset so a captured graph replays with whatever the staging holds)
+    if (cudaMemcpyAsync(h->grouped_dev, h->grouped_host, sizeof(GroupedProblem) * static_cast<size_t>(count),
+                        cudaMemcpyHostToDevice, h->stream) != cudaSuccess ||
+        cudaMemcpyAsync(static_cast<uint8_t*>(h->grouped_dev) + kGroupedUnitsOff,
+                        static_cast<uint8_t*>(h->grouped_host) + kGroupedUnitsOff,
+                        kGroupedCountOff + sizeof(int) - kGroupedUnitsOff, cudaMemcpyHostToDevice, h->stream) !=
+            cudaSuccess)
+        return SHGEMM_STATUS_CUDA_ERROR;
+    h->grouped_copied_count = count;
+    cudaEventRecord(h->grouped_copied, h->stream);
+    GroupedParams P;
+    std::memset(&P, 0, sizeof(P));
+    P.problems = static_cast<const GroupedProblem*>(h->grouped_dev);
+    P.units = reinterpret_cast<const int2*>(static_cast<uint8_t*>(h->grouped_dev) + kGroupedUnitsOff);
+    P.num_units = reinterpret_cast<const int*>(static_cast<uint8_t*>(h->grouped_dev) + kGroupedCountOff);
+    P.error_flag = h->error_word;
+    P.wait_limit_ns = static_cast<uint64_t>(h->wait_limit_ms) * 1000000ull;
+    P.op_c = op_c;
+    const KernelEntry e = grouped_table(compute_type, op_a == kOpT);
+    void* args[] = {&P};
+    // One CTA per SM whatever the batch: a captured launch stays valid for other batches.
+    const cudaError_t err = cudaLaunchKernel(e.fn, dim3(h->num_sms), dim3(512), args, e.smem, h->stream);
+    h->launches++;
+    if (err != cudaSuccess) {
+        cudaGetLastError();
+        return SHGEMM_STATUS_LAUNCH_FAILED;
+    }
+    if (h->debug_mode)
+        std::printf("[grouped] problems = %d, units = %d, compute_type = %s\n", count, h->grouped_units,
+                    compute_type == kTF32 ? "TF32" : "FP16");
     return SHGEMM_STATUS_OK;
 }
 

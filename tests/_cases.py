@@ -38,6 +38,17 @@ def make_inputs(rng, m, n, k, op_a, op_b, op_c, dist="uniform", pad=0):
     return dict(A=A, B=B, C=C, lda=lda, ldb=ldb, ldc=ldc)
 
 
+def make_inputs_with_ld(rng, m, n, k, op_a, op_b, op_c, lda, ldb, ldc, dist="uniform"):
+    """make_inputs with explicit leading dimensions."""
+    na = max(1, stored_shape(op_a, m, k, lda))
+    nb = max(1, stored_shape(op_b, k, n, ldb))
+    nc = max(1, stored_shape(op_c, m, n, ldc))
+    A = rng.uniform(-1, 1, na).astype(np.float32)
+    B = rng.uniform(-1, 1, nb).astype(np.float16)
+    C = rng.uniform(-1, 1, nc).astype(np.float32)
+    return dict(A=A, B=B, C=C, lda=lda, ldb=ldb, ldc=ldc)
+
+
 def run_gpu(h, tc, op_a, op_b, m, n, k, alpha, inp, beta, op_c, hs=False):
     """Calls shgemm (or hsgemm with hs=True) on the GPU; returns the C buffer as numpy."""
     import torch

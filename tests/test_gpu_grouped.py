@@ -1,0 +1,153 @@
+"""Grouped launches (many uneven problems, one persistent kernel) and their CUDA-graph
+replay with new tables. The reference has no grouped path; its equivalent is a host
+loop of shgemm calls, which is what every result here is checked against (through
+the oracle and the single-problem entry point)."""
+import numpy as np
+import pytest
+
+import oracle
+from tests import _cases as K
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def h(cuda_device):
+    import shgemm_b200 as sg
+
+    hd = sg.Handle(0)
+    yield hd
+    hd.close()
+
+
+def _batch(rng, count, op_a, k_max=1500):
+    shapes = []
+    ns = [1, 17, 32, 33, 64, 100, 128, 200, 256, 300]
+    for i in range(count):
+        m = int(rng.integers(1, 700))
+        n = ns[i % len(ns)]
+        k = int(rng.integers(0, k_max)) if i % 7 else 0
+        shapes.append((m, n, k))
+    return shapes
+
+
+def _run_batch(h, shapes, tc, op_a, rng, beta=0.0, stream_capture=False):
+    import torch
+
+    import shgemm_b200 as sg
+
+    inputs, dev, probs = [], [], []
+    for (m, n, k) in shapes:
+        # leading dimensions TMA can address: lda a multiple of 4 floats, ldb of 8 halves
+        lda = ((m if op_a == 0 else k) + 4 + 3) // 4 * 4
+        ldb = (k + 8 + 7) // 8 * 8
+        inp = K.make_inputs_with_ld(rng, m, n, k, op_a, 0, 0, lda, ldb, m + 3)
+        A = torch.from_numpy(inp["A"]).cuda()
+        B = torch.from_numpy(inp["B"].view(np.int16)).cuda().view(torch.float16)
+        C = torch.from_numpy(inp["C"].copy()).cuda()
+        inputs.append(inp)
+        dev.append((A, B, C))
+        probs.append((m, n, k, A, inp["lda"], B, inp["ldb"], C, inp["ldc"], 1.0, beta))
+    return inputs, dev, probs
+
+
+@pytest.mark.parametrize("tc", [oracle.FP16, oracle.TF32])
+@pytest.mark.parametrize("op_a", [0, 1])
+def test_grouped_matches_oracle(h, tc, op_a):
+    import torch
+
+    import shgemm_b200 as sg
+
+    rng = np.random.default_rng(100 + tc * 10 + op_a)
+    shapes = _batch(rng, 24, op_a)
+    inputs, dev, probs = _run_batch(h, shapes, tc, op_a, rng, beta=0.5)
+    sg.shgemm_grouped(h, probs, tc, op_a=op_a)
+    torch.cuda.synchronize()
+    assert h.check_error() == 0
+    for (m, n, k), inp, (_, _, C) in zip(shapes, inputs, dev):
+        gpu_c = C.cpu().numpy()
+        orc = K.run_oracle(tc, op_a, 0, m, n, k, 1.0, inp, 0.5, 0, chunk=0)
+        ref = K.fp64(op_a, 0, m, n, k, 1.0, inp, 0.5, 0)
+        sgc = K.sgemm(op_a, 0, m, n, k, 1.0, inp, 0.5, 0)
+        K.assert_parity(K.parity_report(gpu_c, orc, ref, sgc, m, n, inp["ldc"], 0))
+
+
+def test_grouped_result_same_alone_and_in_the_mix(h):
+    """A problem's result does not depend on the batch it runs in (bit for bit)."""
+    import torch
+
+    import shgemm_b200 as sg
+
+    rng = np.random.default_rng(5)
+    shapes = _batch(rng, 16, 0)
+    inputs, dev, probs = _run_batch(h, shapes, oracle.FP16, 0, rng)
+    sg.shgemm_grouped(h, probs, sg.fp16)
+    torch.cuda.synchronize()
+    mixed = [C.clone() for (_, _, C) in dev]
+    for i, q in enumerate(probs):
+        dev[i][2].zero_()
+        sg.shgemm_grouped(h, [q], sg.fp16)
+        torch.cuda.synchronize()
+        assert torch.equal(dev[i][2], mixed[i]), i
+
+
+def test_grouped_graph_replay_with_new_tables(h):
+    """One captured grouped launch replayed with two different batches."""
+    import torch
+
+    import shgemm_b200 as sg
+
+    rng = np.random.default_rng(9)
+    s = torch.cuda.Stream()
+    h.set_stream(s)
+    try:
+        shapes1 = [(300, 64, 512), (129, 256, 1000), (640, 32, 320), (64, 128, 2048)]
+        in1, dev1, pr1 = _run_batch(h, shapes1, oracle.FP16, 0, rng)
+        # warm-up outside the capture, then capture the same call
+        with torch.cuda.stream(s):
+            sg.shgemm_grouped(h, pr1, sg.fp16)
+        s.synchronize()
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g, stream=s):
+            sg.shgemm_grouped(h, pr1, sg.fp16)
+        for (_, _, C) in dev1:
+            C.zero_()
+        torch.cuda.synchronize()
+        g.replay()
+        torch.cuda.synchronize()
+        for (m, n, k), inp, (_, _, C) in zip(shapes1, in1, dev1):
+            orc = K.run_oracle(oracle.FP16, 0, 0, m, n, k, 1.0, inp, 0.0, 0, chunk=0)
+            ref = K.fp64(0, 0, m, n, k, 1.0, inp, 0.0, 0)
+            sgc = K.sgemm(0, 0, m, n, k, 1.0, inp, 0.0, 0)
+            K.assert_parity(K.parity_report(C.cpu().numpy(), orc, ref, sgc, m, n, inp["ldc"], 0))
+        # a different batch (fewer problems, other sizes and buffers) through the same graph
+        shapes2 = [(500, 200, 700), (77, 17, 1500), (1000, 256, 128)]
+        in2, dev2, pr2 = _run_batch(h, shapes2, oracle.FP16, 0, rng)
+        sg.grouped_update(h, pr2, sg.fp16)
+        g.replay()
+        torch.cuda.synchronize()
+        assert h.check_error() == 0
+        for (m, n, k), inp, (_, _, C) in zip(shapes2, in2, dev2):
+            orc = K.run_oracle(oracle.FP16, 0, 0, m, n, k, 1.0, inp, 0.0, 0, chunk=0)
+            ref = K.fp64(0, 0, m, n, k, 1.0, inp, 0.0, 0)
+            sgc = K.sgemm(0, 0, m, n, k, 1.0, inp, 0.0, 0)
+            K.assert_parity(K.parity_report(C.cpu().numpy(), orc, ref, sgc, m, n, inp["ldc"], 0))
+        del g
+    finally:
+        h.set_stream(torch.cuda.current_stream())
+
+
+def test_grouped_rejects_unsupported(h):
+    import torch
+
+    import shgemm_b200 as sg
+
+    A = torch.zeros(64 * 64 + 8, device="cuda")
+    B = torch.zeros(64 * 64 + 8, device="cuda", dtype=torch.float16)
+    C = torch.zeros(64 * 64, device="cuda")
+    with pytest.raises(sg.ShgemmError) as ei:  # op_b = op_t is not supported by grouped launches
+        sg.shgemm_grouped(h, [(64, 64, 64, A, 64, B, 64, C, 64)], sg.fp16, op_b=sg.op_t)
+    assert ei.value.status == 2
+    with pytest.raises(sg.ShgemmError) as ei:  # lda not 16-byte aligned
+        sg.shgemm_grouped(h, [(61, 64, 64, A, 61, B, 64, C, 64)], sg.fp16)
+    assert ei.value.status == 2
