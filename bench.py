@@ -44,6 +44,11 @@ WORKLOADS = {
     "sketch": dict(m=4096, n=256, k=1 << 20, op_a=1, op_b=0, tc=0, alpha=1.0, beta=0.0, dist="sketch",
                    desc="left sketch Y = Omega^T A, A 2^20 x 4096 FP32 (low rank + noise), Omega 2^20 x 256 "
                         "binary16 N(0,1/256), split-K, fp16 compute", op_c=1, bound="hbm"),
+    # 512 uneven right sketches in one graph-captured grouped launch
+    "grouped": dict(m=0, n=0, k=0, op_a=0, op_b=0, tc=0, alpha=1.0, beta=0.0, dist="grouped", count=512, bound="hbm",
+                    desc="grouped batch of 512 uneven right sketches Y_i = A_i Omega_i, m_i log-U[64,8192], "
+                         "k_i log-U[256,16384], n_i in {32,64,128,256}, A_i rank n_i/2 (sigma_j = j^-1.5) + N(0,1e-4), "
+                         "Omega_i Rademacher/sqrt(n_i), fp16 compute, one CUDA-graph-captured launch"),
 }
 
 
@@ -241,6 +246,171 @@ def run_reference_arm(args, wl):
     return 0
 
 
+def make_grouped_batch(count, dev, seed=0):
+    """Config 4's uneven sketch batch on the device; returns problem tuples and sizes."""
+    import numpy as np
+    import torch
+
+    rng = np.random.default_rng(seed)
+    g = torch.Generator(device=dev)
+    g.manual_seed(seed)
+    ms = np.exp(rng.uniform(np.log(64), np.log(8192), count)).astype(int)
+    ks = np.exp(rng.uniform(np.log(256), np.log(16384), count)).astype(int)
+    ns = rng.choice([32, 64, 128, 256], count)
+    probs, shapes, keep = [], [], []
+    for m, k, n in zip(ms, ks, ns):
+        m, k, n = int(m), int(k), int(n)
+        lda = (m + 3) // 4 * 4
+        ldb = (k + 7) // 8 * 8
+        r = max(1, n // 2)
+        # A = U diag(sigma) V^T + N(0, 1e-4): rank n/2, sigma_j = j^-1.5
+        U = torch.randn(m, r, device=dev, generator=g) / np.sqrt(m)
+        V = torch.randn(k, r, device=dev, generator=g) / np.sqrt(k)
+        sig = torch.arange(1, r + 1, device=dev, dtype=torch.float32).pow(-1.5)
+        Afull = torch.empty(k, lda, device=dev)  # column-major m x k with leading dimension lda
+        Afull[:, :m] = ((U * sig) @ V.T).T
+        Afull[:, :m].add_(torch.randn(k, m, device=dev, generator=g), alpha=1e-2)
+        Om = torch.empty(n, ldb, device=dev, dtype=torch.float16)  # column-major k x n, ld = ldb
+        Om[:, :k] = ((torch.randint(0, 2, (n, k), device=dev, generator=g) * 2 - 1).float() / np.sqrt(n)).half()
+        Y = torch.zeros(n, m, device=dev)
+        A = Afull.reshape(-1)
+        B = Om.reshape(-1)
+        C = Y.reshape(-1)
+        keep.append((A, B, C))
+        probs.append((m, n, k, A, lda, B, ldb, C, m, 1.0, 0.0))
+        shapes.append((m, n, k))
+    return probs, shapes, keep
+
+
+def run_grouped(args, wl):
+    import numpy as np
+    import torch
+
+    import shgemm_b200 as sg
+    from shgemm_b200 import evaluation as ev
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    dev = torch.device(f"cuda:{local}")
+    torch.cuda.set_device(dev)
+    h = sg.Handle(local)
+    stream = torch.cuda.Stream(dev)
+    h.set_stream(stream)
+    probs, shapes, keep = make_grouped_batch(wl["count"], dev, seed=rank)
+    torch.cuda.synchronize(dev)
+    flops = sum(2.0 * m * n * k for (m, n, k) in shapes)
+    bytes_min = sum(4.0 * m * k + 2.0 * k * n + 4.0 * m * n for (m, n, k) in shapes)
+
+    # capture the grouped launch once, replay it per step
+    with torch.cuda.stream(stream):
+        sg.shgemm_grouped(h, probs, wl["tc"])
+    stream.synchronize()
+    graph = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(graph, stream=stream):
+        sg.shgemm_grouped(h, probs, wl["tc"])
+    for _ in range(args.warmup):
+        graph.replay()
+    torch.cuda.synchronize(dev)
+    if dist:
+        dist.barrier()
+    launches0 = h.launch_count()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        e0.record(stream)
+        for _ in range(args.steps):
+            graph.replay()
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+    # graph replays do not pass through the library's counter: one grouped kernel per replay
+    launches = args.steps
+    t = torch.tensor([e0.elapsed_time(e1)], device=dev, dtype=torch.float64)
+    if dist:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_step = float(t.item()) / args.steps
+    value = world * flops / (ms_step * 1e-3) / 1e12
+    assert h.check_error() == 0
+
+    # the per-call baseline: one shgemm launch per problem, same stream
+    def per_call():
+        for (m, n, k, A, lda, B, ldb, C, ldc, al, be) in probs:
+            sg.shgemm(h, 0, 0, m, n, k, al, A, lda, B, ldb, be, C, ldc, wl["tc"])
+
+    with torch.cuda.stream(stream):
+        per_call()
+        stream.synchronize()
+        p0 = torch.cuda.Event(enable_timing=True)
+        p1 = torch.cuda.Event(enable_timing=True)
+        steps_pc = max(1, min(args.steps, 5))
+        p0.record(stream)
+        for _ in range(steps_pc):
+            per_call()
+        p1.record(stream)
+    torch.cuda.synchronize(dev)
+    ms_pc = p0.elapsed_time(p1) / steps_pc
+    per_call_tflops = flops / (ms_pc * 1e-3) / 1e12
+
+    # error on a sample of problems vs the FP64 product
+    graph.replay()
+    torch.cuda.synchronize(dev)
+    errs = []
+    for i in range(0, len(probs), max(1, len(probs) // 16)):
+        m, n, k, A, lda, B, ldb, C, ldc, al, be = probs[i]
+        c64 = ev.fp64_product(h, 0, 0, m, n, k, A, lda, B, ldb)
+        errs.append(ev.error(h, m, n, C, ldc, c64)["rel_fro"])
+        Bf = B.view(n, ldb)[:, :k].float()
+        Af = A.view(k, lda)[:, :m].T
+        S = (Af @ Bf.T).T.contiguous().reshape(-1)  # n x m row-major == m x n column-major
+        errs[-1] = (errs[-1], ev.error(h, m, n, S, m, c64)["rel_fro"])
+    del graph
+
+    peaks, peak_kind = load_peaks()
+    peak = peaks.get("hbm_gbs", 6650.0)
+    achieved = bytes_min / (ms_step * 1e-3) / 1e9
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        cpu = cpu_baseline(dict(wl, k=4096, tc=wl["tc"]))
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "TFLOP/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32 split to fp16 (tensor) / f32 accumulate",
+            "data": "synthetic (seeded, config 4 shapes and distributions)",
+            "config": {"workload": wl["desc"], "problems": len(probs), "total_flops_2mnk": flops,
+                       "algorithmic_bytes": bytes_min, "l2": "inputs exceed L2 (no flush needed)",
+                       "parallelism": f"replicas x{world}"},
+            "per_call_baseline": {"value": per_call_tflops, "unit": "TFLOP/s", "ms_per_step": ms_pc,
+                                  "launches_per_step": len(probs),
+                                  "what": "the same problems as one shgemm call (one launch) each"},
+            "speedup_vs_per_call": value / world / per_call_tflops,
+            "issued_tflops": 2 * value,
+            "gpu_launches": launches,
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                         "traffic": None, "peak_kind": f"{peak_kind} HBM copy bandwidth",
+                         "work_per_launch": f"sum over problems of A + Omega + Y = {bytes_min:.4e} bytes"},
+            "clocks": clk.summary(),
+            "error": {"sample_rel_err_fp64": [e[0] for e in errs], "sample_sgemm_rel_err_fp64": [e[1] for e in errs],
+                      "max_rel_err_fp64": max(e[0] for e in errs)},
+            "e2e": None,
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    h.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -259,6 +429,8 @@ def main():
     args.warmup = max(3, args.warmup)
     if args.impl == "reference":
         return run_reference_arm(args, wl)
+    if wl["dist"] == "grouped":
+        return run_grouped(args, wl)
 
     import torch
 

@@ -99,7 +99,7 @@ struct TileCfg {
     static constexpr int HALF_N = BN / 2;                        // columns per epilogue warp
     // Per-thread registers after setmaxnreg: warpgroups 0-1 (producer, MMA, split) and
     // 2-3 (epilogue, which holds HALF_N running sums); 256 x (SPLIT_REGS + EPI_REGS) = 65536.
-    static constexpr int SPLIT_REGS = BN == 256 ? 80 : 112;
+    static constexpr int SPLIT_REGS = BN == 256 ? 72 : 112;
     static constexpr int EPI_REGS = 256 - SPLIT_REGS;
     static constexpr int BAR_BYTES = 1024;
     static constexpr int SMEM_BYTES = SA * A_STAGE + SB * B_STAGE + BAR_BYTES + 1024;
@@ -737,11 +737,13 @@ __device__ __forceinline__ void tile_kernel_body(const Params& p) {
         const uint32_t lane_addr = static_cast<uint32_t>(q * 32) << 16;
         uint32_t gc = 0;
         for (int u = blockIdx.x; u < num_units; u += gridDim.x) {
-            UnitDesc ud;
-            get_unit<Cfg>(p, u, ud);
-            const int tm = ud.tm, tn = ud.tn, s0 = ud.s0, s1 = ud.s1;
-            const int nsteps = s1 - s0;
-            const int hn = ud.bn / 2;  // columns of this warp's half (<= HN)
+            int nsteps, hn;
+            {
+                UnitDesc ud;
+                get_unit<Cfg>(p, u, ud);
+                nsteps = ud.s1 - ud.s0;
+                hn = ud.bn / 2;  // columns of this warp's half (<= HN)
+            }
             uint64_t acc2[HN / 2];  // running sums, packed in pairs of columns
 #pragma unroll
             for (int j = 0; j < HN / 2; ++j) acc2[j] = 0ull;
@@ -775,6 +777,10 @@ __device__ __forceinline__ void tile_kernel_body(const Params& p) {
             }
             {
                 auto acc = [&](int j) -> float { return (j & 1) ? ptx::f2_hi(acc2[j >> 1]) : ptx::f2_lo(acc2[j >> 1]); };
+                // the unit's output fields, read again here so they are not live during the drain
+                UnitDesc ud;
+                get_unit<Cfg>(p, u, ud);
+                const int tm = ud.tm, tn = ud.tn;
                 const int row = tm * Cfg::BM + row_in_tile;
                 const int col0 = tn * ud.bn + half * hn;
                 if (row < ud.m) {

@@ -81,11 +81,12 @@ def test_grouped_result_same_alone_and_in_the_mix(h):
     rng = np.random.default_rng(5)
     shapes = _batch(rng, 16, 0)
     inputs, dev, probs = _run_batch(h, shapes, oracle.FP16, 0, rng)
+    initial = [C.clone() for (_, _, C) in dev]
     sg.shgemm_grouped(h, probs, sg.fp16)
     torch.cuda.synchronize()
     mixed = [C.clone() for (_, _, C) in dev]
     for i, q in enumerate(probs):
-        dev[i][2].zero_()
+        dev[i][2].copy_(initial[i])
         sg.shgemm_grouped(h, [q], sg.fp16)
         torch.cuda.synchronize()
         assert torch.equal(dev[i][2], mixed[i]), i
