@@ -317,15 +317,15 @@ def run_grouped(args, wl):
     graph = torch.cuda.CUDAGraph()
     with torch.cuda.graph(graph, stream=stream):
         sg.shgemm_grouped(h, probs, wl["tc"])
-    for _ in range(args.warmup):
-        graph.replay()
+    with torch.cuda.stream(stream):  # replays run on the current stream
+        for _ in range(args.warmup):
+            graph.replay()
     torch.cuda.synchronize(dev)
     if dist:
         dist.barrier()
-    launches0 = h.launch_count()
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
-    with ClockSampler(local) as clk:
+    with ClockSampler(local) as clk, torch.cuda.stream(stream):
         e0.record(stream)
         for _ in range(args.steps):
             graph.replay()
@@ -359,18 +359,24 @@ def run_grouped(args, wl):
     ms_pc = p0.elapsed_time(p1) / steps_pc
     per_call_tflops = flops / (ms_pc * 1e-3) / 1e12
 
-    # error on a sample of problems vs the FP64 product
-    graph.replay()
+    # error on a sample of problems vs the FP64 product (outputs of a graph replay)
+    for (_, _, C) in keep:
+        C.zero_()
+    with torch.cuda.stream(stream):
+        graph.replay()
     torch.cuda.synchronize(dev)
     errs = []
-    for i in range(0, len(probs), max(1, len(probs) // 16)):
-        m, n, k, A, lda, B, ldb, C, ldc, al, be = probs[i]
-        c64 = ev.fp64_product(h, 0, 0, m, n, k, A, lda, B, ldb)
-        errs.append(ev.error(h, m, n, C, ldc, c64)["rel_fro"])
-        Bf = B.view(n, ldb)[:, :k].float()
-        Af = A.view(k, lda)[:, :m].T
-        S = (Af @ Bf.T).T.contiguous().reshape(-1)  # n x m row-major == m x n column-major
-        errs[-1] = (errs[-1], ev.error(h, m, n, S, m, c64)["rel_fro"])
+    torch.backends.cuda.matmul.allow_tf32 = False
+    with torch.cuda.stream(stream):  # the library's error kernels run on the handle's stream
+        for i in range(0, len(probs), max(1, len(probs) // 16)):
+            m, n, k, A, lda, B, ldb, C, ldc, al, be = probs[i]
+            c64 = ev.fp64_product(h, 0, 0, m, n, k, A, lda, B, ldb)
+            e_sh = ev.error(h, m, n, C, ldc, c64)["rel_fro"]
+            Bf = B.view(n, ldb)[:, :k].float()
+            Af = A.view(k, lda)[:, :m].T
+            S = (Af @ Bf.T).T.contiguous().reshape(-1)  # n x m row-major == m x n column-major
+            errs.append((e_sh, ev.error(h, m, n, S, m, c64)["rel_fro"]))
+    torch.cuda.synchronize(dev)
     del graph
 
     peaks, peak_kind = load_peaks()

@@ -113,7 +113,8 @@ int shgemm_b200_shgemm_grouped(shgemm_b200_handle_t handle, int op_a, int op_b, 
 
 /* Rewrites the pinned host staging with a new batch without enqueueing anything
  * (for replaying a captured grouped launch). The batch must use the op_a,
- * compute type and op_c the launch was captured with. */
+ * compute type and op_c the launch was captured with, and no replay of that
+ * launch may still be pending (its copy reads the staging): synchronise first. */
 int shgemm_b200_grouped_update(shgemm_b200_handle_t handle, int op_a, int op_b, int compute_type, int op_c,
                                const shgemm_b200_problem* problems, int count);
 

@@ -84,8 +84,12 @@ struct TileCfg {
     static constexpr int HI_BYTES = BM * 128;  // BM rows of 128 bytes (both modes)
     static constexpr int A_STAGE = 2 * HI_BYTES;  // raw FP32 tile, then hi + lo tiles
     static constexpr int B_STAGE = BN * 128;      // binary16 tile; TF32: widened tile
-    // MN-major hi/lo tiles (binary16, M-contiguous A): 64-wide m atoms of BK k rows.
-    static constexpr int MN_ATOM_BYTES = BK * 128;
+    // binary16 compute: the split runs on 16 independent items per stage (8 rows x 64 k
+    // of a K-major tile, or 8 k x 64 m of an M-major one), each converted in place by one warp.
+    static constexpr int SPLIT_ITEMS = 16;
+    // M-major raw A (binary16 compute): two [BK][64 m] boxes; hi/lo atoms of item
+    // (k group g, m half h) at h * MN_HALF_BYTES + g * 2048 (+1024 for lo).
+    static constexpr int MN_HALF_BYTES = BK * 64 * 4;
     static constexpr int SMEM_BUDGET = 224 * 1024;
     static constexpr int SA = 4;
     static constexpr int SB_FIT = (SMEM_BUDGET - SA * A_STAGE) / B_STAGE;
@@ -253,185 +257,211 @@ __device__ __forceinline__ void split4_tf32(const float4 x, float4& hi, float4& 
     lo.w = ptx::to_tf32_rna(ptx::f2_hi(d1));
 }
 
-// One k-step of the split warps (thread sidx of SPLIT_THREADS), in place:
+// binary16 compute: one split item, converted in place by one warp.
+// K-major A (item = rows 8i .. 8i+7): the raw tile is two [128 rows][32 floats] 128B-swizzled
+// sub-tiles (k 0-31, 32-63); hi row r replaces raw row r of the first, lo row r that of the
+// second, both [64 halves] K-major with a 128-byte swizzle.
+// M-major A (item = k group g = i & 7 of m half h = i >> 3): the raw tile is two [64 k][64 m]
+// boxes (256-byte rows); the item's 8 raw rows (2 KB) become its hi atom (8 k x 64 m halves,
+// 128B swizzle) and, 1 KB above it, its lo atom.
+// Lane l covers output chunks (16 bytes, 8 values) chosen so that each group of 8 lanes
+// touches 8 distinct 16-byte bank groups on every load and store.
+template <class Cfg, bool A_KMAJOR>
+__device__ __forceinline__ void split_item_load(const uint8_t* st, int item, int lane, float4 (&x)[4]) {
+    if constexpr (A_KMAJOR) {
+        const int row = item * 8 + (lane & 7), cb = lane >> 3, sw = lane & 7;
+        const uint8_t* r0 = st + row * 128;
+        const uint8_t* r1 = r0 + Cfg::BM * 128;
+        x[0] = *reinterpret_cast<const float4*>(r0 + (((2 * cb) ^ sw) << 4));
+        x[1] = *reinterpret_cast<const float4*>(r0 + (((2 * cb + 1) ^ sw) << 4));
+        x[2] = *reinterpret_cast<const float4*>(r1 + (((2 * cb) ^ sw) << 4));
+        x[3] = *reinterpret_cast<const float4*>(r1 + (((2 * cb + 1) ^ sw) << 4));
+    } else {
+        const uint8_t* base = st + (item >> 3) * Cfg::MN_HALF_BYTES + (item & 7) * 2048;
+        const int c = lane & 7, first = (c >> 2) & 1;
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const uint8_t* rp = base + ((lane >> 3) + 4 * h) * 256 + c * 32;
+            const float4 xa = *reinterpret_cast<const float4*>(rp + 16 * first);
+            const float4 xb = *reinterpret_cast<const float4*>(rp + 16 * (1 - first));
+            x[2 * h] = first ? xb : xa;
+            x[2 * h + 1] = first ? xa : xb;
+        }
+    }
+}
+
+template <class Cfg, bool A_KMAJOR>
+__device__ __forceinline__ void split_item_store(uint8_t* st, int item, int lane, const float4 (&x)[4]) {
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+        const float v[8] = {x[2 * h].x, x[2 * h].y, x[2 * h].z, x[2 * h].w,
+                            x[2 * h + 1].x, x[2 * h + 1].y, x[2 * h + 1].z, x[2 * h + 1].w};
+        uint4 hv, lv;
+        split8_f16(v, hv, lv);
+        uint8_t* hp;
+        uint8_t* lp;
+        if constexpr (A_KMAJOR) {
+            const int row = item * 8 + (lane & 7), c = (lane >> 3) + 4 * h, sw = lane & 7;
+            hp = st + row * 128 + ((c ^ sw) << 4);
+            lp = hp + Cfg::BM * 128;
+        } else {
+            const int r = (lane >> 3) + 4 * h, c = lane & 7;
+            hp = st + (item >> 3) * Cfg::MN_HALF_BYTES + (item & 7) * 2048 + r * 128 + ((c ^ r) << 4);
+            lp = hp + 1024;
+        }
+        *reinterpret_cast<uint4*>(hp) = hv;
+        *reinterpret_cast<uint4*>(lp) = lv;
+    }
+}
+
+// The items i = first, first + SPLIT_WARPS, ... of one stage (binary16 compute). An item's
+// outputs overwrite only its own raw bytes, so a warp needs no other warp to have read the
+// stage: __syncwarp orders its lanes' loads before their stores. The next item's loads are
+// issued before the current item's conversion.
+template <class Cfg, bool A_KMAJOR>
+__device__ __forceinline__ void split_stage_f16(uint8_t* st, int first, int lane) {
+    float4 cur[4];
+    split_item_load<Cfg, A_KMAJOR>(st, first, lane, cur);
+    for (int it = first; it < Cfg::SPLIT_ITEMS; it += Cfg::SPLIT_WARPS) {
+        float4 nxt[4];
+        const bool more = it + Cfg::SPLIT_WARPS < Cfg::SPLIT_ITEMS;
+        if (more) split_item_load<Cfg, A_KMAJOR>(st, it + Cfg::SPLIT_WARPS, lane, nxt);
+        __syncwarp();
+        split_item_store<Cfg, A_KMAJOR>(st, it, lane, cur);
+        if (more) {
+#pragma unroll
+            for (int e = 0; e < 4; ++e) cur[e] = nxt[e];
+        }
+    }
+}
+
+// TF32 compute: one k-step of the split warps (thread sidx of SPLIT_THREADS), in place:
 // phase 1 reads this thread's share of the raw tiles into registers;
 // `all_read()` returns once every split thread has done so (false on timeout);
 // phase 2 converts and overwrites the stages with the UMMA tiles:
 //   A stage: hi at [0, HI_BYTES), lo at [HI_BYTES, 2 HI_BYTES)
-//   B stage (TF32 only): the widened [BN][32] TF32 tile.
+//   B stage: the widened [BN][32] TF32 tile.
 template <class Cfg, bool A_KMAJOR, bool B_KMAJOR, class AllRead>
-__device__ __forceinline__ bool split_step(uint8_t* a_st, uint8_t* b_st, int sidx, AllRead&& all_read) {
+__device__ __forceinline__ bool split_step_tf32(uint8_t* a_st, uint8_t* b_st, int sidx, AllRead&& all_read) {
     constexpr int NT = Cfg::SPLIT_THREADS;
     uint8_t* hi_t = a_st;
     uint8_t* lo_t = a_st + Cfg::HI_BYTES;
-    if constexpr (!Cfg::kTf32) {
-        constexpr int U = (1024 + NT - 1) / NT;  // units of 8 values per thread
-        float4 x[U][2];
+    constexpr int BN = Cfg::BN;
+    // ---- phase 1: A
+    constexpr int UA = A_KMAJOR ? (1024 + NT - 1) / NT : (256 + NT - 1) / NT;
+    float4 xa[UA][A_KMAJOR ? 1 : 4];
 #pragma unroll
-        for (int j = 0; j < U; ++j) {
-            const int u = sidx + j * NT;
+    for (int j = 0; j < UA; ++j) {
+        const int u = sidx + j * NT;
+        if constexpr (A_KMAJOR) {
+            // raw: [128 rows][32 floats] 128B-swizzled. Unit: (row, 16-byte chunk c).
             if (u < 1024) {
-                if constexpr (A_KMAJOR) {
-                    // raw: two [128 rows][32 floats] 128B-swizzled sub-tiles (k 0-31, 32-63).
-                    // Unit: (row, 16-byte output chunk c).
-                    const int row = u & 127, c = u >> 7, sw = row & 7, j0 = (c & 3) * 2;
-                    const uint8_t* rp = a_st + (c >> 2) * (Cfg::BM * 128) + row * 128;
-                    x[j][0] = *reinterpret_cast<const float4*>(rp + ((j0 ^ sw) << 4));
-                    x[j][1] = *reinterpret_cast<const float4*>(rp + (((j0 + 1) ^ sw) << 4));
-                } else {
-                    // raw: [64 k][128 m] floats (512-byte rows). Unit: (k, group g of 8
-                    // consecutive m); the read order keeps 8-thread phases conflict-free.
-                    const int g = u & 15, k = u >> 4, first = (g >> 2) & 1;
-                    const uint8_t* rp = a_st + k * 512 + g * 32;
-                    const float4 xa = *reinterpret_cast<const float4*>(rp + 16 * first);
-                    const float4 xb = *reinterpret_cast<const float4*>(rp + 16 * (1 - first));
-                    x[j][0] = first ? xb : xa;
-                    x[j][1] = first ? xa : xb;
-                }
+                const int row = u & 127, c = u >> 7;
+                xa[j][0] = *reinterpret_cast<const float4*>(a_st + row * 128 + ((c ^ (row & 7)) << 4));
+            }
+        } else {
+            // raw: [32 k][128 m] floats. Unit: (m group g of 4, k group kq of 4).
+            if (u < 256) {
+                const int g = u & 31, kq = u >> 5;
+#pragma unroll
+                for (int r = 0; r < 4; ++r)
+                    xa[j][r] = *reinterpret_cast<const float4*>(a_st + (kq * 4 + r) * 512 + g * 16);
             }
         }
-        if (!all_read()) return false;
-#pragma unroll
-        for (int j = 0; j < U; ++j) {
-            const int u = sidx + j * NT;
-            if (u < 1024) {
-                const float v[8] = {x[j][0].x, x[j][0].y, x[j][0].z, x[j][0].w,
-                                    x[j][1].x, x[j][1].y, x[j][1].z, x[j][1].w};
-                uint4 h, l;
-                split8_f16(v, h, l);
-                int off;
-                if constexpr (A_KMAJOR) {
-                    // out: [128 rows][64 halves] K-major, 128B swizzle
-                    const int row = u & 127, c = u >> 7;
-                    off = row * 128 + ((c ^ (row & 7)) << 4);
-                } else {
-                    // out: MN-major, two atoms of [64 k rows][64 m halves], 128B swizzle
-                    const int g = u & 15, k = u >> 4;
-                    off = (g >> 3) * Cfg::MN_ATOM_BYTES + k * 128 + (((g & 7) ^ (k & 7)) << 4);
-                }
-                *reinterpret_cast<uint4*>(hi_t + off) = h;
-                *reinterpret_cast<uint4*>(lo_t + off) = l;
-            }
-        }
-        return true;
-    } else {
-        constexpr int BN = Cfg::BN;
-        // ---- phase 1: A
-        constexpr int UA = A_KMAJOR ? (1024 + NT - 1) / NT : (256 + NT - 1) / NT;
-        float4 xa[UA][A_KMAJOR ? 1 : 4];
-#pragma unroll
-        for (int j = 0; j < UA; ++j) {
-            const int u = sidx + j * NT;
-            if constexpr (A_KMAJOR) {
-                // raw: [128 rows][32 floats] 128B-swizzled. Unit: (row, 16-byte chunk c).
-                if (u < 1024) {
-                    const int row = u & 127, c = u >> 7;
-                    xa[j][0] = *reinterpret_cast<const float4*>(a_st + row * 128 + ((c ^ (row & 7)) << 4));
-                }
-            } else {
-                // raw: [32 k][128 m] floats. Unit: (m group g of 4, k group kq of 4).
-                if (u < 256) {
-                    const int g = u & 31, kq = u >> 5;
-#pragma unroll
-                    for (int r = 0; r < 4; ++r)
-                        xa[j][r] = *reinterpret_cast<const float4*>(a_st + (kq * 4 + r) * 512 + g * 16);
-                }
-            }
-        }
-        // ---- phase 1: B (binary16, exact in TF32)
-        constexpr int UB = B_KMAJOR ? (BN * 4 + NT - 1) / NT : (BN * 8 + NT - 1) / NT;
-        uint4 xb_k[B_KMAJOR ? UB : 1];
-        uint2 xb_m[B_KMAJOR ? 1 : UB];
-#pragma unroll
-        for (int j = 0; j < UB; ++j) {
-            const int u = sidx + j * NT;
-            if constexpr (B_KMAJOR) {
-                // raw: [BN][32] binary16, 64-byte rows, 64B swizzle. Unit: (row n, raw chunk rc).
-                if (u < BN * 4) {
-                    const int n = u % BN, rc = u / BN;
-                    xb_k[j] = *reinterpret_cast<const uint4*>(b_st + n * 64 + ((rc ^ ((n >> 1) & 3)) << 4));
-                }
-            } else {
-                // raw: [32 k][BN] binary16. Unit: (column n, output chunk c = k 4c .. 4c+3).
-                if (u < BN * 8) {
-                    const int n = u % BN, c = u / BN;
-                    const uint16_t* bh = reinterpret_cast<const uint16_t*>(b_st);
-                    xb_m[j].x = uint32_t(bh[(c * 4 + 0) * BN + n]) | (uint32_t(bh[(c * 4 + 1) * BN + n]) << 16);
-                    xb_m[j].y = uint32_t(bh[(c * 4 + 2) * BN + n]) | (uint32_t(bh[(c * 4 + 3) * BN + n]) << 16);
-                }
-            }
-        }
-        if (!all_read()) return false;
-        // ---- phase 2: A -> hi/lo [128 rows][32] TF32, K-major, 128B swizzle
-#pragma unroll
-        for (int j = 0; j < UA; ++j) {
-            const int u = sidx + j * NT;
-            if constexpr (A_KMAJOR) {
-                if (u < 1024) {
-                    const int row = u & 127, c = u >> 7;
-                    const int off = row * 128 + ((c ^ (row & 7)) << 4);
-                    float4 h, l;
-                    split4_tf32(xa[j][0], h, l);
-                    *reinterpret_cast<float4*>(hi_t + off) = h;
-                    *reinterpret_cast<float4*>(lo_t + off) = l;
-                }
-            } else {
-                if (u < 256) {
-                    const int g = u & 31, kq = u >> 5;
-                    float4 h[4], l[4];  // h[r]: k = 4kq + r, m = 4g .. 4g+3
-#pragma unroll
-                    for (int r = 0; r < 4; ++r) split4_tf32(xa[j][r], h[r], l[r]);
-                    // transpose 4 x 4; rotate the row order so 8-thread store phases
-                    // hit distinct 16-byte bank groups
-#pragma unroll
-                    for (int r = 0; r < 4; ++r) {
-                        const int rr = (r + (g >> 1)) & 3;
-                        const int row = 4 * g + rr;
-                        const float4 hv = rr == 0   ? make_float4(h[0].x, h[1].x, h[2].x, h[3].x)
-                                          : rr == 1 ? make_float4(h[0].y, h[1].y, h[2].y, h[3].y)
-                                          : rr == 2 ? make_float4(h[0].z, h[1].z, h[2].z, h[3].z)
-                                                    : make_float4(h[0].w, h[1].w, h[2].w, h[3].w);
-                        const float4 lv = rr == 0   ? make_float4(l[0].x, l[1].x, l[2].x, l[3].x)
-                                          : rr == 1 ? make_float4(l[0].y, l[1].y, l[2].y, l[3].y)
-                                          : rr == 2 ? make_float4(l[0].z, l[1].z, l[2].z, l[3].z)
-                                                    : make_float4(l[0].w, l[1].w, l[2].w, l[3].w);
-                        const int off = row * 128 + ((kq ^ (row & 7)) << 4);
-                        *reinterpret_cast<float4*>(hi_t + off) = hv;
-                        *reinterpret_cast<float4*>(lo_t + off) = lv;
-                    }
-                }
-            }
-        }
-        // ---- phase 2: B -> [BN][32] TF32, K-major, 128B swizzle
-#pragma unroll
-        for (int j = 0; j < UB; ++j) {
-            const int u = sidx + j * NT;
-            if constexpr (B_KMAJOR) {
-                if (u < BN * 4) {
-                    const int n = u % BN, rc = u / BN, sw = n & 7;
-                    const __half2* hp = reinterpret_cast<const __half2*>(&xb_k[j]);
-                    const float2 f0 = __half22float2(hp[0]);
-                    const float2 f1 = __half22float2(hp[1]);
-                    const float2 f2 = __half22float2(hp[2]);
-                    const float2 f3 = __half22float2(hp[3]);
-                    *reinterpret_cast<float4*>(b_st + n * 128 + (((2 * rc) ^ sw) << 4)) =
-                        make_float4(f0.x, f0.y, f1.x, f1.y);
-                    *reinterpret_cast<float4*>(b_st + n * 128 + (((2 * rc + 1) ^ sw) << 4)) =
-                        make_float4(f2.x, f2.y, f3.x, f3.y);
-                }
-            } else {
-                if (u < BN * 8) {
-                    const int n = u % BN, c = u / BN;
-                    const __half2* hp = reinterpret_cast<const __half2*>(&xb_m[j]);
-                    const float2 f0 = __half22float2(hp[0]);
-                    const float2 f1 = __half22float2(hp[1]);
-                    *reinterpret_cast<float4*>(b_st + n * 128 + ((c ^ (n & 7)) << 4)) =
-                        make_float4(f0.x, f0.y, f1.x, f1.y);
-                }
-            }
-        }
-        return true;
     }
+    // ---- phase 1: B (binary16, exact in TF32)
+    constexpr int UB = B_KMAJOR ? (BN * 4 + NT - 1) / NT : (BN * 8 + NT - 1) / NT;
+    uint4 xb_k[B_KMAJOR ? UB : 1];
+    uint2 xb_m[B_KMAJOR ? 1 : UB];
+#pragma unroll
+    for (int j = 0; j < UB; ++j) {
+        const int u = sidx + j * NT;
+        if constexpr (B_KMAJOR) {
+            // raw: [BN][32] binary16, 64-byte rows, 64B swizzle. Unit: (row n, raw chunk rc).
+            if (u < BN * 4) {
+                const int n = u % BN, rc = u / BN;
+                xb_k[j] = *reinterpret_cast<const uint4*>(b_st + n * 64 + ((rc ^ ((n >> 1) & 3)) << 4));
+            }
+        } else {
+            // raw: [32 k][BN] binary16. Unit: (column n, output chunk c = k 4c .. 4c+3).
+            if (u < BN * 8) {
+                const int n = u % BN, c = u / BN;
+                const uint16_t* bh = reinterpret_cast<const uint16_t*>(b_st);
+                xb_m[j].x = uint32_t(bh[(c * 4 + 0) * BN + n]) | (uint32_t(bh[(c * 4 + 1) * BN + n]) << 16);
+                xb_m[j].y = uint32_t(bh[(c * 4 + 2) * BN + n]) | (uint32_t(bh[(c * 4 + 3) * BN + n]) << 16);
+            }
+        }
+    }
+    if (!all_read()) return false;
+    // ---- phase 2: A -> hi/lo [128 rows][32] TF32, K-major, 128B swizzle
+#pragma unroll
+    for (int j = 0; j < UA; ++j) {
+        const int u = sidx + j * NT;
+        if constexpr (A_KMAJOR) {
+            if (u < 1024) {
+                const int row = u & 127, c = u >> 7;
+                const int off = row * 128 + ((c ^ (row & 7)) << 4);
+                float4 h, l;
+                split4_tf32(xa[j][0], h, l);
+                *reinterpret_cast<float4*>(hi_t + off) = h;
+                *reinterpret_cast<float4*>(lo_t + off) = l;
+            }
+        } else {
+            if (u < 256) {
+                const int g = u & 31, kq = u >> 5;
+                float4 h[4], l[4];  // h[r]: k = 4kq + r, m = 4g .. 4g+3
+#pragma unroll
+                for (int r = 0; r < 4; ++r) split4_tf32(xa[j][r], h[r], l[r]);
+                // transpose 4 x 4; rotate the row order so 8-thread store phases
+                // hit distinct 16-byte bank groups
+#pragma unroll
+                for (int r = 0; r < 4; ++r) {
+                    const int rr = (r + (g >> 1)) & 3;
+                    const int row = 4 * g + rr;
+                    const float4 hv = rr == 0   ? make_float4(h[0].x, h[1].x, h[2].x, h[3].x)
+                                      : rr == 1 ? make_float4(h[0].y, h[1].y, h[2].y, h[3].y)
+                                      : rr == 2 ? make_float4(h[0].z, h[1].z, h[2].z, h[3].z)
+                                                : make_float4(h[0].w, h[1].w, h[2].w, h[3].w);
+                    const float4 lv = rr == 0   ? make_float4(l[0].x, l[1].x, l[2].x, l[3].x)
+                                      : rr == 1 ? make_float4(l[0].y, l[1].y, l[2].y, l[3].y)
+                                      : rr == 2 ? make_float4(l[0].z, l[1].z, l[2].z, l[3].z)
+                                                : make_float4(l[0].w, l[1].w, l[2].w, l[3].w);
+                    const int off = row * 128 + ((kq ^ (row & 7)) << 4);
+                    *reinterpret_cast<float4*>(hi_t + off) = hv;
+                    *reinterpret_cast<float4*>(lo_t + off) = lv;
+                }
+            }
+        }
+    }
+    // ---- phase 2: B -> [BN][32] TF32, K-major, 128B swizzle
+#pragma unroll
+    for (int j = 0; j < UB; ++j) {
+        const int u = sidx + j * NT;
+        if constexpr (B_KMAJOR) {
+            if (u < BN * 4) {
+                const int n = u % BN, rc = u / BN, sw = n & 7;
+                const __half2* hp = reinterpret_cast<const __half2*>(&xb_k[j]);
+                const float2 f0 = __half22float2(hp[0]);
+                const float2 f1 = __half22float2(hp[1]);
+                const float2 f2 = __half22float2(hp[2]);
+                const float2 f3 = __half22float2(hp[3]);
+                *reinterpret_cast<float4*>(b_st + n * 128 + (((2 * rc) ^ sw) << 4)) =
+                    make_float4(f0.x, f0.y, f1.x, f1.y);
+                *reinterpret_cast<float4*>(b_st + n * 128 + (((2 * rc + 1) ^ sw) << 4)) =
+                    make_float4(f2.x, f2.y, f3.x, f3.y);
+            }
+        } else {
+            if (u < BN * 8) {
+                const int n = u % BN, c = u / BN;
+                const __half2* hp = reinterpret_cast<const __half2*>(&xb_m[j]);
+                const float2 f0 = __half22float2(hp[0]);
+                const float2 f1 = __half22float2(hp[1]);
+                *reinterpret_cast<float4*>(b_st + n * 128 + ((c ^ (n & 7)) << 4)) =
+                    make_float4(f0.x, f0.y, f1.x, f1.y);
+            }
+        }
+    }
+    return true;
 }
 
 template <int TC, int BN, bool A_KMAJOR, bool B_KMAJOR, class Params>
@@ -450,7 +480,7 @@ __device__ __forceinline__ void tile_kernel_body(const Params& p) {
     uint8_t* b_base = a_base + SA * Cfg::A_STAGE;
     uint64_t* bars = reinterpret_cast<uint64_t*>(b_base + SB * Cfg::B_STAGE);
     uint64_t* a_full = bars;           // TMA landed the raw A tile
-    uint64_t* a_read = a_full + SA;    // every split warp holds its share in registers
+    uint64_t* a_read = a_full + SA;    // TF32: every split warp holds its share in registers
     uint64_t* a_split = a_read + SA;   // hi/lo tiles written (and, for TF32, B widened)
     uint64_t* a_empty = a_split + SA;  // MMAs reading the stage completed
     uint64_t* b_full = a_empty + SA;
@@ -531,6 +561,11 @@ __device__ __forceinline__ void tile_kernel_body(const Params& p) {
                             for (int sub = 0; sub < Cfg::BK / 32; ++sub)
                                 ptx::tma_load_2d(a_dst + sub * (Cfg::BM * 128), ud.tmap_a, &a_full[as],
                                                  kc + 32 * sub, tm * Cfg::BM);
+                        } else if constexpr (!kTf32) {
+#pragma unroll
+                            for (int h = 0; h < 2; ++h)
+                                ptx::tma_load_2d(a_dst + h * Cfg::MN_HALF_BYTES, ud.tmap_a, &a_full[as],
+                                                 tm * Cfg::BM + 64 * h, kc);
                         } else {
                             ptx::tma_load_2d(a_dst, ud.tmap_a, &a_full[as], tm * Cfg::BM, kc);
                         }
@@ -615,15 +650,16 @@ __device__ __forceinline__ void tile_kernel_body(const Params& p) {
                     {
                         const uint32_t d = tmem_base + db * BN;
                         const uint32_t hi_s = ptx::smem_u32(a_base + as * Cfg::A_STAGE);
-                        const uint32_t lo_s = hi_s + Cfg::HI_BYTES;
+                        const uint32_t lo_s = hi_s + ((A_KMAJOR || kTf32) ? Cfg::HI_BYTES : 1024);
                         const uint32_t b_s = ptx::smem_u32(b_base + bs * Cfg::B_STAGE);
                         auto a_desc = [&](uint32_t base, int kk) -> uint64_t {
                             if constexpr (A_KMAJOR || kTf32) {
                                 return ptx::make_smem_desc(base + kk * 32, 16, 1024, ptx::kLayoutSW128);
                             } else {
-                                // MN-major: 64-wide m atoms MN_ATOM_BYTES apart, 8-row k groups 1024
-                                // bytes apart; one UMMA_K = 16 step is 16 rows of 128 bytes.
-                                return ptx::make_smem_desc(base + kk * 2048, Cfg::MN_ATOM_BYTES, 1024,
+                                // MN-major: 64-wide m atoms MN_HALF_BYTES apart, 8-row k groups 2048
+                                // bytes apart (hi and lo atoms interleaved); one UMMA_K = 16 step is
+                                // two k groups.
+                                return ptx::make_smem_desc(base + kk * 4096, Cfg::MN_HALF_BYTES, 2048,
                                                            ptx::kLayoutSW128);
                             }
                         };
@@ -688,6 +724,9 @@ __device__ __forceinline__ void tile_kernel_body(const Params& p) {
         const int sidx = (warp - 2) * 32 + lane;
         int as = 0, bs = 0;
         uint32_t aph = 0, bph = 0;
+        // binary16: global item g of this CTA's item sequence goes to split warp g % SPLIT_WARPS;
+        // `first` is this warp's first item of the current stage.
+        int first = warp - 2;
         for (int u = blockIdx.x; u < num_units; u += gridDim.x) {
             UnitDesc ud;
             get_unit<Cfg>(p, u, ud);
@@ -697,14 +736,18 @@ __device__ __forceinline__ void tile_kernel_body(const Params& p) {
                     fail(kErrSplitTimeout);
                     goto split_done;
                 }
-                {
+                if constexpr (!kTf32) {
+                    split_stage_f16<Cfg, A_KMAJOR>(a_base + as * Cfg::A_STAGE, first, lane);
+                    first -= Cfg::SPLIT_ITEMS % NSPLIT;
+                    if (first < 0) first += NSPLIT;
+                } else {
                     auto all_read = [&]() -> bool {
                         __syncwarp();
                         if (lane == 0) ptx::mbar_arrive(&a_read[as]);
                         return ptx::mbar_wait(&a_read[as], aph, abort_flag, limit);
                     };
-                    if (!split_step<Cfg, A_KMAJOR, B_KMAJOR>(a_base + as * Cfg::A_STAGE, b_base + bs * Cfg::B_STAGE,
-                                                              sidx, all_read)) {
+                    if (!split_step_tf32<Cfg, A_KMAJOR, B_KMAJOR>(a_base + as * Cfg::A_STAGE,
+                                                                   b_base + bs * Cfg::B_STAGE, sidx, all_read)) {
                         fail(kErrSplitTimeout);
                         goto split_done;
                     }

@@ -77,6 +77,10 @@ bool make_tmap(CUtensorMap* map, CUtensorMapDataType dtype, const void* base, ui
     return r == CUDA_SUCCESS;
 }
 
+// Width (m) of one TMA box of an M-major FP32 operand: the binary16 kernels load a 128-row
+// tile as two 64-wide boxes (one per half of the split's items), the TF32 kernels as one.
+constexpr uint32_t a_mmajor_box(int tc) { return tc == kFP16 ? 64 : 128; }
+
 using TileKernelFn = void (*)(TileGemmParams);
 
 template <int TC, int BN, bool AK, bool BK>
@@ -580,12 +584,12 @@ static int run_tiled(shgemm_b200_handle_t h, int op_a, int op_b, size_t m, size_
     std::memset(&P, 0, sizeof(P));
     bool ok;
     // FP32 operand: K-major tiles are [128 rows][32 floats] with a 128-byte swizzle;
-    // M-major tiles are [bk][128 floats] unswizzled.
+    // M-major tiles are [bk][a_mmajor_box(tc) floats] unswizzled.
     if (a_kmajor)
         ok = make_tmap(&P.tmap_a, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, a, k, m, lda * 4, 32, 128,
                        CU_TENSOR_MAP_SWIZZLE_128B);
     else
-        ok = make_tmap(&P.tmap_a, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, a, m, k, lda * 4, 128, bk,
+        ok = make_tmap(&P.tmap_a, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, a, m, k, lda * 4, a_mmajor_box(tc), bk,
                        CU_TENSOR_MAP_SWIZZLE_NONE);
     if (!ok) return SHGEMM_STATUS_NOT_SUPPORTED;
     if (tc == kFP16) {
@@ -848,11 +852,15 @@ int grouped_stage(shgemm_b200_handle_t h, int op_a, int op_b, int tc, int op_c, 
         (tc != kFP16 && tc != kTF32))
         return op_b == kOpT ? SHGEMM_STATUS_NOT_SUPPORTED : SHGEMM_STATUS_INVALID_VALUE;
     if (count > kGroupedMaxProblems) return SHGEMM_STATUS_NOT_SUPPORTED;
-    // The staging buffer may still be the source of a pending copy: wait for it.
+    // The staging buffer may still be the source of a pending eager copy: wait for it
+    // (not while capturing, where host waits are illegal; copies replayed from a
+    // captured graph are the caller's to wait for).
     cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
-    cudaStreamIsCapturing(h->stream, &cap);
-    if (cap == cudaStreamCaptureStatusNone && cudaEventSynchronize(h->grouped_copied) != cudaSuccess)
+    if (cudaStreamIsCapturing(h->stream, &cap) != cudaSuccess) cap = cudaStreamCaptureStatusNone;
+    if (cap == cudaStreamCaptureStatusNone && cudaEventSynchronize(h->grouped_copied) != cudaSuccess) {
+        cudaGetLastError();
         return SHGEMM_STATUS_CUDA_ERROR;
+    }
     auto* host = static_cast<uint8_t*>(h->grouped_host);
     auto* gp = reinterpret_cast<GroupedProblem*>(host);
     auto* units = reinterpret_cast<int2*>(host + kGroupedUnitsOff);
@@ -884,7 +892,7 @@ int grouped_stage(shgemm_b200_handle_t h, int op_a, int op_b, int tc, int op_c, 
             bool ok = op_a == kOpT ? make_tmap(&g.tmap_a, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, q.a, q.k, q.m, q.lda * 4, 32,
                                                128, CU_TENSOR_MAP_SWIZZLE_128B)
                                    : make_tmap(&g.tmap_a, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, q.a, q.m, q.k, q.lda * 4,
-                                               128, bk, CU_TENSOR_MAP_SWIZZLE_NONE);
+                                               a_mmajor_box(tc), bk, CU_TENSOR_MAP_SWIZZLE_NONE);
             ok = ok && (tc == kFP16 ? make_tmap(&g.tmap_b, CU_TENSOR_MAP_DATA_TYPE_FLOAT16, q.b, q.k, q.n, q.ldb * 2,
                                                 64, bn, CU_TENSOR_MAP_SWIZZLE_128B)
                                     : make_tmap(&g.tmap_b, CU_TENSOR_MAP_DATA_TYPE_FLOAT16, q.b, q.k, q.n, q.ldb * 2,
@@ -953,7 +961,9 @@ int shgemm_b200_shgemm_grouped(shgemm_b200_handle_t h, int op_a, int op_b, int c
             cudaSuccess)
         return SHGEMM_STATUS_CUDA_ERROR;
     h->grouped_copied_count = count;
-    cudaEventRecord(h->grouped_copied, h->stream);
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    cudaStreamIsCapturing(h->stream, &cap);
+    if (cap == cudaStreamCaptureStatusNone) cudaEventRecord(h->grouped_copied, h->stream);
     GroupedParams P;
     std::memset(&P, 0, sizeof(P));
     P.problems = static_cast<const GroupedProblem*>(h->grouped_dev);

@@ -114,7 +114,8 @@ def test_grouped_graph_replay_with_new_tables(h):
         for (_, _, C) in dev1:
             C.zero_()
         torch.cuda.synchronize()
-        g.replay()
+        with torch.cuda.stream(s):
+            g.replay()
         torch.cuda.synchronize()
         for (m, n, k), inp, (_, _, C) in zip(shapes1, in1, dev1):
             orc = K.run_oracle(oracle.FP16, 0, 0, m, n, k, 1.0, inp, 0.0, 0, chunk=0)
@@ -125,7 +126,8 @@ def test_grouped_graph_replay_with_new_tables(h):
         shapes2 = [(500, 200, 700), (77, 17, 1500), (1000, 256, 128)]
         in2, dev2, pr2 = _run_batch(h, shapes2, oracle.FP16, 0, rng)
         sg.grouped_update(h, pr2, sg.fp16)
-        g.replay()
+        with torch.cuda.stream(s):
+            g.replay()
         torch.cuda.synchronize()
         assert h.check_error() == 0
         for (m, n, k), inp, (_, _, C) in zip(shapes2, in2, dev2):
