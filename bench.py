@@ -49,6 +49,11 @@ WORKLOADS = {
                     desc="grouped batch of 512 uneven right sketches Y_i = A_i Omega_i, m_i log-U[64,8192], "
                          "k_i log-U[256,16384], n_i in {32,64,128,256}, A_i rank n_i/2 (sigma_j = j^-1.5) + N(0,1e-4), "
                          "Omega_i Rademacher/sqrt(n_i), fp16 compute, one CUDA-graph-captured launch"),
+    # the same batch in TF32 compute, Omega_i handed over widened to FP32 (as the sketch server keeps it)
+    "grouped_tf32": dict(m=0, n=0, k=0, op_a=0, op_b=0, tc=1, alpha=1.0, beta=0.0, dist="grouped", count=512,
+                         bound="hbm", b_fp32=True,
+                         desc="grouped batch of 512 uneven right sketches (shapes as the fp16 batch), tf32 compute, "
+                              "Omega_i widened to FP32 once, one CUDA-graph-captured launch"),
 }
 
 
@@ -308,15 +313,27 @@ def run_grouped(args, wl):
     probs, shapes, keep = make_grouped_batch(wl["count"], dev, seed=rank)
     torch.cuda.synchronize(dev)
     flops = sum(2.0 * m * n * k for (m, n, k) in shapes)
-    bytes_min = sum(4.0 * m * k + 2.0 * k * n + 4.0 * m * n for (m, n, k) in shapes)
+    b_bytes = 4.0 if wl.get("b_fp32") else 2.0
+    bytes_min = sum(4.0 * m * k + b_bytes * k * n + 4.0 * m * n for (m, n, k) in shapes)
+    gprobs, keep_w = probs, []
+    if wl.get("b_fp32"):
+        # Omega_i widened to FP32 once (exact: binary16 values), K-major with a 16-byte ld
+        gprobs = []
+        for (m, n, k, A, lda, B, ldb, C, ldc, al, be) in probs:
+            ldb4 = (k + 3) // 4 * 4
+            Bw = torch.zeros(n, ldb4, device=dev)
+            Bw[:, :k] = B.view(n, ldb)[:, :k].float()
+            keep_w.append(Bw)
+            gprobs.append((m, n, k, A, lda, Bw.reshape(-1), ldb4, C, ldc, al, be))
+        h.set_config(sg.CFG_GROUPED_B_FP32, 1)
 
     # capture the grouped launch once, replay it per step
     with torch.cuda.stream(stream):
-        sg.shgemm_grouped(h, probs, wl["tc"])
+        sg.shgemm_grouped(h, gprobs, wl["tc"])
     stream.synchronize()
     graph = torch.cuda.CUDAGraph()
     with torch.cuda.graph(graph, stream=stream):
-        sg.shgemm_grouped(h, probs, wl["tc"])
+        sg.shgemm_grouped(h, gprobs, wl["tc"])
     with torch.cuda.stream(stream):  # replays run on the current stream
         for _ in range(args.warmup):
             graph.replay()
@@ -389,7 +406,8 @@ def run_grouped(args, wl):
         line = {
             "metric": METRIC, "value": value, "unit": "TFLOP/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f32 split to fp16 (tensor) / f32 accumulate",
+            "vs_baseline": None, "dtype": "f32 split to fp16 (tensor) / f32 accumulate" if wl["tc"] == 0
+            else "f32 split to tf32 (tensor) / f32 accumulate",
             "data": "synthetic (seeded, config 4 shapes and distributions)",
             "config": {"workload": wl["desc"], "problems": len(probs), "total_flops_2mnk": flops,
                        "algorithmic_bytes": bytes_min, "l2": "inputs exceed L2 (no flush needed)",

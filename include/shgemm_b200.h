@@ -45,7 +45,10 @@ enum {
 enum {
     SHGEMM_CFG_SPLIT_K = 2,       /* 0 = automatic, 1 = never split, s > 1 = force s slices */
     SHGEMM_CFG_WAIT_LIMIT_MS = 3, /* bound on every in-kernel wait (default 2000 ms) */
-    SHGEMM_CFG_GROUP_M = 4        /* tile rasterisation group along m (default 8) */
+    SHGEMM_CFG_GROUP_M = 4,       /* tile rasterisation group along m (default 8) */
+    SHGEMM_CFG_GROUPED_B_FP32 = 5 /* 1: grouped TF32 batches pass B as FP32 values that are
+                                     exactly binary16 (a widened copy), loaded without a
+                                     conversion; 0 (default): B is binary16 */
 };
 
 /* mtk::shgemm::create (include/shgemm/shgemm.hpp:94; src/shgemm.cu:401-490).

@@ -71,25 +71,34 @@ struct alignas(64) TileGemmParams {
     int group_m;          // rasterisation group along m
 };
 
-template <int TC, int BN_, bool A_KMAJOR, bool B_KMAJOR>
+// B_WIDE (TF32 compute only): the binary16 operand arrives already widened to FP32
+// (K-major), so it is loaded straight into the TF32 tile layout and the split warps
+// handle the FP32 operand alone.
+template <int TC, int BN_, bool A_KMAJOR, bool B_KMAJOR, bool B_WIDE = false>
 struct TileCfg {
     static constexpr int BM = 128;
     static constexpr int BN = BN_;
     static constexpr bool kTf32 = (TC == kTF32);
+    static constexpr bool kBWide = B_WIDE;
+    // split warps work on independent items, each converted in place by one warp
+    static constexpr bool kItemSplit = !kTf32 || kBWide;
     static constexpr int BK = kTf32 ? 32 : 64;  // one 128-byte swizzle row of the compute type
     static constexpr int UMMA_K = kTf32 ? 8 : 16;
     static constexpr int KSUB = BK / UMMA_K;  // UMMAs per operand per k-step
     static constexpr int A_RAW = BM * BK * 4;
-    static constexpr int B_RAW = BN * BK * 2;
+    static constexpr int B_RAW = BN * BK * (kBWide ? 4 : 2);
     static constexpr int HI_BYTES = BM * 128;  // BM rows of 128 bytes (both modes)
     static constexpr int A_STAGE = 2 * HI_BYTES;  // raw FP32 tile, then hi + lo tiles
     static constexpr int B_STAGE = BN * 128;      // binary16 tile; TF32: widened tile
-    // binary16 compute: the split runs on 16 independent items per stage (8 rows x 64 k
-    // of a K-major tile, or 8 k x 64 m of an M-major one), each converted in place by one warp.
-    static constexpr int SPLIT_ITEMS = 16;
+    // Split items per stage. binary16: 8 rows x 64 k of a K-major tile, or 8 k x 64 m of an
+    // M-major one. TF32 (B_WIDE): 8 rows x 32 k of a K-major tile, or one [32 k][32 m] box of
+    // an M-major one.
+    static constexpr int SPLIT_ITEMS = (kTf32 && !A_KMAJOR) ? 4 : 16;
     // M-major raw A (binary16 compute): two [BK][64 m] boxes; hi/lo atoms of item
     // (k group g, m half h) at h * MN_HALF_BYTES + g * 2048 (+1024 for lo).
     static constexpr int MN_HALF_BYTES = BK * 64 * 4;
+    // M-major raw A (TF32, B_WIDE): four [32 k][32 m] boxes of MN_BOX_BYTES.
+    static constexpr int MN_BOX_BYTES = BK * 32 * 4;
     static constexpr int SMEM_BUDGET = 224 * 1024;
     static constexpr int SA = 4;
     static constexpr int SB_FIT = (SMEM_BUDGET - SA * A_STAGE) / B_STAGE;
@@ -107,7 +116,8 @@ struct TileCfg {
     static constexpr int EPI_REGS = 256 - SPLIT_REGS;
     static constexpr int BAR_BYTES = 1024;
     static constexpr int SMEM_BYTES = SA * A_STAGE + SB * B_STAGE + BAR_BYTES + 1024;
-    static_assert(BN == 64 || BN == 128 || (BN == 256 && !kTf32), "tile N");
+    static_assert(BN == 64 || BN == 128 || (BN == 256 && (!kTf32 || kBWide)), "tile N");
+    static_assert(!kBWide || (kTf32 && B_KMAJOR), "widened B: TF32 compute, K-major");
     static_assert(A_STAGE % 1024 == 0 && B_STAGE % 1024 == 0 && A_RAW <= A_STAGE, "1024B-aligned stages");
     static_assert(SMEM_BYTES <= 232448, "dynamic shared memory limit");
 };
@@ -335,6 +345,46 @@ __device__ __forceinline__ void split_stage_f16(uint8_t* st, int first, int lane
     }
 }
 
+// TF32 compute with a widened B: the items of one stage.
+// K-major A (item = rows 8i .. 8i+7 of the [128 rows][32 floats] 128B-swizzled raw tile):
+// each lane converts two 16-byte chunks in place (hi) and writes lo at the same offset
+// HI_BYTES above; no lane reads what another writes.
+// M-major A (item = box i, [32 k][32 m] floats with 128-byte rows at i * MN_BOX_BYTES):
+// lane l gathers column m = 32 i + l, then (after __syncwarp) writes hi row m over the
+// box, [32 TF32] K-major with a 128-byte swizzle, and lo row m HI_BYTES above.
+template <class Cfg, bool A_KMAJOR>
+__device__ __forceinline__ void split_stage_tf32w(uint8_t* st, int first, int lane) {
+    for (int it = first; it < Cfg::SPLIT_ITEMS; it += Cfg::SPLIT_WARPS) {
+        if constexpr (A_KMAJOR) {
+            const int row = it * 8 + (lane & 7), sw = lane & 7;
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                uint8_t* p = st + row * 128 + ((((lane >> 3) + 4 * h) ^ sw) << 4);
+                float4 hv, lv;
+                split4_tf32(*reinterpret_cast<const float4*>(p), hv, lv);
+                *reinterpret_cast<float4*>(p) = hv;
+                *reinterpret_cast<float4*>(p + Cfg::HI_BYTES) = lv;
+            }
+        } else {
+            uint8_t* box = st + it * Cfg::MN_BOX_BYTES;
+            float v[32];
+#pragma unroll
+            for (int k = 0; k < 32; ++k) v[k] = *reinterpret_cast<const float*>(box + k * 128 + lane * 4);
+            __syncwarp();
+            const int m = it * 32 + lane;
+            uint8_t* hp = st + m * 128;
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+                float4 hv, lv;
+                split4_tf32(make_float4(v[4 * j], v[4 * j + 1], v[4 * j + 2], v[4 * j + 3]), hv, lv);
+                const int off = (j ^ (m & 7)) << 4;
+                *reinterpret_cast<float4*>(hp + off) = hv;
+                *reinterpret_cast<float4*>(hp + Cfg::HI_BYTES + off) = lv;
+            }
+        }
+    }
+}
+
 // TF32 compute: one k-step of the split warps (thread sidx of SPLIT_THREADS), in place:
 // phase 1 reads this thread's share of the raw tiles into registers;
 // `all_read()` returns once every split thread has done so (false on timeout);
@@ -464,9 +514,9 @@ __device__ __forceinline__ bool split_step_tf32(uint8_t* a_st, uint8_t* b_st, in
     return true;
 }
 
-template <int TC, int BN, bool A_KMAJOR, bool B_KMAJOR, class Params>
+template <int TC, int BN, bool A_KMAJOR, bool B_KMAJOR, bool B_WIDE, class Params>
 __device__ __forceinline__ void tile_kernel_body(const Params& p) {
-    using Cfg = TileCfg<TC, BN, A_KMAJOR, B_KMAJOR>;
+    using Cfg = TileCfg<TC, BN, A_KMAJOR, B_KMAJOR, B_WIDE>;
     constexpr int SA = Cfg::SA;
     constexpr int SB = Cfg::SB;
     constexpr bool kTf32 = Cfg::kTf32;
@@ -566,6 +616,11 @@ __device__ __forceinline__ void tile_kernel_body(const Params& p) {
                             for (int h = 0; h < 2; ++h)
                                 ptx::tma_load_2d(a_dst + h * Cfg::MN_HALF_BYTES, ud.tmap_a, &a_full[as],
                                                  tm * Cfg::BM + 64 * h, kc);
+                        } else if constexpr (B_WIDE) {
+#pragma unroll
+                            for (int b = 0; b < 4; ++b)
+                                ptx::tma_load_2d(a_dst + b * Cfg::MN_BOX_BYTES, ud.tmap_a, &a_full[as],
+                                                 tm * Cfg::BM + 32 * b, kc);
                         } else {
                             ptx::tma_load_2d(a_dst, ud.tmap_a, &a_full[as], tm * Cfg::BM, kc);
                         }
@@ -582,7 +637,7 @@ __device__ __forceinline__ void tile_kernel_body(const Params& p) {
                     }
                     {
                         uint8_t* b_dst = b_base + bs * Cfg::B_STAGE;
-                        ptx::mbar_arrive_expect_tx(&b_full[bs], ud.bn * Cfg::BK * 2);
+                        ptx::mbar_arrive_expect_tx(&b_full[bs], ud.bn * Cfg::BK * (B_WIDE ? 4 : 2));
                         if constexpr (B_KMAJOR) {
                             ptx::tma_load_2d(b_dst, ud.tmap_b, &b_full[bs], kc, tn * ud.bn);
                         } else if constexpr (!kTf32) {
@@ -636,7 +691,7 @@ __device__ __forceinline__ void tile_kernel_body(const Params& p) {
                         fail(kErrMmaTimeout);
                         goto mma_done;
                     }
-                    if constexpr (!kTf32) {
+                    if constexpr (!kTf32 || B_WIDE) {
                         if (!ptx::mbar_wait(&b_full[bs], bph, abort_flag, limit)) {
                             fail(kErrMmaTimeout);
                             goto mma_done;
@@ -732,12 +787,15 @@ __device__ __forceinline__ void tile_kernel_body(const Params& p) {
             get_unit<Cfg>(p, u, ud);
             for (int st = ud.s0; st < ud.s1; ++st) {
                 if (!ptx::mbar_wait(&a_full[as], aph, abort_flag, limit) ||
-                    (kTf32 && !ptx::mbar_wait(&b_full[bs], bph, abort_flag, limit))) {
+                    (kTf32 && !B_WIDE && !ptx::mbar_wait(&b_full[bs], bph, abort_flag, limit))) {
                     fail(kErrSplitTimeout);
                     goto split_done;
                 }
-                if constexpr (!kTf32) {
-                    split_stage_f16<Cfg, A_KMAJOR>(a_base + as * Cfg::A_STAGE, first, lane);
+                if constexpr (Cfg::kItemSplit) {
+                    if constexpr (kTf32)
+                        split_stage_tf32w<Cfg, A_KMAJOR>(a_base + as * Cfg::A_STAGE, first, lane);
+                    else
+                        split_stage_f16<Cfg, A_KMAJOR>(a_base + as * Cfg::A_STAGE, first, lane);
                     first -= Cfg::SPLIT_ITEMS % NSPLIT;
                     if (first < 0) first += NSPLIT;
                 } else {
@@ -760,7 +818,7 @@ __device__ __forceinline__ void tile_kernel_body(const Params& p) {
                     as = 0;
                     aph ^= 1u;
                 }
-                if constexpr (kTf32) {
+                if constexpr (kTf32 && !B_WIDE) {
                     if (++bs == SB) {
                         bs = 0;
                         bph ^= 1u;
@@ -874,13 +932,13 @@ __device__ __forceinline__ void tile_kernel_body(const Params& p) {
 // Single problem (optionally split-K): descriptors in the kernel's parameter space.
 template <int TC, int BN, bool A_KMAJOR, bool B_KMAJOR>
 __global__ void __launch_bounds__(512, 1) shgemm_tile_kernel(const __grid_constant__ TileGemmParams p) {
-    tile_kernel_body<TC, BN, A_KMAJOR, B_KMAJOR>(p);
+    tile_kernel_body<TC, BN, A_KMAJOR, B_KMAJOR, false>(p);
 }
 
 // Many problems in one launch: per-problem descriptors and a unit list in device memory.
-template <int TC, int BN, bool A_KMAJOR, bool B_KMAJOR>
+template <int TC, int BN, bool A_KMAJOR, bool B_KMAJOR, bool B_WIDE>
 __global__ void __launch_bounds__(512, 1) shgemm_grouped_kernel(const __grid_constant__ GroupedParams p) {
-    tile_kernel_body<TC, BN, A_KMAJOR, B_KMAJOR>(p);
+    tile_kernel_body<TC, BN, A_KMAJOR, B_KMAJOR, B_WIDE>(p);
 }
 
 }  // namespace shgemm_b200

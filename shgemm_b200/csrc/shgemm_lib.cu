@@ -37,7 +37,8 @@ struct shgemm_b200_handle {
     void* grouped_dev = nullptr;
     void* grouped_host = nullptr;
     cudaEvent_t grouped_copied = nullptr;
-    int grouped_tc = -1, grouped_op_a = -1, grouped_op_b = -1, grouped_op_c = -1;
+    int grouped_tc = -1, grouped_op_a = -1, grouped_op_b = -1, grouped_op_c = -1, grouped_b32 = -1;
+    int grouped_b_fp32 = 0;  // SHGEMM_CFG_GROUPED_B_FP32
     int grouped_units = 0;
     int grouped_copied_count = 0;  // problem slots the last enqueued copy covers
 };
@@ -78,8 +79,9 @@ bool make_tmap(CUtensorMap* map, CUtensorMapDataType dtype, const void* base, ui
 }
 
 // Width (m) of one TMA box of an M-major FP32 operand: the binary16 kernels load a 128-row
-// tile as two 64-wide boxes (one per half of the split's items), the TF32 kernels as one.
-constexpr uint32_t a_mmajor_box(int tc) { return tc == kFP16 ? 64 : 128; }
+// tile as two 64-wide boxes (one per half of the split's items), the TF32 kernels with a
+// widened B as four 32-wide boxes (one per item), the other TF32 kernels as one.
+constexpr uint32_t a_mmajor_box(int tc, bool b_wide = false) { return tc == kFP16 ? 64 : (b_wide ? 32 : 128); }
 
 using TileKernelFn = void (*)(TileGemmParams);
 
@@ -110,19 +112,22 @@ KernelEntry kernel_table(int tc, int bn, int ak, int bk) {
     return {nullptr, 0};
 }
 
-template <int TC, int BN, bool AK>
-void* grouped_kernel_ptr() {
-    return reinterpret_cast<void*>(&shgemm_grouped_kernel<TC, BN, AK, true>);
+template <int TC, int BN, bool AK, bool BW>
+KernelEntry grouped_entry() {
+    return {reinterpret_cast<void*>(&shgemm_grouped_kernel<TC, BN, AK, true, BW>),
+            TileCfg<TC, BN, AK, true, BW>::SMEM_BYTES};
 }
 
-// Grouped kernels: binary16 compute with tile N up to 256, TF32 up to 128; B K-major.
-constexpr int kGroupedMaxBnF16 = 256, kGroupedMaxBnTf32 = 128;
-KernelEntry grouped_table(int tc, int ak) {
-    if (tc == kFP16)
-        return ak ? KernelEntry{grouped_kernel_ptr<kFP16, kGroupedMaxBnF16, true>(), tile_smem<kFP16, kGroupedMaxBnF16, true, true>()}
-                  : KernelEntry{grouped_kernel_ptr<kFP16, kGroupedMaxBnF16, false>(), tile_smem<kFP16, kGroupedMaxBnF16, false, true>()};
-    return ak ? KernelEntry{grouped_kernel_ptr<kTF32, kGroupedMaxBnTf32, true>(), tile_smem<kTF32, kGroupedMaxBnTf32, true, true>()}
-              : KernelEntry{grouped_kernel_ptr<kTF32, kGroupedMaxBnTf32, false>(), tile_smem<kTF32, kGroupedMaxBnTf32, false, true>()};
+// Grouped kernels (B K-major): binary16 compute with tile N up to 256; TF32 up to 128 with
+// a binary16 B, up to 256 with a widened (FP32) B.
+constexpr int kGroupedMaxBnF16 = 256, kGroupedMaxBnTf32 = 128, kGroupedMaxBnTf32Wide = 256;
+KernelEntry grouped_table(int tc, int ak, bool b_wide) {
+    if (tc == kFP16) return ak ? grouped_entry<kFP16, kGroupedMaxBnF16, true, false>()
+                               : grouped_entry<kFP16, kGroupedMaxBnF16, false, false>();
+    if (b_wide) return ak ? grouped_entry<kTF32, kGroupedMaxBnTf32Wide, true, true>()
+                          : grouped_entry<kTF32, kGroupedMaxBnTf32Wide, false, true>();
+    return ak ? grouped_entry<kTF32, kGroupedMaxBnTf32, true, false>()
+              : grouped_entry<kTF32, kGroupedMaxBnTf32, false, false>();
 }
 
 // Table layout (device copy and host staging): problems, then units, then the unit count.
@@ -443,10 +448,11 @@ int shgemm_b200_create(shgemm_b200_handle_t* out, int device) {
                     }
                 }
     for (int tc = 0; tc < 2; ++tc)
-        for (int ak = 0; ak < 2; ++ak) {
-            KernelEntry e = grouped_table(tc, ak);
-            cudaFuncSetAttribute(e.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, e.smem);
-        }
+        for (int ak = 0; ak < 2; ++ak)
+            for (int bw = 0; bw < 2; ++bw) {
+                KernelEntry e = grouped_table(tc, ak, bw != 0);
+                cudaFuncSetAttribute(e.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, e.smem);
+            }
     if (cudaGetLastError() != cudaSuccess || cudaMalloc(&h->grouped_dev, kGroupedBytes) != cudaSuccess ||
         cudaMallocHost(&h->grouped_host, kGroupedBytes) != cudaSuccess ||
         cudaEventCreateWithFlags(&h->grouped_copied, cudaEventDisableTiming) != cudaSuccess) {
@@ -510,6 +516,10 @@ int shgemm_b200_set_config(shgemm_b200_handle_t h, int key, long long v) {
             if (v < 1 || v > 1024) return SHGEMM_STATUS_INVALID_VALUE;
             h->group_m = v;
             return SHGEMM_STATUS_OK;
+        case SHGEMM_CFG_GROUPED_B_FP32:
+            if (v != 0 && v != 1) return SHGEMM_STATUS_INVALID_VALUE;
+            h->grouped_b_fp32 = static_cast<int>(v);
+            return SHGEMM_STATUS_OK;
         default:
             return SHGEMM_STATUS_INVALID_VALUE;
     }
@@ -521,6 +531,7 @@ int shgemm_b200_get_config(shgemm_b200_handle_t h, int key, long long* v) {
         case SHGEMM_CFG_SPLIT_K: *v = h->split_k; return SHGEMM_STATUS_OK;
         case SHGEMM_CFG_WAIT_LIMIT_MS: *v = h->wait_limit_ms; return SHGEMM_STATUS_OK;
         case SHGEMM_CFG_GROUP_M: *v = h->group_m; return SHGEMM_STATUS_OK;
+        case SHGEMM_CFG_GROUPED_B_FP32: *v = h->grouped_b_fp32; return SHGEMM_STATUS_OK;
         default: return SHGEMM_STATUS_INVALID_VALUE;
     }
 }
@@ -837,8 +848,8 @@ int shgemm_b200_eval_error(shgemm_b200_handle_t h, size_t m, size_t n, const flo
 // Grouped launches: many problems, one persistent kernel.
 namespace {
 
-int grouped_tile_n(int tc, size_t n) {
-    const int cap = tc == kFP16 ? kGroupedMaxBnF16 : kGroupedMaxBnTf32;
+int grouped_tile_n(int tc, bool b_wide, size_t n) {
+    const int cap = tc == kFP16 ? kGroupedMaxBnF16 : (b_wide ? kGroupedMaxBnTf32Wide : kGroupedMaxBnTf32);
     int bn = 32;
     while (bn < cap && static_cast<size_t>(bn) < n) bn *= 2;
     return bn;
@@ -865,6 +876,8 @@ int grouped_stage(shgemm_b200_handle_t h, int op_a, int op_b, int tc, int op_c, 
     auto* gp = reinterpret_cast<GroupedProblem*>(host);
     auto* units = reinterpret_cast<int2*>(host + kGroupedUnitsOff);
     const int bk = tc == kFP16 ? 64 : 32;
+    const bool b_wide = tc == kTF32 && h->grouped_b_fp32 != 0;  // B given as FP32 (exact binary16 values)
+    const size_t b_elem = b_wide ? 4 : 2;
     struct Cost {
         long long cost;
         int2 unit;
@@ -880,23 +893,28 @@ int grouped_stage(shgemm_b200_handle_t h, int op_a, int op_b, int tc, int op_c, 
         if (!q.c || q.ldc < c_rows) return SHGEMM_STATUS_INVALID_VALUE;
         if (q.m >= (1u << 31) || q.n >= (1u << 31) || q.k >= (1u << 31) || (q.m + 127) / 128 > 0xFFFF)
             return SHGEMM_STATUS_NOT_SUPPORTED;
-        const int bn = grouped_tile_n(tc, q.n);
+        const int bn = grouped_tile_n(tc, b_wide, q.n);
         const long long tiles_n = static_cast<long long>((q.n + bn - 1) / bn);
         if (tiles_n > 0x7FFF) return SHGEMM_STATUS_NOT_SUPPORTED;
         if (q.k > 0) {
             if (!q.a || !q.b || q.lda < std::max<size_t>(1, a_rows) || q.ldb < std::max<size_t>(1, b_rows))
                 return SHGEMM_STATUS_INVALID_VALUE;
             if ((reinterpret_cast<uintptr_t>(q.a) & 15) || (reinterpret_cast<uintptr_t>(q.b) & 15) ||
-                (q.lda * 4) % 16 || (q.ldb * 2) % 16)
+                (q.lda * 4) % 16 || (q.ldb * b_elem) % 16)
                 return SHGEMM_STATUS_NOT_SUPPORTED;  // grouped launches take TMA-addressable operands only
             bool ok = op_a == kOpT ? make_tmap(&g.tmap_a, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, q.a, q.k, q.m, q.lda * 4, 32,
                                                128, CU_TENSOR_MAP_SWIZZLE_128B)
                                    : make_tmap(&g.tmap_a, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, q.a, q.m, q.k, q.lda * 4,
-                                               a_mmajor_box(tc), bk, CU_TENSOR_MAP_SWIZZLE_NONE);
-            ok = ok && (tc == kFP16 ? make_tmap(&g.tmap_b, CU_TENSOR_MAP_DATA_TYPE_FLOAT16, q.b, q.k, q.n, q.ldb * 2,
-                                                64, bn, CU_TENSOR_MAP_SWIZZLE_128B)
-                                    : make_tmap(&g.tmap_b, CU_TENSOR_MAP_DATA_TYPE_FLOAT16, q.b, q.k, q.n, q.ldb * 2,
-                                                32, bn, CU_TENSOR_MAP_SWIZZLE_64B));
+                                               a_mmajor_box(tc, b_wide), bk, CU_TENSOR_MAP_SWIZZLE_NONE);
+            if (tc == kFP16)
+                ok = ok && make_tmap(&g.tmap_b, CU_TENSOR_MAP_DATA_TYPE_FLOAT16, q.b, q.k, q.n, q.ldb * 2, 64, bn,
+                                     CU_TENSOR_MAP_SWIZZLE_128B);
+            else if (b_wide)  // [bn][32] FP32 rows of 128 bytes: the TF32 tile layout itself
+                ok = ok && make_tmap(&g.tmap_b, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, q.b, q.k, q.n, q.ldb * 4, 32, bn,
+                                     CU_TENSOR_MAP_SWIZZLE_128B);
+            else
+                ok = ok && make_tmap(&g.tmap_b, CU_TENSOR_MAP_DATA_TYPE_FLOAT16, q.b, q.k, q.n, q.ldb * 2, 32, bn,
+                                     CU_TENSOR_MAP_SWIZZLE_64B);
             if (!ok) return SHGEMM_STATUS_NOT_SUPPORTED;
         }
         g.c = q.c;
@@ -920,6 +938,7 @@ int grouped_stage(shgemm_b200_handle_t h, int op_a, int op_b, int tc, int op_c, 
     for (size_t u = 0; u < list.size(); ++u) units[u] = list[u].unit;
     *reinterpret_cast<int*>(host + kGroupedCountOff) = static_cast<int>(list.size());
     h->grouped_tc = tc;
+    h->grouped_b32 = b_wide ? 1 : 0;
     h->grouped_op_a = op_a;
     h->grouped_op_b = op_b;
     h->grouped_op_c = op_c;
@@ -935,12 +954,13 @@ int shgemm_b200_grouped_update(shgemm_b200_handle_t h, int op_a, int op_b, int c
                                const shgemm_b200_problem* problems, int count) {
     if (!h) return SHGEMM_STATUS_INVALID_VALUE;
     DeviceGuard g(h->device);
-    const int prev_tc = h->grouped_tc, prev_a = h->grouped_op_a, prev_c = h->grouped_op_c;
+    const int prev_tc = h->grouped_tc, prev_a = h->grouped_op_a, prev_c = h->grouped_op_c, prev_b = h->grouped_b32;
     const int st = grouped_stage(h, op_a, op_b, compute_type, op_c, problems, count);
     if (st != SHGEMM_STATUS_OK) return st;
     // A captured launch was built for one kernel variant and copies a fixed number of
     // problem slots: the batch must keep the variant and fit those slots.
-    if (prev_tc >= 0 && (prev_tc != compute_type || prev_a != op_a || prev_c != op_c)) return SHGEMM_STATUS_INVALID_VALUE;
+    if (prev_tc >= 0 && (prev_tc != compute_type || prev_a != op_a || prev_c != op_c || prev_b != h->grouped_b32))
+        return SHGEMM_STATUS_INVALID_VALUE;
     if (count > h->grouped_copied_count) return SHGEMM_STATUS_INVALID_VALUE;
     return SHGEMM_STATUS_OK;
 }
@@ -972,7 +992,7 @@ int shgemm_b200_shgemm_grouped(shgemm_b200_handle_t h, int op_a, int op_b, int c
     P.error_flag = h->error_word;
     P.wait_limit_ns = static_cast<uint64_t>(h->wait_limit_ms) * 1000000ull;
     P.op_c = op_c;
-    const KernelEntry e = grouped_table(compute_type, op_a == kOpT);
+    const KernelEntry e = grouped_table(compute_type, op_a == kOpT, h->grouped_b32 == 1);
     void* args[] = {&P};
     // One CTA per SM whatever the batch: a captured launch stays valid for other batches.
     const cudaError_t err = cudaLaunchKernel(e.fn, dim3(h->num_sms), dim3(512), args, e.smem, h->stream);

@@ -72,6 +72,38 @@ def test_grouped_matches_oracle(h, tc, op_a):
         K.assert_parity(K.parity_report(gpu_c, orc, ref, sgc, m, n, inp["ldc"], 0))
 
 
+@pytest.mark.parametrize("op_a", [0, 1])
+def test_grouped_tf32_widened_b_matches_oracle(h, op_a):
+    """TF32 batches whose B is handed over already widened to FP32 (exact binary16 values)."""
+    import torch
+
+    import shgemm_b200 as sg
+
+    rng = np.random.default_rng(300 + op_a)
+    shapes = _batch(rng, 24, op_a)
+    inputs, dev, probs = _run_batch(h, shapes, oracle.TF32, op_a, rng, beta=0.5)
+    wide = []
+    for (m, n, k, A, lda, B, ldb, C, ldc, al, be) in probs:
+        ldb4 = (k + 3) // 4 * 4 + 4  # a 16-byte multiple of FP32
+        Bw = torch.zeros(max(1, n * ldb4), device=B.device, dtype=torch.float32)
+        if k > 0:
+            Bw.view(n, ldb4)[:, :k] = B.view(n, ldb)[:, :k].float()
+        wide.append((m, n, k, A, lda, Bw, ldb4, C, ldc, al, be))
+    h.set_config(sg.CFG_GROUPED_B_FP32, 1)
+    try:
+        sg.shgemm_grouped(h, wide, sg.tf32, op_a=op_a)
+        torch.cuda.synchronize()
+    finally:
+        h.set_config(sg.CFG_GROUPED_B_FP32, 0)
+    assert h.check_error() == 0
+    for (m, n, k), inp, (_, _, C) in zip(shapes, inputs, dev):
+        gpu_c = C.cpu().numpy()
+        orc = K.run_oracle(oracle.TF32, op_a, 0, m, n, k, 1.0, inp, 0.5, 0, chunk=0)
+        ref = K.fp64(op_a, 0, m, n, k, 1.0, inp, 0.5, 0)
+        sgc = K.sgemm(op_a, 0, m, n, k, 1.0, inp, 0.5, 0)
+        K.assert_parity(K.parity_report(gpu_c, orc, ref, sgc, m, n, inp["ldc"], 0))
+
+
 def test_grouped_result_same_alone_and_in_the_mix(h):
     """A problem's result does not depend on the batch it runs in (bit for bit)."""
     import torch
