@@ -49,6 +49,13 @@ WORKLOADS = {
                     desc="grouped batch of 512 uneven right sketches Y_i = A_i Omega_i, m_i log-U[64,8192], "
                          "k_i log-U[256,16384], n_i in {32,64,128,256}, A_i rank n_i/2 (sigma_j = j^-1.5) + N(0,1e-4), "
                          "Omega_i Rademacher/sqrt(n_i), fp16 compute, one CUDA-graph-captured launch"),
+    # a Poisson stream of sketch requests into the sketch server
+    "served": dict(m=0, n=0, k=0, op_a=0, op_b=0, tc=1, alpha=1.0, beta=0.0, dist="served", bound="tensor",
+                   rate=2000.0, duration=60.0, budget=40 << 30, draws=4, m_min=1024, m_max=65536, k_min=1024,
+                   k_max=16384, ns=(64, 128, 256),
+                   desc="served sketch stream: Poisson arrivals at 2000 req/s, m log-U[1024,65536], "
+                        "k log-U[1024,16384], n in {64,128,256}, 4 Gaussian Omega draws per resident A "
+                        "(rank n, sigma_j = j^-2, + N(0,1e-6)), tf32 compute, 40 GB admission budget"),
     # the same batch in TF32 compute, Omega_i handed over widened to FP32 (as the sketch server keeps it)
     "grouped_tf32": dict(m=0, n=0, k=0, op_a=0, op_b=0, tc=1, alpha=1.0, beta=0.0, dist="grouped", count=512,
                          bound="hbm", b_fp32=True,
@@ -190,7 +197,7 @@ def cpu_baseline(wl, seconds_target=12.0):
     import oracle
 
     rng = np.random.default_rng(0)
-    k = min(wl["k"], 16384)
+    k = min(wl["k"] or 4096, 16384)
     ms = ns = 256
     # grow the sample until it takes a few seconds
     while True:
@@ -221,7 +228,7 @@ def run_reference_arm(args, wl):
     import oracle
 
     rng = np.random.default_rng(0)
-    k = min(wl["k"], 16384)
+    k = min(wl["k"] or 4096, 16384)  # batch / stream workloads: a representative k
     ms = ns = 512
     A = rng.standard_normal(ms * k).astype(np.float32)
     B = rng.standard_normal(k * ns).astype(np.float16)
@@ -435,6 +442,209 @@ def run_grouped(args, wl):
     return 0
 
 
+def make_sketch_pools(wl, dev, seed):
+    """One device-resident A per n: m_max x k_max column-major (lda = m_max), rank n with
+    sigma_j = j^-2, plus N(0, 1e-6) noise. A request's A is an m x k window of the pool of
+    its n (a window of a rank-n matrix has rank <= n), so the stream needs no per-request
+    generation; each request is still charged its own A bytes by the server's admission."""
+    import numpy as np
+    import torch
+
+    M, Kx = wl["m_max"], wl["k_max"]
+    pools = {}
+    torch.backends.cuda.matmul.allow_tf32 = False
+    for n in wl["ns"]:
+        g = torch.Generator(device=dev)
+        g.manual_seed(seed * 1000 + n)
+        U = torch.randn(M, n, device=dev, generator=g) / np.sqrt(M)
+        V = torch.randn(Kx, n, device=dev, generator=g) / np.sqrt(Kx)
+        sig = torch.arange(1, n + 1, device=dev, dtype=torch.float32).pow(-2.0)
+        T = torch.empty(Kx, M, device=dev)  # row j of T = column j of A
+        torch.matmul(V * sig, U.T, out=T)
+        for c in range(0, Kx, 1024):
+            T[c:c + 1024].add_(torch.randn(min(1024, Kx - c), M, device=dev, generator=g), alpha=1e-3)
+        del U, V
+        pools[n] = T
+    torch.cuda.synchronize(dev)
+    return pools
+
+
+def sketch_requests(wl, pools, seed, count):
+    """Seeded request shapes and A windows: (m, n, k, A address, lda, omega seed)."""
+    import numpy as np
+
+    rng = np.random.default_rng(seed)
+    M, Kx = wl["m_max"], wl["k_max"]
+    out = []
+    for i in range(count):
+        m = int(np.exp(rng.uniform(np.log(wl["m_min"]), np.log(M))))
+        k = int(np.exp(rng.uniform(np.log(wl["k_min"]), np.log(Kx))))
+        n = int(rng.choice(wl["ns"]))
+        r0 = int(rng.integers(0, M - m + 1)) // 4 * 4  # 16-byte aligned window
+        c0 = int(rng.integers(0, Kx - k + 1))
+        out.append((m, n, k, pools[n].data_ptr() + 4 * (r0 + c0 * M), M, seed * 1000003 + i))
+    return out
+
+
+def run_served(args, wl):
+    import numpy as np
+    import torch
+
+    import shgemm_b200 as sg
+    from shgemm_b200 import evaluation as ev
+    from shgemm_b200 import server as srv
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    dev = torch.device(f"cuda:{local}")
+    torch.cuda.set_device(dev)
+    rate = args.rate or wl["rate"]
+    duration = args.duration or wl["duration"]
+    draws, tc = wl["draws"], wl["tc"]
+    pools = make_sketch_pools(wl, dev, seed=rank)
+    reqs = sketch_requests(wl, pools, seed=rank, count=int(rate * duration * 1.5) + 64)
+    mean_flops = float(np.mean([2.0 * m * n * draws * k for (m, n, k, _, _, _) in reqs]))
+
+    server = srv.SketchServer(local, hbm_budget_bytes=wl["budget"], compute_type=tc, streams=2, auto_release=True)
+    # warm-up: a few short bursts through the same server (kernels, arena, streams)
+    warm = sketch_requests(wl, pools, seed=10_000 + rank, count=8 * args.warmup)
+    for (m, n, k, a, lda, sd) in warm:
+        server.submit(m, n, k, a, lda, draws=draws, seed=sd)
+    server.drain()
+    server.reset_stats()
+    if dist:
+        dist.barrier()
+
+    arrival = np.random.default_rng(20_000 + rank)
+    with ClockSampler(local) as clk:
+        t0 = time.perf_counter()
+        due, i = 0.0, 0
+        while i < len(reqs):
+            due += arrival.exponential(1.0 / rate)
+            if due > duration:
+                break
+            while time.perf_counter() - t0 < due:
+                pass
+            m, n, k, a, lda, sd = reqs[i]
+            server.submit(m, n, k, a, lda, draws=draws, seed=sd)
+            i += 1
+        submitted_s = time.perf_counter() - t0
+        server.drain(timeout_ms=1e6)
+    st = server.stats()
+    server.close()
+    offered = i * mean_flops / duration / 1e12
+    span = st["span_s"]
+    flops = st["flops_completed"]
+    tt = torch.tensor([span, flops, st["p50_ms"], st["p99_ms"]], device=dev, dtype=torch.float64)
+    if dist:
+        spans = tt.clone()
+        dist.all_reduce(spans, op=dist.ReduceOp.MAX)
+        fl = tt.clone()
+        dist.all_reduce(fl, op=dist.ReduceOp.SUM)
+        span, flops = float(spans[0]), float(fl[1])
+    value = flops / span / 1e12
+
+    # per-call baseline: the same kind of requests as plain shgemm calls, one per Omega draw
+    h = sg.Handle(local)
+    stream = torch.cuda.Stream(dev)
+    h.set_stream(stream)
+    sample = reqs[:min(len(reqs), 64)]
+    oms = []
+    for (m, n, k, a, lda, sd) in sample:
+        ldb = (k + 7) // 8 * 8
+        om = torch.empty(n * draws * ldb, device=dev, dtype=torch.float16)
+        for j in range(draws):
+            srv.generate_omega(om[j * n * ldb:], ldb, k, n, srv.GAUSSIAN, srv.draw_seed(sd, j), n ** -0.5,
+                               stream=stream)
+        oms.append((om, ldb))
+    ymax = max(m * n for (m, n, _, _, _, _) in sample)
+    Y = torch.empty(ymax, device=dev)
+
+    def per_call():
+        for (m, n, k, a, lda, sd), (om, ldb) in zip(sample, oms):
+            for j in range(draws):
+                sg.shgemm(h, 0, 0, m, n, k, 1.0, a, lda, om[j * n * ldb:], ldb, 0.0, Y, m, tc)
+
+    with torch.cuda.stream(stream):
+        per_call()
+        p0, p1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        p0.record(stream)
+        per_call()
+        p1.record(stream)
+    torch.cuda.synchronize(dev)
+    pc_flops = sum(2.0 * m * n * draws * k for (m, n, k, _, _, _) in sample)
+    per_call_tflops = pc_flops / (p0.elapsed_time(p1) * 1e-3) / 1e12
+
+    # error of a few served results against the FP64 product (results kept: no auto-release)
+    errs = []
+    if not args.no_error:
+        chk = srv.SketchServer(local, hbm_budget_bytes=8 << 30, compute_type=tc, auto_release=False)
+        for (m, n, k, a, lda, sd), (om, ldb) in list(zip(sample, oms))[:4]:
+            t = chk.submit(m, n, k, a, lda, draws=draws, seed=sd)
+            chk.wait(t)
+            _, y, ldy, _ = chk.poll(t)
+            for j in range(draws):
+                c64 = ev.fp64_product(h, 0, 0, m, n, k, a, lda, om[j * n * ldb:], ldb)
+                errs.append(ev.error(h, m, n, y + 4 * j * m * n, m, c64)["rel_fro"])
+            chk.release(t)
+        chk.close()
+    h.close()
+
+    peaks, peak_kind = load_peaks()
+    tf32_peak = peaks.get("bf16_tflops_sustained", 1376.1) / 2  # TF32 runs at half the 16-bit rate
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "TFLOP/s", "n_gpus": world, "steps": int(st["completed"]),
+            "warmup": args.warmup, "ms_per_step": 1e3 * span / max(1, st["completed"]), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32 split to tf32 (tensor) / f32 accumulate" if tc else "f32 split to fp16 (tensor) / f32 accumulate",
+            "data": "synthetic (seeded, config 5 shapes and distributions; A windows of device-resident "
+                    "low-rank pools, Omega generated on the device per request)",
+            "config": {"workload": wl["desc"], "rate_req_s": rate, "duration_s": duration, "requests": i,
+                       "draws": draws, "budget_bytes": wl["budget"], "streams": 2,
+                       "step": "one served request (ms_per_step = stream span / requests completed)",
+                       "timing": "host clock: first submit to the last completion seen by the server",
+                       "parallelism": f"replicas x{world}"},
+            "served": {"p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"], "mean_ms": st["mean_ms"],
+                       "max_ms": st["max_ms"], "completed": st["completed"], "failed": st["failed"],
+                       "batches": st["batches"], "span_s": span, "submit_s": submitted_s,
+                       "offered_tflops": offered, "peak_resident_bytes": st["peak_resident_bytes"]},
+            "per_call_baseline": {"value": per_call_tflops, "unit": "TFLOP/s",
+                                  "what": f"first {len(sample)} requests as plain shgemm calls, one per Omega draw, "
+                                          "back to back on one stream"},
+            "speedup_vs_per_call": value / world / per_call_tflops,
+            "issued_tflops": 2 * value,
+            # per batch: one grouped launch plus one Omega generation per draw of each request
+            "gpu_launches": int(st["batches"]) + int(st["completed"]) * draws,
+            "roofline": {"bound": "tensor", "achieved": 2 * value / world, "peak": tf32_peak if tc else
+                         peaks.get("bf16_tflops_sustained", 1376.1), "unit": "TFLOP/s",
+                         "frac": 2 * value / world / (tf32_peak if tc else peaks.get("bf16_tflops_sustained", 1376.1)),
+                         "traffic": None,
+                         "peak_kind": f"{peak_kind} sustained dense bf16 (halved for tf32)",
+                         "work_per_launch": "issued 4mnk of the batch's requests"},
+            "clocks": clk.summary(),
+            "error": {"sample_rel_err_fp64": errs, "max_rel_err_fp64": max(errs) if errs else None},
+            "e2e": None,
+            "e2e_note": "requests reference device-resident A by design (the server keeps A, Omega and Y on "
+                        "the device); no host copies are part of a request",
+            "cpu_baseline": None,
+        }
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -446,6 +656,8 @@ def main():
     ap.add_argument("--no-error", action="store_true", help="skip the FP64 error measurement")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer end-to-end measurement")
+    ap.add_argument("--rate", type=float, default=None, help="served: arrivals per second")
+    ap.add_argument("--duration", type=float, default=None, help="served: seconds of arrivals")
     args = ap.parse_args()
     wl = dict(WORKLOADS[args.workload])
     if args.tc:
@@ -455,6 +667,8 @@ def main():
         return run_reference_arm(args, wl)
     if wl["dist"] == "grouped":
         return run_grouped(args, wl)
+    if wl["dist"] == "served":
+        return run_served(args, wl)
 
     import torch
 

@@ -199,6 +199,84 @@ size_t shgemm_b200_noalloc_scratch_bytes(void);
  * word (as shgemm_b200_check_error does for a handle). No counterpart in the reference. */
 int shgemm_b200_noalloc_check_error(void* cuda_stream, int* device_code);
 
+/* ------------------------------------------------------------------------
+ * Sketch generation and the sketch server. No counterpart in the reference
+ * (whose sketches are host loops of shgemm calls).
+ * ------------------------------------------------------------------------ */
+
+/* Distribution of a generated sketch operand Omega. */
+enum { SHGEMM_OMEGA_GAUSSIAN = 0, SHGEMM_OMEGA_RADEMACHER = 1 };
+
+/* Writes Omega (k x cols, column-major, leading dimension ld elements) on `cuda_stream`:
+ * entry (r, c) = scale * g(seed, c * k + r) rounded to binary16, g standard normal
+ * (Box-Muller over a splitmix64 counter hash) or a random sign. fp32 = 0 stores
+ * binary16; fp32 = 1 stores the same binary16 values widened to FP32 (the B operand
+ * of a TF32 batch with SHGEMM_CFG_GROUPED_B_FP32). */
+int shgemm_b200_generate_omega(void* cuda_stream, void* dst, size_t ld, size_t k, size_t cols, int dist,
+                               unsigned long long seed, float scale, int fp32);
+
+typedef struct shgemm_b200_server* shgemm_b200_server_t;
+
+typedef struct {
+    size_t hbm_budget_bytes; /* admission budget: A + Omega + Y of every admitted request */
+    int compute_type;        /* SHGEMM_TC_FP16 or SHGEMM_TC_TF32 */
+    int max_batch;           /* requests per grouped launch (<= 8192; 0: 512) */
+    int streams;             /* grouped launches in flight at once (1..8; 0: 2) */
+    int auto_release;        /* 1: a completed request's Y is freed at once (throughput runs) */
+} shgemm_b200_server_config;
+
+/* One sketch request: Y = A [Omega_1 ... Omega_draws], A m x k FP32 column-major
+ * (op_n, 16-byte aligned with lda a multiple of 4, device memory the caller keeps
+ * unchanged until the request completes). Omega_j (k x n) is what
+ * shgemm_b200_generate_omega writes for seed omega_seed * 1099511628211 + j.
+ * Y is m x (draws n), column-major with ld m, allocated by the server inside the budget. */
+typedef struct {
+    size_t m, n, k;
+    const float* a;
+    size_t lda;
+    int draws;
+    int omega_dist;          /* SHGEMM_OMEGA_* */
+    float omega_scale;       /* e.g. 1/sqrt(n) */
+    unsigned long long omega_seed;
+} shgemm_b200_sketch_request;
+
+enum { SHGEMM_REQ_QUEUED = 0, SHGEMM_REQ_ADMITTED = 1, SHGEMM_REQ_RUNNING = 2, SHGEMM_REQ_DONE = 3,
+       SHGEMM_REQ_FAILED = 4, SHGEMM_REQ_UNKNOWN = 5 };
+
+typedef struct {
+    unsigned long long submitted, completed, failed, batches;
+    double p50_ms, p99_ms, mean_ms, max_ms; /* submit -> completion observed, completed requests */
+    double flops_completed;                 /* sum of 2 m (draws n) k */
+    double span_s;                          /* first submit -> last completion */
+    size_t peak_resident_bytes;             /* max over time of the admitted A + Omega + Y bytes */
+    size_t resident_bytes;
+    unsigned long long queued, in_flight;   /* now */
+} shgemm_b200_server_stats;
+
+/* Starts a server thread on `device` that admits requests first-come first-served
+ * while their A + Omega + Y bytes fit the budget, generates their Omega draws,
+ * batches the admitted requests into grouped launches on up to `streams` streams
+ * (so a new batch starts while earlier ones finish) and records each completion.
+ * Omega and Y live in one device arena of the budget's size allocated here. */
+int shgemm_b200_server_create(shgemm_b200_server_t* server, int device, const shgemm_b200_server_config* config);
+int shgemm_b200_server_destroy(shgemm_b200_server_t server);
+/* Queues a request (returns at once). SHGEMM_STATUS_NOT_SUPPORTED if it can never fit the budget. */
+int shgemm_b200_server_submit(shgemm_b200_server_t server, const shgemm_b200_sketch_request* request,
+                              unsigned long long* ticket);
+/* State of a request; when done, *y / *ldy give its result and *latency_ms the
+ * submit-to-completion time. Any output pointer may be NULL. */
+int shgemm_b200_server_poll(shgemm_b200_server_t server, unsigned long long ticket, int* state, float** y,
+                            size_t* ldy, double* latency_ms);
+/* Waits (up to timeout_ms) until the request is done or failed. */
+int shgemm_b200_server_wait(shgemm_b200_server_t server, unsigned long long ticket, double timeout_ms, int* state);
+/* Waits (up to timeout_ms) until every submitted request is done or failed. */
+int shgemm_b200_server_drain(shgemm_b200_server_t server, double timeout_ms);
+/* Returns a completed request's Y to the budget (not needed with auto_release). */
+int shgemm_b200_server_release(shgemm_b200_server_t server, unsigned long long ticket);
+int shgemm_b200_server_get_stats(shgemm_b200_server_t server, shgemm_b200_server_stats* stats);
+/* Forgets the latency samples and counters (not the requests in flight). */
+int shgemm_b200_server_reset_stats(shgemm_b200_server_t server);
+
 #ifdef __cplusplus
 }
 #endif

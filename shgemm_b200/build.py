@@ -12,7 +12,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libshgemm_b200.so")
-SOURCES = ["shgemm_lib.cu", "shgemm_api.cpp"]
+SOURCES = ["shgemm_lib.cu", "shgemm_api.cpp", "shgemm_server.cpp"]
 HEADERS = ["ptx.cuh", "shgemm_kernel.cuh"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
@@ -40,7 +40,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
     if not force and up_to_date():
         return LIB
     cmd = [nvcc(), *ARCH, "-O3", "-lineinfo", "-std=c++17", "-shared", "-Xcompiler", "-fPIC",
-           "-Xcompiler", "-fvisibility=default", "--expt-relaxed-constexpr",
+           "-Xcompiler", "-fvisibility=default", "-Xcompiler", "-pthread", "--expt-relaxed-constexpr",
            "-I", os.path.join(ROOT, "include"), "-I", CSRC]
     if verbose:
         cmd += ["-Xptxas", "-v"]

@@ -186,6 +186,39 @@ __global__ void splitk_reduce_kernel(const float* __restrict__ ws, int slices, i
     }
 }
 
+// Sketch operand generator: entry (r, c) of a k x cols column-major Omega from a
+// counter hash of (seed, c * k + r) -- splitmix64's finaliser (Steele, Lea and Flood,
+// "Fast splittable pseudorandom number generators", 2014) -- then Box-Muller for a
+// standard normal or the top bit for a sign; scaled and rounded to binary16.
+__device__ __forceinline__ uint64_t mix64(uint64_t z) {
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+
+__global__ void omega_kernel(void* dst, uint64_t ld, uint64_t k, uint64_t cols, int dist, uint64_t seed, float scale,
+                             int fp32) {
+    const uint64_t total = k * cols;
+    for (uint64_t idx = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; idx < total;
+         idx += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        const uint64_t c = idx / k, r = idx - c * k;
+        const uint64_t x = mix64(seed * 0x9E3779B97F4A7C15ull + idx + 1);
+        float v;
+        if (dist == SHGEMM_OMEGA_RADEMACHER) {
+            v = (x >> 63) ? -scale : scale;
+        } else {
+            const float u1 = static_cast<float>((x >> 40) + 1) * 0x1p-24f;  // (0, 1]
+            const float u2 = static_cast<float>((x >> 16) & 0xFFFFFFull) * 0x1p-24f;
+            v = scale * (sqrtf(-2.0f * logf(u1)) * cospif(2.0f * u2));
+        }
+        const __half hv = __float2half_rn(v);
+        if (fp32)
+            static_cast<float*>(dst)[r + c * ld] = __half2float(hv);
+        else
+            static_cast<__half*>(dst)[r + c * ld] = hv;
+    }
+}
+
 __global__ void selftest_wait_kernel(int* error_flag, uint64_t limit_ns) {
     __shared__ __align__(8) uint64_t bar;
     __shared__ int abort_flag;
@@ -566,6 +599,22 @@ int shgemm_b200_check_error(shgemm_b200_handle_t h, int* device_code) {
 int shgemm_b200_get_launch_count(shgemm_b200_handle_t h, long long* count) {
     if (!h || !count) return SHGEMM_STATUS_INVALID_VALUE;
     *count = h->launches.load();
+    return SHGEMM_STATUS_OK;
+}
+
+int shgemm_b200_generate_omega(void* cuda_stream, void* dst, size_t ld, size_t k, size_t cols, int dist,
+                               unsigned long long seed, float scale, int fp32) {
+    if ((dist != SHGEMM_OMEGA_GAUSSIAN && dist != SHGEMM_OMEGA_RADEMACHER) || (fp32 != 0 && fp32 != 1) || ld < k)
+        return SHGEMM_STATUS_INVALID_VALUE;
+    if (k == 0 || cols == 0) return SHGEMM_STATUS_OK;
+    if (!dst) return SHGEMM_STATUS_INVALID_VALUE;
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const uint64_t total = static_cast<uint64_t>(k) * cols;
+    const unsigned blocks = static_cast<unsigned>(std::min<uint64_t>((total + 255) / 256, static_cast<uint64_t>(sms) * 8));
+    omega_kernel<<<blocks, 256, 0, static_cast<cudaStream_t>(cuda_stream)>>>(dst, ld, k, cols, dist, seed, scale, fp32);
+    if (cudaGetLastError() != cudaSuccess) return SHGEMM_STATUS_LAUNCH_FAILED;
     return SHGEMM_STATUS_OK;
 }
 

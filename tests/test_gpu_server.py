@@ -1,0 +1,182 @@
+"""The sketch server: on-device Omega generation, results against the oracle, the same
+result alone and in a mix of concurrent requests, and HBM-budget admission. No
+reference counterpart (the reference's callers run one shgemm() per sketch)."""
+import numpy as np
+import pytest
+
+import oracle
+from tests import _cases as K
+
+pytestmark = pytest.mark.gpu
+
+
+def _rand_a(rng, m, k):
+    import torch
+
+    lda = (m + 3) // 4 * 4 + 4
+    A = rng.uniform(-1, 1, lda * k).astype(np.float32)
+    return A, lda, torch.from_numpy(A).cuda()
+
+
+def _omega_host(k, n, draw_seed, fp32, scale, dist=0):
+    """Omega of one draw, generated on the device by the library and copied back as binary16."""
+    import torch
+
+    from shgemm_b200 import server as srv
+
+    if fp32:
+        ld = (k + 3) // 4 * 4
+        buf = torch.zeros(n * ld, device="cuda", dtype=torch.float32)
+    else:
+        ld = (k + 7) // 8 * 8
+        buf = torch.zeros(n * ld, device="cuda", dtype=torch.float16)
+    srv.generate_omega(buf, ld, k, n, dist, draw_seed, scale, fp32)
+    torch.cuda.synchronize()
+    om = buf.view(n, ld)[:, :k].cpu().numpy()
+    return om.astype(np.float16), om
+
+
+@pytest.mark.parametrize("dist", [0, 1])
+def test_generate_omega(cuda_device, dist):
+    from shgemm_b200 import server as srv
+
+    k, n = 4096, 64
+    scale = n ** -0.5
+    h16, _ = _omega_host(k, n, 7, False, scale, dist)
+    h16b, _ = _omega_host(k, n, 7, False, scale, dist)
+    h32, raw32 = _omega_host(k, n, 7, True, scale, dist)
+    other, _ = _omega_host(k, n, 8, False, scale, dist)
+    assert np.array_equal(h16.view(np.uint16), h16b.view(np.uint16))        # deterministic
+    assert np.array_equal(h16.astype(np.float32), raw32)                     # widened copy is exact
+    assert not np.array_equal(h16, other)                                     # seeds differ
+    x = h16.astype(np.float64)
+    if dist == srv.GAUSSIAN:
+        assert abs(x.mean()) < 5 * scale / np.sqrt(x.size)
+        assert abs(x.std() / scale - 1) < 0.02
+    else:
+        assert np.allclose(np.abs(x), np.float16(scale))
+        assert abs(np.mean(x > 0) - 0.5) < 0.01
+
+
+@pytest.mark.parametrize("tc", [oracle.FP16, oracle.TF32])
+def test_server_result_matches_oracle(cuda_device, tc):
+    import torch
+
+    from shgemm_b200 import server as srv
+
+    rng = np.random.default_rng(40 + tc)
+    m, n, k, draws, seed = 333, 48, 777, 3, 12345
+    A, lda, A_dev = _rand_a(rng, m, k)
+    with srv.SketchServer(0, hbm_budget_bytes=1 << 30, compute_type=tc) as s:
+        t = s.submit(m, n, k, A_dev, lda, draws=draws, seed=seed)
+        assert s.wait(t) == srv.DONE
+        st, y, ldy, lat = s.poll(t)
+        assert st == srv.DONE and y and ldy == m and lat >= 0
+        Y = _view(y, m * n * draws).clone()
+        torch.cuda.synchronize()
+        s.release(t)
+    Y = Y.cpu().numpy()
+    for j in range(draws):
+        om16, _ = _omega_host(k, n, srv.draw_seed(seed, j), tc == oracle.TF32, n ** -0.5)
+        inp = dict(A=A, B=om16.reshape(-1), C=np.zeros(m * n, np.float32), lda=lda, ldb=k, ldc=m)
+        gpu = Y[j * m * n:(j + 1) * m * n]
+        orc = K.run_oracle(tc, 0, 0, m, n, k, 1.0, inp, 0.0, 0, chunk=0)
+        ref = K.fp64(0, 0, m, n, k, 1.0, inp, 0.0, 0)
+        sgc = K.sgemm(0, 0, m, n, k, 1.0, inp, 0.0, 0)
+        K.assert_parity(K.parity_report(gpu, orc, ref, sgc, m, n, m, 0))
+
+
+def _view(addr, count):
+    """A CUDA float32 tensor over `count` floats at device address `addr` (no copy)."""
+    import torch
+
+    class _Buf:
+        __cuda_array_interface__ = {"shape": (count,), "typestr": "<f4", "data": (addr, False), "version": 3}
+
+    return torch.as_tensor(_Buf(), device="cuda")
+
+
+def test_server_same_result_alone_and_in_the_mix(cuda_device):
+    """One request's Y is bit-identical whether it runs alone or among concurrent requests."""
+    import torch
+
+    from shgemm_b200 import server as srv
+
+    rng = np.random.default_rng(77)
+    m, n, k = 1000, 64, 3000
+    _, lda, A_dev = _rand_a(rng, m, k)
+    others = []
+    for i in range(15):
+        mo, ko = int(rng.integers(100, 3000)), int(rng.integers(300, 5000))
+        _, ldo, Ao = _rand_a(rng, mo, ko)
+        others.append((mo, int(rng.choice([32, 64, 128])), ko, Ao, ldo))
+    for tc in (oracle.TF32, oracle.FP16):
+        with srv.SketchServer(0, hbm_budget_bytes=2 << 30, compute_type=tc, streams=2) as s:
+            t = s.submit(m, n, k, A_dev, lda, draws=4, seed=99)
+            s.wait(t)
+            _, y, _, _ = s.poll(t)
+            alone = _view(y, m * n * 4).clone()
+            s.release(t)
+            tickets = [s.submit(mo, no, ko, Ao, ldo, draws=4, seed=1000 + i)
+                       for i, (mo, no, ko, Ao, ldo) in enumerate(others[:8])]
+            t = s.submit(m, n, k, A_dev, lda, draws=4, seed=99)
+            tickets += [s.submit(mo, no, ko, Ao, ldo, draws=4, seed=2000 + i)
+                        for i, (mo, no, ko, Ao, ldo) in enumerate(others[8:])]
+            s.drain()
+            st, y, _, _ = s.poll(t)
+            assert st == srv.DONE
+            mixed = _view(y, m * n * 4).clone()
+            assert s.stats()["batches"] >= 2
+            for q in tickets + [t]:
+                s.release(q)
+        torch.cuda.synchronize()
+        assert torch.equal(alone, mixed), tc
+
+
+def test_server_admission_respects_budget(cuda_device):
+    from shgemm_b200 import server as srv
+
+    rng = np.random.default_rng(3)
+    m, n, k, draws = 2048, 128, 4096, 4
+    _, lda, A_dev = _rand_a(rng, m, k)
+    per_req = lda * k * 4 + k * n * draws * 4 + m * n * draws * 4
+    budget = int(per_req * 2.5)
+    with srv.SketchServer(0, hbm_budget_bytes=budget, compute_type=oracle.TF32, auto_release=True) as s:
+        tickets = [s.submit(m, n, k, A_dev, lda, draws=draws, seed=i) for i in range(12)]
+        s.drain()
+        st = s.stats()
+        assert st["completed"] == 12 and st["failed"] == 0
+        assert 0 < st["peak_resident_bytes"] <= budget
+        assert st["resident_bytes"] == 0
+        assert st["p99_ms"] >= st["p50_ms"] > 0
+        assert all(s.poll(t)[0] == srv.DONE for t in tickets)
+        # a request that can never fit is refused at submit
+        with pytest.raises(Exception):
+            s.submit(m, n, k * 4, A_dev, lda, draws=draws)
+
+
+def test_server_poisson_stream(cuda_device):
+    """A short Poisson stream of uneven requests: all complete, latencies recorded."""
+    import time
+
+    from shgemm_b200 import server as srv
+
+    rng = np.random.default_rng(11)
+    pool_k, pool_m = 4096, 4096
+    _, lda, A_dev = _rand_a(rng, pool_m, pool_k)
+    with srv.SketchServer(0, hbm_budget_bytes=4 << 30, compute_type=oracle.TF32, auto_release=True) as s:
+        t0 = time.perf_counter()
+        due = 0.0
+        for i in range(120):
+            due += rng.exponential(1 / 2000.0)
+            while time.perf_counter() - t0 < due:
+                pass
+            m = int(np.exp(rng.uniform(np.log(256), np.log(pool_m))))
+            k = int(np.exp(rng.uniform(np.log(256), np.log(pool_k))))
+            n = int(rng.choice([64, 128, 256]))
+            s.submit(m, n, k, A_dev, lda, draws=4, seed=i)
+        s.drain()
+        st = s.stats()
+    assert st["completed"] == 120 and st["failed"] == 0
+    assert st["batches"] >= 2
+    assert st["p99_ms"] >= st["p50_ms"] > 0
