@@ -46,10 +46,44 @@ enum {
     SHGEMM_CFG_SPLIT_K = 2,       /* 0 = automatic, 1 = never split, s > 1 = force s slices */
     SHGEMM_CFG_WAIT_LIMIT_MS = 3, /* bound on every in-kernel wait (default 2000 ms) */
     SHGEMM_CFG_GROUP_M = 4,       /* tile rasterisation group along m (default 8) */
-    SHGEMM_CFG_GROUPED_B_FP32 = 5 /* 1: grouped TF32 batches pass B as FP32 values that are
-                                     exactly binary16 (a widened copy), loaded without a
-                                     conversion; 0 (default): B is binary16 */
+    SHGEMM_CFG_GROUPED_B_FP32 = 5, /* 1: grouped TF32 batches pass B as FP32 values that are
+                                      exactly binary16 (a widened copy), loaded without a
+                                      conversion; 0 (default): B is binary16 */
+    SHGEMM_CFG_AUTOTUNE = 6        /* 0: heuristic plans only; 1 (default): a shape whose bucket
+                                      the autotuner has an entry for uses it; 2: as 1, and a call
+                                      with beta == 0 on an untuned bucket tunes it first */
 };
+
+/* ------------------------------------------------------------------------
+ * Autotuner. No reference counterpart (the reference fixes its tile tables at
+ * compile time, src/shgemm.cu:429-488, and picks one of two levels per call,
+ * src/shgemm.cu:643-656). A shape bucket is (compute type, op_a, op_b,
+ * floor(log2 m), floor(log2 n), floor(log2 k)); its entry names the tile N,
+ * the split-K slice count and the tile rasterisation group. The k-chunk of the
+ * FP32 drain is not tuned: it is one k-step (64 binary16 / 32 TF32 k), the
+ * longest interval that keeps the tensor core's truncation within the error bar.
+ * ------------------------------------------------------------------------ */
+typedef struct {
+    int tile_n;   /* 64, 128 or 256 (binary16); 64 or 128 (TF32) */
+    int slices;   /* split-K slices, 1 = none */
+    int group_m;  /* tiles along m per rasterisation group */
+    float time_us;
+} shgemm_b200_tuned_config;
+
+/* Times every candidate configuration on the given operands (C is overwritten with
+ * A B: the runs use alpha = 1, beta = 0), stores the fastest for the shape's bucket
+ * and returns it in *best. Synchronises the handle's stream; not while capturing.
+ * Operands must be TMA-addressable (16-byte aligned, 16-byte leading dimensions). */
+int shgemm_b200_autotune(shgemm_b200_handle_t handle, int op_a, int op_b, size_t m, size_t n, size_t k,
+                         const float* a, size_t lda, const void* b, size_t ldb, float* c, size_t ldc,
+                         int compute_type, shgemm_b200_tuned_config* best);
+/* The entry for a shape's bucket: SHGEMM_STATUS_OK and *cfg, or SHGEMM_STATUS_INVALID_VALUE if none. */
+int shgemm_b200_autotune_lookup(shgemm_b200_handle_t handle, int op_a, int op_b, size_t m, size_t n, size_t k,
+                                int compute_type, shgemm_b200_tuned_config* cfg);
+/* Writes / reads the table as text, one bucket per line. Loading adds to the table. */
+int shgemm_b200_autotune_save(shgemm_b200_handle_t handle, const char* path);
+int shgemm_b200_autotune_load(shgemm_b200_handle_t handle, const char* path);
+int shgemm_b200_autotune_clear(shgemm_b200_handle_t handle);
 
 /* mtk::shgemm::create (include/shgemm/shgemm.hpp:94; src/shgemm.cu:401-490).
  * Binds the handle to `device` (the reference hard-codes device 0, src/shgemm.cu:419-425),

@@ -24,7 +24,7 @@ op_n, op_t = 0, 1          # operation_t (include/shgemm/shgemm.hpp:36-39)
 fp16, tf32 = 0, 1          # tc_t (include/shgemm/shgemm.hpp:41-44)
 P0, P1 = 0, 1              # detail::kernel_level (include/shgemm/shgemm.hpp:30-34)
 
-CFG_SPLIT_K, CFG_WAIT_LIMIT_MS, CFG_GROUP_M, CFG_GROUPED_B_FP32 = 2, 3, 4, 5
+CFG_SPLIT_K, CFG_WAIT_LIMIT_MS, CFG_GROUP_M, CFG_GROUPED_B_FP32, CFG_AUTOTUNE = 2, 3, 4, 5, 6
 
 STATUS = {0: "OK", 1: "INVALID_VALUE", 2: "NOT_SUPPORTED", 3: "ALLOC_FAILED", 4: "LAUNCH_FAILED",
           5: "TIMEOUT", 6: "CUDA_ERROR", 7: "SCRATCH_TOO_SMALL"}
@@ -40,6 +40,16 @@ class Problem(ctypes.Structure):
     _fields_ = [("m", ctypes.c_size_t), ("n", ctypes.c_size_t), ("k", ctypes.c_size_t), ("a", ctypes.c_void_p),
                 ("lda", ctypes.c_size_t), ("b", ctypes.c_void_p), ("ldb", ctypes.c_size_t), ("c", ctypes.c_void_p),
                 ("ldc", ctypes.c_size_t), ("alpha", ctypes.c_float), ("beta", ctypes.c_float)]
+
+
+class TunedConfig(ctypes.Structure):
+    """shgemm_b200_tuned_config: the autotuner's choice for a shape bucket (include/shgemm_b200.h)."""
+
+    _fields_ = [("tile_n", ctypes.c_int), ("slices", ctypes.c_int), ("group_m", ctypes.c_int),
+                ("time_us", ctypes.c_float)]
+
+    def as_dict(self) -> dict:
+        return {"tile_n": self.tile_n, "slices": self.slices, "group_m": self.group_m, "time_us": self.time_us}
 
 
 class ShgemmError(RuntimeError):
@@ -83,6 +93,11 @@ def lib() -> ctypes.CDLL:
         "shgemm_b200_shgemm_grouped": [vp, i, i, i, i, ctypes.POINTER(Problem), i],
         "shgemm_b200_grouped_update": [vp, i, i, i, i, ctypes.POINTER(Problem), i],
         "shgemm_b200_noalloc_check_error": [vp, pi],
+        "shgemm_b200_autotune": [vp, i, i, sz, sz, sz, vp, sz, vp, sz, vp, sz, i, ctypes.POINTER(TunedConfig)],
+        "shgemm_b200_autotune_lookup": [vp, i, i, sz, sz, sz, i, ctypes.POINTER(TunedConfig)],
+        "shgemm_b200_autotune_save": [vp, ctypes.c_char_p],
+        "shgemm_b200_autotune_load": [vp, ctypes.c_char_p],
+        "shgemm_b200_autotune_clear": [vp],
     }
     for name, args in sig.items():
         fn = getattr(L, name)
@@ -177,6 +192,30 @@ class Handle:
         if st not in (0, 5):
             raise ShgemmError(st, "check_error")
         return code.value
+
+    def autotune(self, op_a: int, op_b: int, m: int, n: int, k: int, A, lda: int, B, ldb: int, C, ldc: int,
+                 compute_type: int) -> dict:
+        """Times the candidate plans on these operands (C is overwritten), keeps the fastest
+        for the shape's bucket and returns it."""
+        best = TunedConfig()
+        _check(lib().shgemm_b200_autotune(self.ptr, op_a, op_b, m, n, k, _addr(A), lda, _addr(B), ldb, _addr(C), ldc,
+                                          compute_type, ctypes.byref(best)), "autotune")
+        return best.as_dict()
+
+    def autotune_lookup(self, op_a: int, op_b: int, m: int, n: int, k: int, compute_type: int):
+        """The tuned entry of the shape's bucket, or None."""
+        cfg = TunedConfig()
+        st = lib().shgemm_b200_autotune_lookup(self.ptr, op_a, op_b, m, n, k, compute_type, ctypes.byref(cfg))
+        return cfg.as_dict() if st == 0 else None
+
+    def autotune_save(self, path: str) -> None:
+        _check(lib().shgemm_b200_autotune_save(self.ptr, os.fsencode(path)), "autotune_save")
+
+    def autotune_load(self, path: str) -> None:
+        _check(lib().shgemm_b200_autotune_load(self.ptr, os.fsencode(path)), "autotune_load")
+
+    def autotune_clear(self) -> None:
+        _check(lib().shgemm_b200_autotune_clear(self.ptr), "autotune_clear")
 
     def launch_count(self) -> int:
         v = ctypes.c_longlong()

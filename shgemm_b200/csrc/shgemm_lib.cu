@@ -12,6 +12,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <map>
 #include <mutex>
 #include <vector>
 
@@ -41,6 +42,10 @@ struct shgemm_b200_handle {
     int grouped_b_fp32 = 0;  // SHGEMM_CFG_GROUPED_B_FP32
     int grouped_units = 0;
     int grouped_copied_count = 0;  // problem slots the last enqueued copy covers
+    // autotuner: best (tile N, split-K slices, rasterisation group) per shape bucket
+    int autotune_mode = 1;  // SHGEMM_CFG_AUTOTUNE
+    std::mutex tune_mu;
+    std::map<uint64_t, shgemm_b200_tuned_config> tuned;
 };
 
 namespace {
@@ -366,6 +371,41 @@ int level_bn(int tc, int level) { return tc == kFP16 ? (level ? 256 : 128) : (le
 
 // Tiling and split-K plan. `split_k`: 0 automatic, 1 never, s > 1 forced. Split-K
 // partials need slices * m * n floats of scratch, bounded by `ws_bytes`.
+// Shape bucket of the autotuner: compute type, operand layouts and floor(log2) of m, n, k.
+int ilog2(size_t x) {
+    int r = 0;
+    while (x > 1) {
+        x >>= 1;
+        ++r;
+    }
+    return r;
+}
+uint64_t tune_key(int tc, int op_a, int op_b, size_t m, size_t n, size_t k) {
+    return (static_cast<uint64_t>(tc) << 27) | (static_cast<uint64_t>(op_a) << 26) |
+           (static_cast<uint64_t>(op_b) << 25) | (static_cast<uint64_t>(ilog2(m)) << 16) |
+           (static_cast<uint64_t>(ilog2(n)) << 8) | static_cast<uint64_t>(ilog2(k));
+}
+
+// A tuned configuration applied to a shape: the tile N and the slice count it names,
+// the slices capped by what the workspace holds and by the k-steps there are.
+Plan plan_from_tuned(const shgemm_b200_tuned_config& t, size_t m, size_t n, size_t k, int tc, size_t ws_bytes) {
+    Plan p{};
+    const int bk = (tc == kFP16) ? 64 : 32;
+    p.total_steps = static_cast<int>((k + bk - 1) / bk);
+    p.tiles_m = static_cast<int>((m + 127) / 128);
+    p.bn = t.tile_n;
+    p.level = p.bn == level_bn(tc, 1) ? 1 : 0;
+    p.tiles_n = static_cast<int>((n + p.bn - 1) / p.bn);
+    const size_t per_slice = m * n * sizeof(float);
+    const int fit = per_slice ? static_cast<int>(std::min<size_t>(ws_bytes / per_slice, 1024)) : 0;
+    int slices = std::max(1, t.slices);
+    if (slices > 1 && fit < 2) slices = 1;
+    slices = std::min({slices, std::max(fit, 1), p.total_steps});
+    p.steps_per_slice = (p.total_steps + slices - 1) / slices;
+    p.slices = (p.total_steps + p.steps_per_slice - 1) / p.steps_per_slice;
+    return p;
+}
+
 Plan make_plan_for(int num_sms, int fixed_level, long long split_k, size_t m, size_t n, size_t k, int tc,
                    size_t ws_bytes) {
     Plan p{};
@@ -409,7 +449,19 @@ Plan make_plan_for(int num_sms, int fixed_level, long long split_k, size_t m, si
     return p;
 }
 
-Plan make_plan(const shgemm_b200_handle* h, size_t m, size_t n, size_t k, int tc, size_t ws_bytes) {
+// The plan of a call: the autotuner's entry for the shape's bucket when there is one
+// (and neither a fixed level nor a forced split overrides it), else the heuristic.
+Plan make_plan(shgemm_b200_handle* h, int op_a, int op_b, size_t m, size_t n, size_t k, int tc, size_t ws_bytes,
+               int* group_m) {
+    *group_m = static_cast<int>(h->group_m);
+    if (h->autotune_mode != 0 && h->fixed_level == SHGEMM_LEVEL_AUTO && h->split_k == 0) {
+        std::lock_guard<std::mutex> lk(h->tune_mu);
+        auto it = h->tuned.find(tune_key(tc, op_a, op_b, m, n, k));
+        if (it != h->tuned.end()) {
+            *group_m = it->second.group_m;
+            return plan_from_tuned(it->second, m, n, k, tc, ws_bytes);
+        }
+    }
     return make_plan_for(h->num_sms, h->fixed_level, h->split_k, m, n, k, tc, ws_bytes);
 }
 
@@ -553,6 +605,10 @@ int shgemm_b200_set_config(shgemm_b200_handle_t h, int key, long long v) {
             if (v != 0 && v != 1) return SHGEMM_STATUS_INVALID_VALUE;
             h->grouped_b_fp32 = static_cast<int>(v);
             return SHGEMM_STATUS_OK;
+        case SHGEMM_CFG_AUTOTUNE:
+            if (v < 0 || v > 2) return SHGEMM_STATUS_INVALID_VALUE;
+            h->autotune_mode = static_cast<int>(v);
+            return SHGEMM_STATUS_OK;
         default:
             return SHGEMM_STATUS_INVALID_VALUE;
     }
@@ -565,6 +621,7 @@ int shgemm_b200_get_config(shgemm_b200_handle_t h, int key, long long* v) {
         case SHGEMM_CFG_WAIT_LIMIT_MS: *v = h->wait_limit_ms; return SHGEMM_STATUS_OK;
         case SHGEMM_CFG_GROUP_M: *v = h->group_m; return SHGEMM_STATUS_OK;
         case SHGEMM_CFG_GROUPED_B_FP32: *v = h->grouped_b_fp32; return SHGEMM_STATUS_OK;
+        case SHGEMM_CFG_AUTOTUNE: *v = h->autotune_mode; return SHGEMM_STATUS_OK;
         default: return SHGEMM_STATUS_INVALID_VALUE;
     }
 }
@@ -634,8 +691,12 @@ int shgemm_b200_selftest_wait_timeout(shgemm_b200_handle_t h, unsigned limit_us,
 
 static int run_tiled(shgemm_b200_handle_t h, int op_a, int op_b, size_t m, size_t n, size_t k, float alpha,
                      const float* a, size_t lda, const void* b, size_t ldb, float beta, float* c, size_t ldc, int tc,
-                     int op_c, int* level_out, float* splitk_ws, size_t splitk_bytes) {
-    const Plan pl = make_plan(h, m, n, k, tc, splitk_bytes);
+                     int op_c, int* level_out, float* splitk_ws, size_t splitk_bytes,
+                     const shgemm_b200_tuned_config* force = nullptr) {
+    int group_m = 8;
+    const Plan pl = force ? plan_from_tuned(*force, m, n, k, tc, splitk_bytes)
+                          : make_plan(h, op_a, op_b, m, n, k, tc, splitk_bytes, &group_m);
+    if (force) group_m = force->group_m;
     const bool a_kmajor = (op_a == kOpT);
     const bool b_kmajor = (op_b == kOpN);
     const int bk = (tc == kFP16) ? 64 : 32;
@@ -685,7 +746,7 @@ static int run_tiled(shgemm_b200_handle_t h, int op_a, int op_b, size_t m, size_
     P.num_slices = pl.slices;
     P.steps_per_slice = pl.steps_per_slice;
     P.num_units = pl.tiles_m * pl.tiles_n * pl.slices;
-    P.group_m = static_cast<int>(h->group_m);
+    P.group_m = group_m;
 
     const KernelEntry e = kernel_table(tc, pl.bn, a_kmajor, b_kmajor);
     if (!e.fn) return SHGEMM_STATUS_NOT_SUPPORTED;
@@ -761,9 +822,26 @@ int shgemm_b200_shgemm(shgemm_b200_handle_t h, int op_a, int op_b, size_t m, siz
     // TMA addresses 16-byte aligned bases with 16-byte aligned leading dimensions.
     const bool pack_a = (reinterpret_cast<uintptr_t>(a) & 15) || (lda * 4) % 16;
     const bool pack_b = (reinterpret_cast<uintptr_t>(b) & 15) || (ldb * 2) % 16;
-    if (!pack_a && !pack_b)
+    if (!pack_a && !pack_b) {
+        // SHGEMM_CFG_AUTOTUNE = 2: an untuned bucket is tuned on this call's operands first
+        // (C is overwritten by the candidates, harmless when beta == 0 and C is laid out op_n).
+        if (h->autotune_mode == 2 && beta == 0.0f && op_c == kOpN && h->fixed_level == SHGEMM_LEVEL_AUTO &&
+            h->split_k == 0) {
+            bool have;
+            {
+                std::lock_guard<std::mutex> lk(h->tune_mu);
+                have = h->tuned.count(tune_key(tc, op_a, op_b, m, n, k)) != 0;
+            }
+            cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+            if (!have && cudaStreamIsCapturing(h->stream, &cap) == cudaSuccess && cap == cudaStreamCaptureStatusNone) {
+                const int st = shgemm_b200_autotune(h, op_a, op_b, m, n, k, a, lda, b, ldb, c, ldc, tc, nullptr);
+                if (st != SHGEMM_STATUS_OK) return st;
+            }
+            cudaGetLastError();
+        }
         return run_tiled(h, op_a, op_b, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc, tc, op_c, level_out,
                          h->workspace, h->workspace_bytes);
+    }
 
     // Staging path: copy the unaligned operand(s) slab by slab (k-slabs of a multiple
     // of 64) into the handle's workspace with aligned leading dimensions, then run the
@@ -817,6 +895,180 @@ int shgemm_b200_shgemm(shgemm_b200_handle_t h, int op_a, int op_b, size_t m, siz
         if (st != SHGEMM_STATUS_OK) return st;
     }
     if (level_out) *level_out = level;
+    return SHGEMM_STATUS_OK;
+}
+
+// ---------------------------------------------------------------- autotuner
+static bool tile_n_valid(int tc, int bn) { return bn == 64 || bn == 128 || (bn == 256 && tc == kFP16); }
+
+// Median device time of `reps` runs of one configuration (after one untimed run).
+static int time_config(shgemm_b200_handle_t h, int op_a, int op_b, size_t m, size_t n, size_t k, const float* a,
+                       size_t lda, const void* b, size_t ldb, float* c, size_t ldc, int tc,
+                       const shgemm_b200_tuned_config& cfg, int reps, float* us) {
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) {
+        cudaGetLastError();
+        if (e0) cudaEventDestroy(e0);
+        return SHGEMM_STATUS_CUDA_ERROR;
+    }
+    int lvl = 0, st = SHGEMM_STATUS_OK;
+    std::vector<float> t;
+    for (int r = -1; r < reps && st == SHGEMM_STATUS_OK; ++r) {
+        cudaEventRecord(e0, h->stream);
+        st = run_tiled(h, op_a, op_b, m, n, k, 1.0f, a, lda, b, ldb, 0.0f, c, ldc, tc, kOpN, &lvl, h->workspace,
+                       h->workspace_bytes, &cfg);
+        cudaEventRecord(e1, h->stream);
+        if (cudaEventSynchronize(e1) != cudaSuccess) st = SHGEMM_STATUS_CUDA_ERROR;
+        float ms = 0;
+        cudaEventElapsedTime(&ms, e0, e1);
+        if (r >= 0) t.push_back(ms * 1000.0f);
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (st != SHGEMM_STATUS_OK) {
+        cudaGetLastError();
+        return st;
+    }
+    int code = 0;
+    if (shgemm_b200_check_error(h, &code) != SHGEMM_STATUS_OK) return SHGEMM_STATUS_TIMEOUT;
+    std::sort(t.begin(), t.end());
+    *us = t[t.size() / 2];
+    return SHGEMM_STATUS_OK;
+}
+
+int shgemm_b200_autotune(shgemm_b200_handle_t h, int op_a, int op_b, size_t m, size_t n, size_t k, const float* a,
+                         size_t lda, const void* b, size_t ldb, float* c, size_t ldc, int tc,
+                         shgemm_b200_tuned_config* best_out) {
+    if (!h || !c || m == 0 || n == 0 || k == 0 || !a || !b) return SHGEMM_STATUS_INVALID_VALUE;
+    if ((op_a != kOpN && op_a != kOpT) || (op_b != kOpN && op_b != kOpT) || (tc != kFP16 && tc != kTF32))
+        return SHGEMM_STATUS_INVALID_VALUE;
+    if (ldc < m || lda < (op_a == kOpN ? m : k) || ldb < (op_b == kOpN ? k : n)) return SHGEMM_STATUS_INVALID_VALUE;
+    if ((reinterpret_cast<uintptr_t>(a) & 15) || (lda * 4) % 16 || (reinterpret_cast<uintptr_t>(b) & 15) ||
+        (ldb * 2) % 16 || m >= (1u << 31) || n >= (1u << 31) || k >= (1u << 31))
+        return SHGEMM_STATUS_NOT_SUPPORTED;
+    DeviceGuard g(h->device);
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(h->stream, &cap) != cudaSuccess || cap != cudaStreamCaptureStatusNone) {
+        cudaGetLastError();
+        return SHGEMM_STATUS_NOT_SUPPORTED;
+    }
+    const int bk = tc == kFP16 ? 64 : 32;
+    const int steps = static_cast<int>((k + bk - 1) / bk);
+    const size_t per_slice = m * n * sizeof(float);
+    const int fit = static_cast<int>(std::min<size_t>(h->workspace_bytes / per_slice, 1024));
+    const int tile_ns[] = {64, 128, 256};
+    const int slice_set[] = {1, 2, 3, 4, 6, 8, 12, 16};
+    // one timed run of the heuristic plan sizes the repetitions
+    shgemm_b200_tuned_config best{};
+    {
+        const Plan hp = make_plan_for(h->num_sms, SHGEMM_LEVEL_AUTO, 0, m, n, k, tc, h->workspace_bytes);
+        best = {hp.bn, hp.slices, static_cast<int>(h->group_m), 0.0f};
+        const int st = time_config(h, op_a, op_b, m, n, k, a, lda, b, ldb, c, ldc, tc, best, 1, &best.time_us);
+        if (st != SHGEMM_STATUS_OK) return st;
+    }
+    const int reps = best.time_us > 50000.0f ? 1 : 3;
+    auto consider = [&](shgemm_b200_tuned_config cand) -> int {
+        const int st = time_config(h, op_a, op_b, m, n, k, a, lda, b, ldb, c, ldc, tc, cand, reps, &cand.time_us);
+        if (st != SHGEMM_STATUS_OK) return st;
+        if (cand.time_us < best.time_us) best = cand;
+        return SHGEMM_STATUS_OK;
+    };
+    {
+        // re-time the heuristic plan with the same repetitions as the candidates
+        shgemm_b200_tuned_config heur = best;
+        best.time_us = 3.4e38f;
+        const int st = consider(heur);
+        if (st != SHGEMM_STATUS_OK) return st;
+    }
+    for (int bn : tile_ns) {
+        if (!tile_n_valid(tc, bn)) continue;
+        const long long tiles = static_cast<long long>((m + 127) / 128) * static_cast<long long>((n + bn - 1) / bn);
+        for (int sl : slice_set) {
+            if (sl > 1 && (sl > fit || steps / sl < 4 || tiles >= 2LL * h->num_sms)) continue;
+            const shgemm_b200_tuned_config cand{bn, sl, static_cast<int>(h->group_m), 0.0f};
+            if (cand.tile_n == best.tile_n && cand.slices == best.slices && cand.group_m == best.group_m) continue;
+            const int st = consider(cand);
+            if (st != SHGEMM_STATUS_OK) return st;
+        }
+    }
+    for (int gm : {2, 4, 8, 16, 32}) {
+        if (gm == best.group_m) continue;
+        const int st = consider({best.tile_n, best.slices, gm, 0.0f});
+        if (st != SHGEMM_STATUS_OK) return st;
+    }
+    {
+        std::lock_guard<std::mutex> lk(h->tune_mu);
+        h->tuned[tune_key(tc, op_a, op_b, m, n, k)] = best;
+    }
+    if (h->debug_mode)
+        std::printf("[autotune] (%zu,%zu,%zu) %s: tile = 128x%d, k_slices = %d, group_m = %d, %.1f us\n", m, n, k,
+                    tc == kTF32 ? "TF32" : "FP16", best.tile_n, best.slices, best.group_m, best.time_us);
+    if (best_out) *best_out = best;
+    return SHGEMM_STATUS_OK;
+}
+
+int shgemm_b200_autotune_lookup(shgemm_b200_handle_t h, int op_a, int op_b, size_t m, size_t n, size_t k, int tc,
+                                shgemm_b200_tuned_config* cfg) {
+    if (!h || !cfg || m == 0 || n == 0 || k == 0) return SHGEMM_STATUS_INVALID_VALUE;
+    std::lock_guard<std::mutex> lk(h->tune_mu);
+    auto it = h->tuned.find(tune_key(tc, op_a, op_b, m, n, k));
+    if (it == h->tuned.end()) return SHGEMM_STATUS_INVALID_VALUE;
+    *cfg = it->second;
+    return SHGEMM_STATUS_OK;
+}
+
+int shgemm_b200_autotune_save(shgemm_b200_handle_t h, const char* path) {
+    if (!h || !path) return SHGEMM_STATUS_INVALID_VALUE;
+    FILE* f = std::fopen(path, "w");
+    if (!f) return SHGEMM_STATUS_INVALID_VALUE;
+    std::lock_guard<std::mutex> lk(h->tune_mu);
+    std::fprintf(f, "# shgemm_b200 autotune v1: tc op_a op_b log2m log2n log2k tile_n slices group_m time_us\n");
+    for (const auto& kv : h->tuned) {
+        const uint64_t key = kv.first;
+        std::fprintf(f, "%d %d %d %d %d %d %d %d %d %.3f\n", static_cast<int>((key >> 27) & 1),
+                     static_cast<int>((key >> 26) & 1), static_cast<int>((key >> 25) & 1),
+                     static_cast<int>((key >> 16) & 0xFF), static_cast<int>((key >> 8) & 0xFF),
+                     static_cast<int>(key & 0xFF), kv.second.tile_n, kv.second.slices, kv.second.group_m,
+                     kv.second.time_us);
+    }
+    const bool ok = std::fclose(f) == 0;
+    return ok ? SHGEMM_STATUS_OK : SHGEMM_STATUS_INVALID_VALUE;
+}
+
+int shgemm_b200_autotune_load(shgemm_b200_handle_t h, const char* path) {
+    if (!h || !path) return SHGEMM_STATUS_INVALID_VALUE;
+    FILE* f = std::fopen(path, "r");
+    if (!f) return SHGEMM_STATUS_INVALID_VALUE;
+    char line[256];
+    int status = SHGEMM_STATUS_OK;
+    std::map<uint64_t, shgemm_b200_tuned_config> add;
+    while (std::fgets(line, sizeof(line), f)) {
+        if (line[0] == '#' || line[0] == '\n') continue;
+        int tc, oa, ob, lm, ln, lk, bn, sl, gm;
+        float us;
+        if (std::sscanf(line, "%d %d %d %d %d %d %d %d %d %f", &tc, &oa, &ob, &lm, &ln, &lk, &bn, &sl, &gm, &us) != 10 ||
+            (tc != kFP16 && tc != kTF32) || (oa != 0 && oa != 1) || (ob != 0 && ob != 1) || lm < 0 || lm > 40 ||
+            ln < 0 || ln > 40 || lk < 0 || lk > 40 || !tile_n_valid(tc, bn) || sl < 1 || sl > 1024 || gm < 1 ||
+            gm > 1024) {
+            status = SHGEMM_STATUS_INVALID_VALUE;
+            break;
+        }
+        const uint64_t key = (static_cast<uint64_t>(tc) << 27) | (static_cast<uint64_t>(oa) << 26) |
+                             (static_cast<uint64_t>(ob) << 25) | (static_cast<uint64_t>(lm) << 16) |
+                             (static_cast<uint64_t>(ln) << 8) | static_cast<uint64_t>(lk);
+        add[key] = {bn, sl, gm, us};
+    }
+    std::fclose(f);
+    if (status != SHGEMM_STATUS_OK) return status;
+    std::lock_guard<std::mutex> lk(h->tune_mu);
+    for (const auto& kv : add) h->tuned[kv.first] = kv.second;
+    return SHGEMM_STATUS_OK;
+}
+
+int shgemm_b200_autotune_clear(shgemm_b200_handle_t h) {
+    if (!h) return SHGEMM_STATUS_INVALID_VALUE;
+    std::lock_guard<std::mutex> lk(h->tune_mu);
+    h->tuned.clear();
     return SHGEMM_STATUS_OK;
 }
 
