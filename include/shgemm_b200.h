@@ -49,9 +49,12 @@ enum {
     SHGEMM_CFG_GROUPED_B_FP32 = 5, /* 1: grouped TF32 batches pass B as FP32 values that are
                                       exactly binary16 (a widened copy), loaded without a
                                       conversion; 0 (default): B is binary16 */
-    SHGEMM_CFG_AUTOTUNE = 6        /* 0: heuristic plans only; 1 (default): a shape whose bucket
+    SHGEMM_CFG_AUTOTUNE = 6,       /* 0: heuristic plans only; 1 (default): a shape whose bucket
                                       the autotuner has an entry for uses it; 2: as 1, and a call
                                       with beta == 0 on an untuned bucket tunes it first */
+    SHGEMM_CFG_TILE_KERNEL = 7     /* 0 (default): 128x256 binary16 tiles with a K-major B run the
+                                      kernel that keeps hi/lo in tensor memory; 1: always the
+                                      shared-memory operand kernel */
 };
 
 /* ------------------------------------------------------------------------

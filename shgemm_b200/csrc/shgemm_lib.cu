@@ -18,6 +18,7 @@
 
 #include "shgemm_b200.h"
 #include "shgemm_kernel.cuh"
+#include "shgemm_kernel_tm.cuh"
 
 using namespace shgemm_b200;
 
@@ -44,6 +45,7 @@ struct shgemm_b200_handle {
     int grouped_copied_count = 0;  // problem slots the last enqueued copy covers
     // autotuner: best (tile N, split-K slices, rasterisation group) per shape bucket
     int autotune_mode = 1;  // SHGEMM_CFG_AUTOTUNE
+    int tile_kernel = 0;    // SHGEMM_CFG_TILE_KERNEL
     std::mutex tune_mu;
     std::map<uint64_t, shgemm_b200_tuned_config> tuned;
 };
@@ -115,6 +117,12 @@ KernelEntry kernel_table(int tc, int bn, int ak, int bk) {
 #undef SHG_ENTRY4
 #undef SHG_ENTRY
     return {nullptr, 0};
+}
+
+// Tensor-memory operand kernels (binary16 compute, 128 x 256 tiles, B K-major).
+KernelEntry tm_kernel_table(bool ak) {
+    return ak ? KernelEntry{reinterpret_cast<void*>(&shgemm_tm_kernel<true>), TmCfg<true>::SMEM_BYTES}
+              : KernelEntry{reinterpret_cast<void*>(&shgemm_tm_kernel<false>), TmCfg<false>::SMEM_BYTES};
 }
 
 template <int TC, int BN, bool AK, bool BW>
@@ -532,6 +540,10 @@ int shgemm_b200_create(shgemm_b200_handle_t* out, int device) {
                         return SHGEMM_STATUS_NOT_SUPPORTED;
                     }
                 }
+    for (int ak = 0; ak < 2; ++ak) {
+        KernelEntry e = tm_kernel_table(ak != 0);
+        cudaFuncSetAttribute(e.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, e.smem);
+    }
     for (int tc = 0; tc < 2; ++tc)
         for (int ak = 0; ak < 2; ++ak)
             for (int bw = 0; bw < 2; ++bw) {
@@ -609,6 +621,10 @@ int shgemm_b200_set_config(shgemm_b200_handle_t h, int key, long long v) {
             if (v < 0 || v > 2) return SHGEMM_STATUS_INVALID_VALUE;
             h->autotune_mode = static_cast<int>(v);
             return SHGEMM_STATUS_OK;
+        case SHGEMM_CFG_TILE_KERNEL:
+            if (v < 0 || v > 1) return SHGEMM_STATUS_INVALID_VALUE;
+            h->tile_kernel = static_cast<int>(v);
+            return SHGEMM_STATUS_OK;
         default:
             return SHGEMM_STATUS_INVALID_VALUE;
     }
@@ -622,6 +638,7 @@ int shgemm_b200_get_config(shgemm_b200_handle_t h, int key, long long* v) {
         case SHGEMM_CFG_GROUP_M: *v = h->group_m; return SHGEMM_STATUS_OK;
         case SHGEMM_CFG_GROUPED_B_FP32: *v = h->grouped_b_fp32; return SHGEMM_STATUS_OK;
         case SHGEMM_CFG_AUTOTUNE: *v = h->autotune_mode; return SHGEMM_STATUS_OK;
+        case SHGEMM_CFG_TILE_KERNEL: *v = h->tile_kernel; return SHGEMM_STATUS_OK;
         default: return SHGEMM_STATUS_INVALID_VALUE;
     }
 }
@@ -700,18 +717,21 @@ static int run_tiled(shgemm_b200_handle_t h, int op_a, int op_b, size_t m, size_
     const bool a_kmajor = (op_a == kOpT);
     const bool b_kmajor = (op_b == kOpN);
     const int bk = (tc == kFP16) ? 64 : 32;
+    // binary16 compute with 128 x 256 tiles and a K-major B: the tensor-memory operand kernel
+    const bool use_tm = tc == kFP16 && pl.bn == 256 && b_kmajor && h->tile_kernel == 0;
 
     TileGemmParams P;
     std::memset(&P, 0, sizeof(P));
     bool ok;
     // FP32 operand: K-major tiles are [128 rows][32 floats] with a 128-byte swizzle;
-    // M-major tiles are [bk][a_mmajor_box(tc) floats] unswizzled.
+    // M-major tiles are [bk][box floats] unswizzled (one 128-wide box for the
+    // tensor-memory kernel, a_mmajor_box(tc) wide boxes for the others).
     if (a_kmajor)
         ok = make_tmap(&P.tmap_a, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, a, k, m, lda * 4, 32, 128,
                        CU_TENSOR_MAP_SWIZZLE_128B);
     else
-        ok = make_tmap(&P.tmap_a, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, a, m, k, lda * 4, a_mmajor_box(tc), bk,
-                       CU_TENSOR_MAP_SWIZZLE_NONE);
+        ok = make_tmap(&P.tmap_a, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, a, m, k, lda * 4, use_tm ? 128 : a_mmajor_box(tc),
+                       bk, CU_TENSOR_MAP_SWIZZLE_NONE);
     if (!ok) return SHGEMM_STATUS_NOT_SUPPORTED;
     if (tc == kFP16) {
         if (b_kmajor)
@@ -748,17 +768,18 @@ static int run_tiled(shgemm_b200_handle_t h, int op_a, int op_b, size_t m, size_
     P.num_units = pl.tiles_m * pl.tiles_n * pl.slices;
     P.group_m = group_m;
 
-    const KernelEntry e = kernel_table(tc, pl.bn, a_kmajor, b_kmajor);
+    const KernelEntry e = use_tm ? tm_kernel_table(a_kmajor) : kernel_table(tc, pl.bn, a_kmajor, b_kmajor);
+    const int threads = use_tm ? TmCfg<true>::NUM_THREADS : 512;
     if (!e.fn) return SHGEMM_STATUS_NOT_SUPPORTED;
     const int grid = std::min(P.num_units, h->num_sms);
     if (h->debug_mode) {
         std::printf("[shape=(%zu,%zu,%zu),op_a=%s,op_b=%s,compute_type=%s] kernel_level = %d, tile = 128x%d, "
-                    "k_slices = %d, chunk_k = %d, grid = %d\n",
+                    "k_slices = %d, chunk_k = %d, grid = %d%s\n",
                     m, n, k, op_a == kOpN ? "N" : "T", op_b == kOpN ? "N" : "T", tc == kTF32 ? "TF32" : "FP16",
-                    pl.level, pl.bn, pl.slices, bk, grid);
+                    pl.level, pl.bn, pl.slices, bk, grid, use_tm ? ", operands in TMEM" : "");
     }
     void* args[] = {&P};
-    cudaError_t err = cudaLaunchKernel(e.fn, dim3(grid), dim3(512), args, e.smem, h->stream);
+    cudaError_t err = cudaLaunchKernel(e.fn, dim3(grid), dim3(threads), args, e.smem, h->stream);
     h->launches++;
     if (err != cudaSuccess) {
         cudaGetLastError();
@@ -1369,6 +1390,13 @@ int noalloc_setup(int dev, NoAllocDevice*& out) {
                             return SHGEMM_STATUS_NOT_SUPPORTED;
                         }
                     }
+        for (int ak = 0; ak < 2; ++ak) {
+            KernelEntry e = tm_kernel_table(ak != 0);
+            if (cudaFuncSetAttribute(e.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, e.smem) != cudaSuccess) {
+                cudaGetLastError();
+                return SHGEMM_STATUS_NOT_SUPPORTED;
+            }
+        }
         d.num_sms = sms;
         d.scratch = static_cast<float*>(sp);
         d.error_word = static_cast<int*>(ep);

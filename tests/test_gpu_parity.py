@@ -262,3 +262,27 @@ def test_split_k_deterministic_and_matches(h, tc, op_a, op_b):
         h.set_config(sg.CFG_SPLIT_K, 0)
     K.assert_parity(K.parity_report(c3, orc, ref, sgc, m, n, inp["ldc"], 1))
     assert not np.array_equal(c1.view(np.uint32), c3.view(np.uint32))  # the split path really ran
+
+
+@pytest.mark.parametrize("op_a", [0, 1])
+@pytest.mark.parametrize("mnk", [(1000, 700, 3000), (128, 256, 64), (385, 513, 1111)])
+def test_tensor_memory_kernel_matches_shared_memory_kernel(h, op_a, mnk):
+    """The 128x256 binary16 kernel that keeps hi/lo in tensor memory computes the same
+    products in the same order as the shared-memory operand kernel: bit-identical C,
+    and within the parity bar of the restated reference."""
+    import shgemm_b200 as sg
+
+    m, n, k = mnk
+    sg.enable_kernel_level_fixing(h, 1)  # 128 x 256 tiles
+    try:
+        r_tm, c_tm, inp = _parity(h, oracle.FP16, op_a, 0, 0, m, n, k, beta=0.5, dist="wide", seed=m + op_a)
+        h.set_config(sg.CFG_TILE_KERNEL, 1)
+        try:
+            r_sm, c_sm, _ = _parity(h, oracle.FP16, op_a, 0, 0, m, n, k, beta=0.5, dist="wide", seed=m + op_a)
+        finally:
+            h.set_config(sg.CFG_TILE_KERNEL, 0)
+    finally:
+        sg.disable_kernel_level_fixing(h)
+    K.assert_parity(r_tm)
+    K.assert_parity(r_sm)
+    assert np.array_equal(c_tm.view(np.uint32), c_sm.view(np.uint32))
