@@ -9,15 +9,17 @@
 //  * the split warps read the raw FP32 tile from shared memory and write hi and lo
 //    straight into tensor memory (tcgen05.st); the MMAs take A from tensor memory, so
 //    shared memory carries only the TMA writes and the B operand reads;
-//  * each k-step runs as two N-halves of 128 columns with their own accumulators:
-//    the epilogue drains one half while the tensor core works on the other;
+//  * each k-step runs as two N-halves of 128 columns; the halves go round three
+//    128-column accumulator buffers, so a buffer's drain overlaps the next two halves'
+//    MMAs (about 1024 cycles) instead of one;
 //  * 20 warps: 8 split warps (two per TMEM lane quadrant, one per 32-k half of the
 //    step), 8 epilogue warps (two per quadrant, one per 64-column quarter of each
 //    half), a TMA producer warp and two MMA warps (one per N-half).
 //
-// Tensor memory (512 columns): accumulator of N-half h at columns [128 h, 128 h + 128);
-// operand stage t at [256 + 64 t, 256 + 64 t + 64): hi in the first 32 columns, lo in
-// the next 32 (row i in lane i, k-block kk of 16 in columns 8 kk .. 8 kk + 7).
+// Tensor memory (512 columns): accumulator buffer b at columns [128 b, 128 b + 128), b < 3,
+// used by half h of k-step s when (2 s + h) % 3 == b; operand stage t at
+// [384 + 64 t, 384 + 64 t + 64): hi in the first 32 columns, lo in the next 32 (row i in
+// lane i, k-block kk of 16 in columns 8 kk .. 8 kk + 7).
 #pragma once
 
 #include "shgemm_kernel.cuh"
@@ -32,7 +34,8 @@ struct TmCfg {
     static constexpr int BK = 64;
     static constexpr int A_STAGE = BM * BK * 4;  // raw FP32 tile
     static constexpr int B_STAGE = BN * BK * 2;  // [256 n][64 k] binary16, 128-byte swizzle
-    static constexpr int SA = 4, SB = 3, ST = 4;  // raw A, B, and tensor-memory operand stages
+    static constexpr int SA = 4, SB = 3, ST = 2;  // raw A, B, and tensor-memory operand stages
+    static constexpr int ND = 3;                   // 128-column accumulator buffers
     static constexpr int NUM_THREADS = 640;
     static constexpr int SPLIT_WARPS = 8, EPI_WARP0 = 8, CTRL_WARP0 = 16;
     // setmaxnreg shares: 2 split + 2 epilogue + 1 control warpgroup, out of the
@@ -42,7 +45,8 @@ struct TmCfg {
     static_assert(256 * SPLIT_REGS + 256 * EPI_REGS + 128 * CTRL_REGS <= NUM_THREADS * LAUNCH_REGS,
                   "register split exceeds the launch allocation");
     static constexpr int TMEM_COLS = 512;
-    static constexpr int TMEM_OPERAND0 = 256;
+    static constexpr int TMEM_OPERAND0 = ND * HALF_N;  // 384
+    static_assert(TMEM_OPERAND0 + ST * 64 <= TMEM_COLS, "tensor memory budget");
     static constexpr int BAR_BYTES = 1024;
     static constexpr int SMEM_BYTES = SA * A_STAGE + SB * B_STAGE + BAR_BYTES + 1024;
     static_assert(SMEM_BYTES <= 232448, "dynamic shared memory limit");
@@ -85,9 +89,9 @@ __device__ __forceinline__ void tm_kernel_body(const Params& p) {
     uint64_t* b_empty = b_full + SB;   // MMAs reading the B stage completed
     uint64_t* t_full = b_empty + SB;   // hi/lo operand stage written to tensor memory
     uint64_t* t_empty = t_full + ST;   // MMAs reading the operand stage completed
-    uint64_t* d_full = t_empty + ST;   // N-half accumulator ready to drain
-    uint64_t* d_empty = d_full + 2;    // N-half accumulator drained
-    uint64_t* drain_bar = d_empty + 2;  // one per MMA issuer
+    uint64_t* d_full = t_empty + ST;   // accumulator buffer ready to drain
+    uint64_t* d_empty = d_full + Cfg::ND;  // accumulator buffer drained
+    uint64_t* drain_bar = d_empty + Cfg::ND;  // one per MMA issuer
     uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(drain_bar + 2);
     volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
 
@@ -107,9 +111,9 @@ __device__ __forceinline__ void tm_kernel_body(const Params& p) {
             ptx::mbar_init(&t_full[t], Cfg::SPLIT_WARPS);
             ptx::mbar_init(&t_empty[t], 2);  // both MMA issuers' commits
         }
-        for (int h = 0; h < 2; ++h) {
-            ptx::mbar_init(&d_full[h], 1);
-            ptx::mbar_init(&d_empty[h], 8);
+        for (int b = 0; b < Cfg::ND; ++b) {
+            ptx::mbar_init(&d_full[b], 1);
+            ptx::mbar_init(&d_empty[b], 8);
         }
         ptx::mbar_init(&drain_bar[0], 1);
         ptx::mbar_init(&drain_bar[1], 1);
@@ -220,7 +224,9 @@ __device__ __forceinline__ void tm_kernel_body(const Params& p) {
             for (int i = 0; i < nsteps; ++i) {
 #pragma unroll
                 for (int h = 0; h < 2; ++h) {
-                    if (!ptx::mbar_wait(&d_full[h], gc & 1u, abort_flag, limit)) {
+                    // half h of step gc is use (2 gc + h) / ND of buffer (2 gc + h) % ND
+                    const uint32_t g = 2 * gc + h, buf = g % Cfg::ND;
+                    if (!ptx::mbar_wait(&d_full[buf], (g / Cfg::ND) & 1u, abort_flag, limit)) {
                         fail(kErrEpilogueTimeout);
                         goto epi_done;
                     }
@@ -228,7 +234,7 @@ __device__ __forceinline__ void tm_kernel_body(const Params& p) {
 #pragma unroll
                     for (int j0 = 0; j0 < 64; j0 += 32) {
                         uint32_t r0[16], r1[16];
-                        const uint32_t ta = tmem_base + lane_addr + h * Cfg::HALF_N + cq * 64 + j0;
+                        const uint32_t ta = tmem_base + lane_addr + buf * Cfg::HALF_N + cq * 64 + j0;
                         ptx::tmem_ld_32x32b_x16(ta, r0);
                         ptx::tmem_ld_32x32b_x16(ta + 16, r1);
                         ptx::tmem_ld_wait();
@@ -242,7 +248,7 @@ __device__ __forceinline__ void tm_kernel_body(const Params& p) {
                     }
                     ptx::tc_fence_before();
                     __syncwarp();
-                    if (lane == 0) ptx::mbar_arrive(&d_empty[h]);
+                    if (lane == 0) ptx::mbar_arrive(&d_empty[buf]);
                 }
                 ++gc;
             }
@@ -368,7 +374,6 @@ __device__ __forceinline__ void tm_kernel_body(const Params& p) {
             int ts = 0, bs = 0;
             uint32_t tph = 0, bph = 0, gc = 0;
             bool issued_any = false;
-            const uint32_t d = tmem_base + h * Cfg::HALF_N;
             for (int u = blockIdx.x; u < num_units; u += gridDim.x) {
                 UnitDesc ud;
                 get_unit<Cfg>(p, u, ud);
@@ -376,7 +381,8 @@ __device__ __forceinline__ void tm_kernel_body(const Params& p) {
                 for (int i = 0; i < nsteps; ++i) {
                     if (!ptx::mbar_wait(&t_full[ts], tph, abort_flag, limit) ||
                         !ptx::mbar_wait(&b_full[bs], bph, abort_flag, limit) ||
-                        !ptx::mbar_wait(&d_empty[h], (gc & 1u) ^ 1u, abort_flag, limit)) {
+                        !ptx::mbar_wait(&d_empty[(2 * gc + h) % Cfg::ND], (((2 * gc + h) / Cfg::ND) & 1u) ^ 1u,
+                                        abort_flag, limit)) {
                         fail(kErrMmaTimeout);
                         goto mma_done;
                     }
@@ -384,6 +390,7 @@ __device__ __forceinline__ void tm_kernel_body(const Params& p) {
                     {
                         // rows 128 h .. 128 h + 127 of the [256 n][64 k] B stage
                         const uint32_t b_s = ptx::smem_u32(b_base + bs * Cfg::B_STAGE) + h * (Cfg::HALF_N * 128);
+                        const uint32_t d = tmem_base + ((2 * gc + h) % Cfg::ND) * Cfg::HALF_N;
                         const uint32_t a_hi = tmem_base + Cfg::TMEM_OPERAND0 + ts * 64;
                         const uint32_t a_lo = a_hi + 32;
                         auto bd = [&](int kk) -> uint64_t {
@@ -398,7 +405,7 @@ __device__ __forceinline__ void tm_kernel_body(const Params& p) {
                         for (int kk = 1; kk < 4; ++kk) ptx::umma_f16_ts(d, a_hi + kk * 8, bd(kk), idesc, 1u);
                     }
                     issued_any = true;
-                    ptx::umma_commit(&d_full[h]);
+                    ptx::umma_commit(&d_full[(2 * gc + h) % Cfg::ND]);
                     ptx::umma_commit(&t_empty[ts]);
                     ptx::umma_commit(&b_empty[bs]);
                     if (++ts == ST) {
