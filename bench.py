@@ -670,6 +670,8 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer end-to-end measurement")
     ap.add_argument("--no-autotune", action="store_true", help="plain workloads: use the heuristic plan")
+    ap.add_argument("--k-chunk", type=int, default=64, choices=[64, 128],
+                    help="k between FP32 drains in the tensor-memory kernel (SHGEMM_CFG_K_CHUNK)")
     ap.add_argument("--rate", type=float, default=None, help="served: arrivals per second")
     ap.add_argument("--duration", type=float, default=None, help="served: seconds of arrivals")
     args = ap.parse_args()
@@ -712,6 +714,7 @@ def main():
     A, lda, B, ldb, C, ldc = make_inputs(wl, dev, seed=rank)
     C0 = C.clone() if wl["beta"] != 0 else None
 
+    h.set_config(sg.CFG_K_CHUNK, args.k_chunk)
     # one-off autotune of the shape's bucket (not timed); C is overwritten by it, then restored
     tuned = None
     if not args.no_autotune and op_c == 0:
@@ -848,7 +851,8 @@ def main():
             "data": "synthetic (seeded, workload's shapes and distributions)",
             "config": {"workload": wl["desc"], "m": m, "n": n, "k": k, "op_a": "NT"[wl["op_a"]],
                        "op_b": "NT"[wl["op_b"]], "op_c": "NT"[op_c], "compute_type": ["fp16", "tf32"][wl["tc"]],
-                       "kernel_level": level, "autotuned": tuned, "l2": "inputs exceed L2 (no flush needed)",
+                       "kernel_level": level, "autotuned": tuned, "k_chunk": args.k_chunk,
+                       "l2": "inputs exceed L2 (no flush needed)",
                        "parallelism": f"replicas x{world}"},
             "issued_tflops": world * flops_issued * args.steps / (ms_total * 1e-3) / 1e12,
             "gpu_launches": launches,

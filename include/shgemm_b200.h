@@ -52,9 +52,14 @@ enum {
     SHGEMM_CFG_AUTOTUNE = 6,       /* 0: heuristic plans only; 1 (default): a shape whose bucket
                                       the autotuner has an entry for uses it; 2: as 1, and a call
                                       with beta == 0 on an untuned bucket tunes it first */
-    SHGEMM_CFG_TILE_KERNEL = 7     /* 0 (default): 128x256 binary16 tiles with a K-major B run the
+    SHGEMM_CFG_TILE_KERNEL = 7,    /* 0 (default): 128x256 binary16 tiles with a K-major B run the
                                       kernel that keeps hi/lo in tensor memory; 1: always the
                                       shared-memory operand kernel */
+    SHGEMM_CFG_K_CHUNK = 8         /* k between FP32 round-to-nearest drains of the tensor-core
+                                      accumulator in the tensor-memory kernel: 64 (default) or
+                                      128 (measured: ~1.2x the 64-k error on mixed-sign data,
+                                      ~2.2x on all-positive data, within 2x FP32 SGEMM's error);
+                                      the other kernels always drain every 64 */
 };
 
 /* ------------------------------------------------------------------------

@@ -24,7 +24,8 @@ op_n, op_t = 0, 1          # operation_t (include/shgemm/shgemm.hpp:36-39)
 fp16, tf32 = 0, 1          # tc_t (include/shgemm/shgemm.hpp:41-44)
 P0, P1 = 0, 1              # detail::kernel_level (include/shgemm/shgemm.hpp:30-34)
 
-CFG_SPLIT_K, CFG_WAIT_LIMIT_MS, CFG_GROUP_M, CFG_GROUPED_B_FP32, CFG_AUTOTUNE, CFG_TILE_KERNEL = 2, 3, 4, 5, 6, 7
+CFG_SPLIT_K, CFG_WAIT_LIMIT_MS, CFG_GROUP_M, CFG_GROUPED_B_FP32, CFG_AUTOTUNE, CFG_TILE_KERNEL, CFG_K_CHUNK = (
+    2, 3, 4, 5, 6, 7, 8)
 
 STATUS = {0: "OK", 1: "INVALID_VALUE", 2: "NOT_SUPPORTED", 3: "ALLOC_FAILED", 4: "LAUNCH_FAILED",
           5: "TIMEOUT", 6: "CUDA_ERROR", 7: "SCRATCH_TOO_SMALL"}

@@ -244,6 +244,12 @@ __device__ __forceinline__ void tmem_ld_32x32b_x16(uint32_t taddr, uint32_t (&r)
         : "memory");
 }
 
+// Brings the line holding `addr` into L2 with the evict-last priority, so streaming
+// operand traffic does not push it out before it is used.
+__device__ __forceinline__ void prefetch_l2_evict_last(const void* addr) {
+    asm volatile("prefetch.global.L2::evict_last [%0];" ::"l"(reinterpret_cast<uint64_t>(addr)));
+}
+
 __device__ __forceinline__ void tmem_ld_wait() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
 
 // 32 lanes x 8 consecutive 32-bit columns from registers: thread i writes lane (base lane + i).

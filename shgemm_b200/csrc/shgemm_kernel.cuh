@@ -233,6 +233,50 @@ __device__ __forceinline__ void prefetch_params_maps(const TileGemmParams& p) {
 __device__ __forceinline__ void prefetch_params_maps(const GroupedParams&) {}
 
 // ---------------------------------------------------------------------------
+// Epilogue helpers.
+// Element (row, col) of C: column-major (op_c = N) or stored transposed (op_c = T).
+__device__ __forceinline__ float* c_elem(float* c, uint64_t ldc, int op_c, int row, int col) {
+    return op_c == kOpN ? c + row + static_cast<size_t>(col) * ldc : c + static_cast<size_t>(row) * ldc + col;
+}
+
+// C(row, col0 .. col0 + NC - 1) = alpha * acc(j) + beta * C (C not read when beta == 0);
+// columns at or past n are skipped. With beta != 0 the C values of 4 columns are loaded
+// before any of them is written, so the loads' latencies overlap instead of adding up.
+template <int NC, class AccFn>
+__device__ __forceinline__ void store_row(float* c, uint64_t ldc, int op_c, int row, int col0, int n, float alpha,
+                                          float beta, AccFn&& acc) {
+    const size_t stride = op_c == kOpN ? ldc : 1;
+    float* p = c_elem(c, ldc, op_c, row, col0);
+    if (beta == 0.0f) {
+#pragma unroll
+        for (int j = 0; j < NC; ++j)
+            if (col0 + j < n) p[j * stride] = __fmul_rn(acc(j), alpha);
+        return;
+    }
+#pragma unroll
+    for (int jb = 0; jb < NC; jb += 4) {
+        float cv[4];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) cv[j] = (col0 + jb + j < n) ? p[(jb + j) * stride] : 0.0f;
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+            if (col0 + jb + j < n) p[(jb + j) * stride] = __fmaf_rn(acc(jb + j), alpha, __fmul_rn(beta, cv[j]));
+    }
+}
+
+// Asks L2 to fetch and keep the lines of C(row, col0 .. col0 + NC - 1) ahead of a
+// beta != 0 epilogue.
+template <int NC>
+__device__ __forceinline__ void prefetch_row(float* c, uint64_t ldc, int op_c, int row, int col0, int n) {
+    // op_c = N: a warp's 32 consecutive rows share each column's line; T: a row's columns
+    // are contiguous, one line per 32 columns
+    const int step = op_c == kOpN ? 1 : 32;
+#pragma unroll 1
+    for (int j = 0; j < NC; j += step)
+        if (col0 + j < n) ptx::prefetch_l2_evict_last(c_elem(c, ldc, op_c, row, col0 + j));
+}
+
+// ---------------------------------------------------------------------------
 // Split helpers. hi = T(v), lo = T(2^11 (v - hi)), T = binary16 round-to-nearest-
 // even or TF32 round-to-nearest-away: the reference's split (src/wmmae_shgemm.hpp:30-31).
 __device__ __forceinline__ void split8_f16(const float (&v)[8], uint4& hi, uint4& lo) {
@@ -844,6 +888,11 @@ __device__ __forceinline__ void tile_kernel_body(const Params& p) {
                 get_unit<Cfg>(p, u, ud);
                 nsteps = ud.s1 - ud.s0;
                 hn = ud.bn / 2;  // columns of this warp's half (<= HN)
+                // beta != 0: C of this thread's row into L2 (kept there) while the tile's k-steps run
+                const int row = ud.tm * Cfg::BM + row_in_tile;
+                const int col0 = ud.tn * ud.bn + half * hn;
+                if (ud.beta != 0.0f && !ud.partial && row < ud.m)
+                    prefetch_row<HN>(ud.c, ud.ldc, output_op(p), row, col0, ud.n < col0 + hn ? ud.n : col0 + hn);
             }
             uint64_t acc2[HN / 2];  // running sums, packed in pairs of columns
 #pragma unroll
@@ -892,28 +941,10 @@ __device__ __forceinline__ void tile_kernel_body(const Params& p) {
                             const int col = col0 + j;
                             if (j < hn && col < ud.n) w[static_cast<size_t>(col) * ud.m] = acc(j);
                         }
-                    } else if (output_op(p) == kOpN) {
-                        float* cp = ud.c + row;
-#pragma unroll
-                        for (int j = 0; j < HN; ++j) {
-                            const int col = col0 + j;
-                            if (j < hn && col < ud.n) {
-                                float* dst = cp + static_cast<size_t>(col) * ud.ldc;
-                                *dst = (ud.beta == 0.0f) ? __fmul_rn(acc(j), ud.alpha)
-                                                         : __fmaf_rn(acc(j), ud.alpha, __fmul_rn(ud.beta, *dst));
-                            }
-                        }
                     } else {
-                        float* cp = ud.c + static_cast<size_t>(row) * ud.ldc;
-#pragma unroll
-                        for (int j = 0; j < HN; ++j) {
-                            const int col = col0 + j;
-                            if (j < hn && col < ud.n) {
-                                float* dst = cp + col;
-                                *dst = (ud.beta == 0.0f) ? __fmul_rn(acc(j), ud.alpha)
-                                                         : __fmaf_rn(acc(j), ud.alpha, __fmul_rn(ud.beta, *dst));
-                            }
-                        }
+                        // columns of this warp's half only (a grouped problem's tile may be narrower)
+                        const int n_end = ud.n < col0 + hn ? ud.n : col0 + hn;
+                        store_row<HN>(ud.c, ud.ldc, output_op(p), row, col0, n_end, ud.alpha, ud.beta, acc);
                     }
                 }
             }

@@ -26,7 +26,8 @@
 
 namespace shgemm_b200 {
 
-template <bool A_KMAJOR>
+// KC: k-steps of 64 per FP32 drain (1: every 64 k; 2: every 128 k).
+template <bool A_KMAJOR, int KC = 1>
 struct TmCfg {
     static constexpr int BM = 128;
     static constexpr int BN = 256;
@@ -34,8 +35,11 @@ struct TmCfg {
     static constexpr int BK = 64;
     static constexpr int A_STAGE = BM * BK * 4;  // raw FP32 tile
     static constexpr int B_STAGE = BN * BK * 2;  // [256 n][64 k] binary16, 128-byte swizzle
-    static constexpr int SA = 4, SB = 3, ST = 2;  // raw A, B, and tensor-memory operand stages
-    static constexpr int ND = 3;                   // 128-column accumulator buffers
+    // raw A, B and tensor-memory operand stages; 128-column accumulator buffers: a chunk of
+    // 2 k-steps holds 2 operand stages while its MMAs run, so it takes 4 stages and 2 buffers
+    static constexpr int SA = 4, SB = 3, ST = KC == 1 ? 2 : 4;
+    static constexpr int ND = KC == 1 ? 3 : 2;
+    static_assert(KC == 1 || KC == 2, "k-chunk");
     static constexpr int NUM_THREADS = 640;
     static constexpr int SPLIT_WARPS = 8, EPI_WARP0 = 8, CTRL_WARP0 = 16;
     // setmaxnreg shares: 2 split + 2 epilogue + 1 control warpgroup, out of the
@@ -72,9 +76,9 @@ __device__ __forceinline__ void split16_f16(const float (&v)[16], uint32_t (&hw)
     }
 }
 
-template <bool A_KMAJOR, class Params>
+template <bool A_KMAJOR, int KC, class Params>
 __device__ __forceinline__ void tm_kernel_body(const Params& p) {
-    using Cfg = TmCfg<A_KMAJOR>;
+    using Cfg = TmCfg<A_KMAJOR, KC>;
     constexpr int SA = Cfg::SA, SB = Cfg::SB, ST = Cfg::ST;
 
     extern __shared__ uint8_t smem_raw[];
@@ -217,14 +221,22 @@ __device__ __forceinline__ void tm_kernel_body(const Params& p) {
                 UnitDesc ud;
                 get_unit<Cfg>(p, u, ud);
                 nsteps = ud.s1 - ud.s0;
+                // beta != 0: C of this thread's row into L2 (kept there) while the tile's k-steps run
+                const int row = ud.tm * Cfg::BM + row_in_tile;
+                if (ud.beta != 0.0f && !ud.partial && row < ud.m) {
+#pragma unroll
+                    for (int h = 0; h < 2; ++h)
+                        prefetch_row<64>(ud.c, ud.ldc, output_op(p), row, ud.tn * Cfg::BN + h * Cfg::HALF_N + cq * 64,
+                                         ud.n);
+                }
             }
             uint64_t acc2[64];  // [half][32 column pairs]
 #pragma unroll
             for (int j = 0; j < 64; ++j) acc2[j] = 0ull;
-            for (int i = 0; i < nsteps; ++i) {
+            for (int i = 0; i < nsteps; i += KC) {
 #pragma unroll
                 for (int h = 0; h < 2; ++h) {
-                    // half h of step gc is use (2 gc + h) / ND of buffer (2 gc + h) % ND
+                    // half h of k-chunk gc is use (2 gc + h) / ND of buffer (2 gc + h) % ND
                     const uint32_t g = 2 * gc + h, buf = g % Cfg::ND;
                     if (!ptx::mbar_wait(&d_full[buf], (g / Cfg::ND) & 1u, abort_flag, limit)) {
                         fail(kErrEpilogueTimeout);
@@ -268,28 +280,9 @@ __device__ __forceinline__ void tm_kernel_body(const Params& p) {
                                 const int col = col0 + j;
                                 if (col < ud.n) w[static_cast<size_t>(col) * ud.m] = acc(h * 64 + j);
                             }
-                        } else if (output_op(p) == kOpN) {
-                            float* cp = ud.c + row;
-#pragma unroll
-                            for (int j = 0; j < 64; ++j) {
-                                const int col = col0 + j;
-                                if (col < ud.n) {
-                                    float* dst = cp + static_cast<size_t>(col) * ud.ldc;
-                                    *dst = (ud.beta == 0.0f) ? __fmul_rn(acc(h * 64 + j), ud.alpha)
-                                                             : __fmaf_rn(acc(h * 64 + j), ud.alpha, __fmul_rn(ud.beta, *dst));
-                                }
-                            }
                         } else {
-                            float* cp = ud.c + static_cast<size_t>(row) * ud.ldc;
-#pragma unroll
-                            for (int j = 0; j < 64; ++j) {
-                                const int col = col0 + j;
-                                if (col < ud.n) {
-                                    float* dst = cp + col;
-                                    *dst = (ud.beta == 0.0f) ? __fmul_rn(acc(h * 64 + j), ud.alpha)
-                                                             : __fmaf_rn(acc(h * 64 + j), ud.alpha, __fmul_rn(ud.beta, *dst));
-                                }
-                            }
+                            store_row<64>(ud.c, ud.ldc, output_op(p), row, col0, ud.n, ud.alpha, ud.beta,
+                                          [&](int j) { return acc(h * 64 + j); });
                         }
                     }
                 }
@@ -372,49 +365,85 @@ __device__ __forceinline__ void tm_kernel_body(const Params& p) {
             const int h = warp - (Cfg::CTRL_WARP0 + 1);
             constexpr uint32_t idesc = ptx::make_idesc(false, false, false, Cfg::BM, Cfg::HALF_N);
             int ts = 0, bs = 0;
-            uint32_t tph = 0, bph = 0, gc = 0;
+            uint32_t tph = 0, bph = 0, gc = 0;  // gc counts k-chunks
             bool issued_any = false;
             for (int u = blockIdx.x; u < num_units; u += gridDim.x) {
                 UnitDesc ud;
                 get_unit<Cfg>(p, u, ud);
                 const int nsteps = ud.s1 - ud.s0;
-                for (int i = 0; i < nsteps; ++i) {
-                    if (!ptx::mbar_wait(&t_full[ts], tph, abort_flag, limit) ||
-                        !ptx::mbar_wait(&b_full[bs], bph, abort_flag, limit) ||
-                        !ptx::mbar_wait(&d_empty[(2 * gc + h) % Cfg::ND], (((2 * gc + h) / Cfg::ND) & 1u) ^ 1u,
-                                        abort_flag, limit)) {
+                for (int i = 0; i < nsteps; i += KC) {
+                    const int c = nsteps - i < KC ? nsteps - i : KC;  // k-steps in this chunk
+                    const uint32_t buf = (2 * gc + h) % Cfg::ND;
+                    int tsj[KC], bsj[KC];
+                    bool ok = true;
+                    {
+                        int t = ts, b = bs;
+                        uint32_t tp = tph, bp = bph;
+#pragma unroll
+                        for (int j = 0; j < KC; ++j) {
+                            tsj[j] = t;
+                            bsj[j] = b;
+                            if (j < c) {
+                                ok = ok && ptx::mbar_wait(&t_full[t], tp, abort_flag, limit) &&
+                                     ptx::mbar_wait(&b_full[b], bp, abort_flag, limit);
+                                if (++t == ST) {
+                                    t = 0;
+                                    tp ^= 1u;
+                                }
+                                if (++b == SB) {
+                                    b = 0;
+                                    bp ^= 1u;
+                                }
+                            }
+                        }
+                        ts = t;
+                        tph = tp;
+                        bs = b;
+                        bph = bp;
+                    }
+                    ok = ok && ptx::mbar_wait(&d_empty[buf], (((2 * gc + h) / Cfg::ND) & 1u) ^ 1u, abort_flag, limit);
+                    if (!ok) {
                         fail(kErrMmaTimeout);
                         goto mma_done;
                     }
                     ptx::tc_fence_after();
                     {
-                        // rows 128 h .. 128 h + 127 of the [256 n][64 k] B stage
-                        const uint32_t b_s = ptx::smem_u32(b_base + bs * Cfg::B_STAGE) + h * (Cfg::HALF_N * 128);
-                        const uint32_t d = tmem_base + ((2 * gc + h) % Cfg::ND) * Cfg::HALF_N;
-                        const uint32_t a_hi = tmem_base + Cfg::TMEM_OPERAND0 + ts * 64;
-                        const uint32_t a_lo = a_hi + 32;
-                        auto bd = [&](int kk) -> uint64_t {
-                            return ptx::make_smem_desc(b_s + kk * 32, 16, 1024, ptx::kLayoutSW128);
+                        const uint32_t d = tmem_base + buf * Cfg::HALF_N;
+                        // rows 128 h .. 128 h + 127 of the [256 n][64 k] B stage of step j of the chunk
+                        auto bd = [&](int j, int kk) -> uint64_t {
+                            return ptx::make_smem_desc(ptx::smem_u32(b_base + bsj[j] * Cfg::B_STAGE) +
+                                                           h * (Cfg::HALF_N * 128) + kk * 32,
+                                                       16, 1024, ptx::kLayoutSW128);
                         };
-                        // lo products into a fresh accumulator ...
+                        auto a_hi = [&](int j) -> uint32_t { return tmem_base + Cfg::TMEM_OPERAND0 + tsj[j] * 64; };
+                        // the chunk's lo products into a fresh accumulator ...
 #pragma unroll
-                        for (int kk = 0; kk < 4; ++kk) ptx::umma_f16_ts(d, a_lo + kk * 8, bd(kk), idesc, kk > 0 ? 1u : 0u);
+                        for (int j = 0; j < KC; ++j) {
+                            if (j < c) {
+#pragma unroll
+                                for (int kk = 0; kk < 4; ++kk)
+                                    ptx::umma_f16_ts(d, a_hi(j) + 32 + kk * 8, bd(j, kk), idesc, (j > 0 || kk > 0) ? 1u : 0u);
+                            }
+                        }
                         // ... scaled by 2^-11 under the first hi product, then the other hi products
-                        ptx::umma_f16_ts_scale11(d, a_hi, bd(0), idesc);
+                        ptx::umma_f16_ts_scale11(d, a_hi(0), bd(0, 0), idesc);
 #pragma unroll
-                        for (int kk = 1; kk < 4; ++kk) ptx::umma_f16_ts(d, a_hi + kk * 8, bd(kk), idesc, 1u);
+                        for (int j = 0; j < KC; ++j) {
+                            if (j < c) {
+#pragma unroll
+                                for (int kk = (j == 0 ? 1 : 0); kk < 4; ++kk)
+                                    ptx::umma_f16_ts(d, a_hi(j) + kk * 8, bd(j, kk), idesc, 1u);
+                            }
+                        }
                     }
                     issued_any = true;
-                    ptx::umma_commit(&d_full[(2 * gc + h) % Cfg::ND]);
-                    ptx::umma_commit(&t_empty[ts]);
-                    ptx::umma_commit(&b_empty[bs]);
-                    if (++ts == ST) {
-                        ts = 0;
-                        tph ^= 1u;
-                    }
-                    if (++bs == SB) {
-                        bs = 0;
-                        bph ^= 1u;
+                    ptx::umma_commit(&d_full[buf]);
+#pragma unroll
+                    for (int j = 0; j < KC; ++j) {
+                        if (j < c) {
+                            ptx::umma_commit(&t_empty[tsj[j]]);
+                            ptx::umma_commit(&b_empty[bsj[j]]);
+                        }
                     }
                     ++gc;
                 }
@@ -440,9 +469,9 @@ __device__ __forceinline__ void tm_kernel_body(const Params& p) {
     if (warp == Cfg::CTRL_WARP0) ptx::tmem_dealloc(tmem_base, Cfg::TMEM_COLS);
 }
 
-template <bool A_KMAJOR>
+template <bool A_KMAJOR, int KC>
 __global__ void __launch_bounds__(640, 1) shgemm_tm_kernel(const __grid_constant__ TileGemmParams p) {
-    tm_kernel_body<A_KMAJOR>(p);
+    tm_kernel_body<A_KMAJOR, KC>(p);
 }
 
 }  // namespace shgemm_b200

@@ -46,6 +46,7 @@ struct shgemm_b200_handle {
     // autotuner: best (tile N, split-K slices, rasterisation group) per shape bucket
     int autotune_mode = 1;  // SHGEMM_CFG_AUTOTUNE
     int tile_kernel = 0;    // SHGEMM_CFG_TILE_KERNEL
+    int k_chunk = 64;       // SHGEMM_CFG_K_CHUNK
     std::mutex tune_mu;
     std::map<uint64_t, shgemm_b200_tuned_config> tuned;
 };
@@ -120,9 +121,14 @@ KernelEntry kernel_table(int tc, int bn, int ak, int bk) {
 }
 
 // Tensor-memory operand kernels (binary16 compute, 128 x 256 tiles, B K-major).
-KernelEntry tm_kernel_table(bool ak) {
-    return ak ? KernelEntry{reinterpret_cast<void*>(&shgemm_tm_kernel<true>), TmCfg<true>::SMEM_BYTES}
-              : KernelEntry{reinterpret_cast<void*>(&shgemm_tm_kernel<false>), TmCfg<false>::SMEM_BYTES};
+template <bool AK, int KC>
+KernelEntry tm_entry() {
+    return {reinterpret_cast<void*>(&shgemm_tm_kernel<AK, KC>), TmCfg<AK, KC>::SMEM_BYTES};
+}
+// kc: k-steps of 64 per FP32 drain (1 or 2)
+KernelEntry tm_kernel_table(bool ak, int kc) {
+    if (kc == 2) return ak ? tm_entry<true, 2>() : tm_entry<false, 2>();
+    return ak ? tm_entry<true, 1>() : tm_entry<false, 1>();
 }
 
 template <int TC, int BN, bool AK, bool BW>
@@ -541,8 +547,10 @@ int shgemm_b200_create(shgemm_b200_handle_t* out, int device) {
                     }
                 }
     for (int ak = 0; ak < 2; ++ak) {
-        KernelEntry e = tm_kernel_table(ak != 0);
-        cudaFuncSetAttribute(e.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, e.smem);
+        for (int kc = 1; kc <= 2; ++kc) {
+            KernelEntry e = tm_kernel_table(ak != 0, kc);
+            cudaFuncSetAttribute(e.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, e.smem);
+        }
     }
     for (int tc = 0; tc < 2; ++tc)
         for (int ak = 0; ak < 2; ++ak)
@@ -625,6 +633,10 @@ int shgemm_b200_set_config(shgemm_b200_handle_t h, int key, long long v) {
             if (v < 0 || v > 1) return SHGEMM_STATUS_INVALID_VALUE;
             h->tile_kernel = static_cast<int>(v);
             return SHGEMM_STATUS_OK;
+        case SHGEMM_CFG_K_CHUNK:
+            if (v != 64 && v != 128) return SHGEMM_STATUS_INVALID_VALUE;
+            h->k_chunk = static_cast<int>(v);
+            return SHGEMM_STATUS_OK;
         default:
             return SHGEMM_STATUS_INVALID_VALUE;
     }
@@ -639,6 +651,7 @@ int shgemm_b200_get_config(shgemm_b200_handle_t h, int key, long long* v) {
         case SHGEMM_CFG_GROUPED_B_FP32: *v = h->grouped_b_fp32; return SHGEMM_STATUS_OK;
         case SHGEMM_CFG_AUTOTUNE: *v = h->autotune_mode; return SHGEMM_STATUS_OK;
         case SHGEMM_CFG_TILE_KERNEL: *v = h->tile_kernel; return SHGEMM_STATUS_OK;
+        case SHGEMM_CFG_K_CHUNK: *v = h->k_chunk; return SHGEMM_STATUS_OK;
         default: return SHGEMM_STATUS_INVALID_VALUE;
     }
 }
@@ -768,7 +781,7 @@ static int run_tiled(shgemm_b200_handle_t h, int op_a, int op_b, size_t m, size_
     P.num_units = pl.tiles_m * pl.tiles_n * pl.slices;
     P.group_m = group_m;
 
-    const KernelEntry e = use_tm ? tm_kernel_table(a_kmajor) : kernel_table(tc, pl.bn, a_kmajor, b_kmajor);
+    const KernelEntry e = use_tm ? tm_kernel_table(a_kmajor, h->k_chunk / 64) : kernel_table(tc, pl.bn, a_kmajor, b_kmajor);
     const int threads = use_tm ? TmCfg<true>::NUM_THREADS : 512;
     if (!e.fn) return SHGEMM_STATUS_NOT_SUPPORTED;
     const int grid = std::min(P.num_units, h->num_sms);
@@ -776,7 +789,7 @@ static int run_tiled(shgemm_b200_handle_t h, int op_a, int op_b, size_t m, size_
         std::printf("[shape=(%zu,%zu,%zu),op_a=%s,op_b=%s,compute_type=%s] kernel_level = %d, tile = 128x%d, "
                     "k_slices = %d, chunk_k = %d, grid = %d%s\n",
                     m, n, k, op_a == kOpN ? "N" : "T", op_b == kOpN ? "N" : "T", tc == kTF32 ? "TF32" : "FP16",
-                    pl.level, pl.bn, pl.slices, bk, grid, use_tm ? ", operands in TMEM" : "");
+                    pl.level, pl.bn, pl.slices, use_tm ? h->k_chunk : bk, grid, use_tm ? ", operands in TMEM" : "");
     }
     void* args[] = {&P};
     cudaError_t err = cudaLaunchKernel(e.fn, dim3(grid), dim3(threads), args, e.smem, h->stream);
@@ -1391,10 +1404,12 @@ int noalloc_setup(int dev, NoAllocDevice*& out) {
                         }
                     }
         for (int ak = 0; ak < 2; ++ak) {
-            KernelEntry e = tm_kernel_table(ak != 0);
-            if (cudaFuncSetAttribute(e.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, e.smem) != cudaSuccess) {
-                cudaGetLastError();
-                return SHGEMM_STATUS_NOT_SUPPORTED;
+            for (int kc = 1; kc <= 2; ++kc) {
+                KernelEntry e = tm_kernel_table(ak != 0, kc);
+                if (cudaFuncSetAttribute(e.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, e.smem) != cudaSuccess) {
+                    cudaGetLastError();
+                    return SHGEMM_STATUS_NOT_SUPPORTED;
+                }
             }
         }
         d.num_sms = sms;
