@@ -715,6 +715,9 @@ def main():
     C0 = C.clone() if wl["beta"] != 0 else None
 
     h.set_config(sg.CFG_K_CHUNK, args.k_chunk)
+    if wl["tc"] == 1 and wl["op_b"] == 0:
+        # room for the widened FP32 copy of B (the TF32 route that loads B unconverted)
+        h.set_workspace_size(max(64 << 20, n * ((k + 3) // 4 * 4) * 4 + (1 << 20)))
     # one-off autotune of the shape's bucket (not timed); C is overwritten by it, then restored
     tuned = None
     if not args.no_autotune and op_c == 0:

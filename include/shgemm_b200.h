@@ -114,7 +114,10 @@ int shgemm_b200_set_debug_mode(shgemm_b200_handle_t handle, unsigned on);
 
 /* mtk::shgemm::shgemm (include/shgemm/shgemm.hpp:105-119; src/shgemm.cu:517-686):
  * C = alpha * op(A) * op(B) + beta * C, A FP32, B binary16 (`b` points to __half),
- * op_c == SHGEMM_OP_T stores C transposed. *level_out (may be NULL) receives the
+ * op_c == SHGEMM_OP_T stores C transposed. TF32 calls with a K-contiguous B whose
+ * 128 x 256 tiles fill the GPU and whose widened B (n * round4(k) floats) fits the handle
+ * workspace widen B there first and run the TF32 kernel that loads it unconverted
+ * (not while capturing). *level_out (may be NULL) receives the
  * kernel level used, like the reference's return value. */
 int shgemm_b200_shgemm(shgemm_b200_handle_t handle, int op_a, int op_b, size_t m, size_t n, size_t k,
                        const float* alpha, const float* a, size_t lda, const void* b, size_t ldb,
@@ -159,7 +162,9 @@ int shgemm_b200_shgemm_grouped(shgemm_b200_handle_t handle, int op_a, int op_b, 
 /* Rewrites the pinned host staging with a new batch without enqueueing anything
  * (for replaying a captured grouped launch). The batch must use the op_a,
  * compute type and op_c the launch was captured with, and no replay of that
- * launch may still be pending (its copy reads the staging): synchronise first. */
+ * launch may still be pending (its copy reads the staging): synchronise first.
+ * Every grouped call restages the table, and so does an eager TF32 shgemm call that
+ * takes the widened-B route (see shgemm_b200_shgemm): update before each replay. */
 int shgemm_b200_grouped_update(shgemm_b200_handle_t handle, int op_a, int op_b, int compute_type, int op_c,
                                const shgemm_b200_problem* problems, int count);
 

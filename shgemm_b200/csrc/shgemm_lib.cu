@@ -182,6 +182,18 @@ __global__ void pack_kernel(const T* __restrict__ src, uint64_t ld_src, T* __res
     }
 }
 
+// Widens a k x n binary16 K-contiguous operand (leading dimension ldb) to FP32 with
+// leading dimension ld_dst (the B operand of the TF32 kernels that load it unconverted).
+__global__ void widen_b_kernel(const __half* __restrict__ src, uint64_t ldb, float* __restrict__ dst,
+                               uint64_t ld_dst, int k, int n) {
+    const size_t total = static_cast<size_t>(k) * n;
+    for (size_t idx = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; idx < total;
+         idx += static_cast<size_t>(gridDim.x) * blockDim.x) {
+        const size_t r = idx % k, c = idx / k;
+        dst[r + c * ld_dst] = __half2float(src[r + c * ldb]);
+    }
+}
+
 // Deterministic split-K reduction: slices summed in fixed order 0..S-1, then the
 // same alpha/beta epilogue as the tile kernel (C is not read when beta == 0).
 __global__ void splitk_reduce_kernel(const float* __restrict__ ws, int slices, int m, int n, float* c,
@@ -822,6 +834,53 @@ static void launch_pack(shgemm_b200_handle_t h, const T* src, size_t ld_src, T* 
     h->launches++;
 }
 
+// TF32 compute with a K-contiguous binary16 B: widen B once into the handle's workspace
+// and run the 128 x 256 TF32 kernel that loads FP32 B unconverted (the grouped kernel on
+// a one-problem table). Taken only for eager calls (not while capturing: a captured
+// grouped launch replays whatever table the handle stages later), when the workspace
+// holds the widened B, and when 128 x 256 tiles fill the GPU (no split-K wanted);
+// otherwise SHGEMM_STATUS_NOT_SUPPORTED and the caller uses the tile kernel.
+static int tf32_widened_b(shgemm_b200_handle_t h, int op_a, int op_b, size_t m, size_t n, size_t k, float alpha,
+                          const float* a, size_t lda, const void* b, size_t ldb, float beta, float* c, size_t ldc,
+                          int op_c, int* level_out) {
+    if (op_b != kOpN || !h->grouped_dev || h->tile_kernel != 0 || h->fixed_level != SHGEMM_LEVEL_AUTO ||
+        h->split_k > 1)
+        return SHGEMM_STATUS_NOT_SUPPORTED;
+    const size_t ldw = (k + 3) / 4 * 4;
+    if (ldw * n * sizeof(float) > h->workspace_bytes) return SHGEMM_STATUS_NOT_SUPPORTED;
+    const long long tiles = static_cast<long long>((m + 127) / 128) * static_cast<long long>((n + 255) / 256);
+    if (tiles < h->num_sms || tiles > kGroupedMaxUnits) return SHGEMM_STATUS_NOT_SUPPORTED;
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(h->stream, &cap) != cudaSuccess || cap != cudaStreamCaptureStatusNone) {
+        cudaGetLastError();
+        return SHGEMM_STATUS_NOT_SUPPORTED;
+    }
+    const size_t total = k * n;
+    const int blocks = static_cast<int>(std::min<size_t>((total + 255) / 256, size_t(h->num_sms) * 16));
+    widen_b_kernel<<<blocks, 256, 0, h->stream>>>(static_cast<const __half*>(b), ldb, h->workspace, ldw,
+                                                  static_cast<int>(k), static_cast<int>(n));
+    h->launches++;
+    if (launch_status() != SHGEMM_STATUS_OK) return SHGEMM_STATUS_LAUNCH_FAILED;
+    shgemm_b200_problem q{};
+    q.m = m;
+    q.n = n;
+    q.k = k;
+    q.a = a;
+    q.lda = lda;
+    q.b = h->workspace;
+    q.ldb = ldw;
+    q.c = c;
+    q.ldc = ldc;
+    q.alpha = alpha;
+    q.beta = beta;
+    const int saved = h->grouped_b_fp32;
+    h->grouped_b_fp32 = 1;
+    const int st = shgemm_b200_shgemm_grouped(h, op_a, kOpN, kTF32, op_c, &q, 1);
+    h->grouped_b_fp32 = saved;
+    if (st == SHGEMM_STATUS_OK && level_out) *level_out = SHGEMM_LEVEL_P1;
+    return st;
+}
+
 extern "C" {
 
 int shgemm_b200_shgemm(shgemm_b200_handle_t h, int op_a, int op_b, size_t m, size_t n, size_t k,
@@ -857,6 +916,10 @@ int shgemm_b200_shgemm(shgemm_b200_handle_t h, int op_a, int op_b, size_t m, siz
     const bool pack_a = (reinterpret_cast<uintptr_t>(a) & 15) || (lda * 4) % 16;
     const bool pack_b = (reinterpret_cast<uintptr_t>(b) & 15) || (ldb * 2) % 16;
     if (!pack_a && !pack_b) {
+        if (tc == kTF32) {
+            const int st = tf32_widened_b(h, op_a, op_b, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc, op_c, level_out);
+            if (st != SHGEMM_STATUS_NOT_SUPPORTED) return st;
+        }
         // SHGEMM_CFG_AUTOTUNE = 2: an untuned bucket is tuned on this call's operands first
         // (C is overwritten by the candidates, harmless when beta == 0 and C is laid out op_n).
         if (h->autotune_mode == 2 && beta == 0.0f && op_c == kOpN && h->fixed_level == SHGEMM_LEVEL_AUTO &&

@@ -313,3 +313,23 @@ def test_k_chunk_128(h, dist, op_a):
     assert r128["e_gpu"] <= 2.0 * r128["e_sgemm"] + K.ULP_FLOOR, r128
     print(f"\n{dist} op_a={op_a}: e(64)={r64['e_gpu']:.3e} e(128)={r128['e_gpu']:.3e} "
           f"oracle={r64['e_oracle']:.3e} sgemm={r64['e_sgemm']:.3e}")
+
+
+@pytest.mark.parametrize("op_a", [0, 1])
+def test_tf32_widened_b_route(h, op_a):
+    """TF32 calls whose 128x256 tiles fill the GPU widen B into the workspace and run the
+    TF32 kernel that loads it unconverted: two launches, parity with the restated
+    reference, and the same bar as the in-kernel-widening tile kernel."""
+    import shgemm_b200 as sg
+
+    m, n, k = 2048, 2560, 700
+    before = h.launch_count()
+    r, c_route, _ = _parity(h, oracle.TF32, op_a, 0, 0, m, n, k, beta=0.5, dist="wide", seed=31 + op_a)
+    assert h.launch_count() - before == 2  # widen + TF32 kernel
+    K.assert_parity(r)
+    h.set_config(sg.CFG_TILE_KERNEL, 1)  # the tile kernel that widens B itself
+    try:
+        r_old, _, _ = _parity(h, oracle.TF32, op_a, 0, 0, m, n, k, beta=0.5, dist="wide", seed=31 + op_a)
+    finally:
+        h.set_config(sg.CFG_TILE_KERNEL, 0)
+    K.assert_parity(r_old)
