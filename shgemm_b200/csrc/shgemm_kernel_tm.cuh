@@ -45,7 +45,7 @@ struct TmCfg {
     // setmaxnreg shares: 2 split + 2 epilogue + 1 control warpgroup, out of the
     // 640 x 96 registers the block is launched with.
     static constexpr int LAUNCH_REGS = 96;
-    static constexpr int SPLIT_REGS = 56, EPI_REGS = 152, CTRL_REGS = 56;
+    static constexpr int SPLIT_REGS = 64, EPI_REGS = 152, CTRL_REGS = 48;
     static_assert(256 * SPLIT_REGS + 256 * EPI_REGS + 128 * CTRL_REGS <= NUM_THREADS * LAUNCH_REGS,
                   "register split exceeds the launch allocation");
     static constexpr int TMEM_COLS = 512;
@@ -163,6 +163,7 @@ __device__ __forceinline__ void tm_kernel_body(const Params& p) {
                 {
                     const uint8_t* ast = a_base + as * Cfg::A_STAGE;
                     const uint32_t tcol = tmem_base + lane_addr + Cfg::TMEM_OPERAND0 + ts * 64;
+                    uint32_t hw[16], lw[16];  // both k-blocks of this warp: columns 16 kh .. 16 kh + 15
 #pragma unroll
                     for (int c = 0; c < 2; ++c) {  // k-block kk = 2 kh + c of 16 k
                         float v[16];
@@ -183,11 +184,16 @@ __device__ __forceinline__ void tm_kernel_body(const Params& p) {
 #pragma unroll
                             for (int j = 0; j < 16; ++j) v[j] = *reinterpret_cast<const float*>(cp + j * 512);
                         }
-                        uint32_t hw[8], lw[8];
-                        split16_f16(v, hw, lw);
-                        ptx::tmem_st_32x32b_x8(tcol + (2 * kh + c) * 8, hw);
-                        ptx::tmem_st_32x32b_x8(tcol + 32 + (2 * kh + c) * 8, lw);
+                        uint32_t h8[8], l8[8];
+                        split16_f16(v, h8, l8);
+#pragma unroll
+                        for (int e = 0; e < 8; ++e) {
+                            hw[8 * c + e] = h8[e];
+                            lw[8 * c + e] = l8[e];
+                        }
                     }
+                    ptx::tmem_st_32x32b_x16(tcol + 16 * kh, hw);
+                    ptx::tmem_st_32x32b_x16(tcol + 32 + 16 * kh, lw);
                 }
                 ptx::tmem_st_wait();
                 ptx::tc_fence_before();
