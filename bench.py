@@ -114,7 +114,7 @@ class ClockSampler:
                 self.proc.kill()
 
     def summary(self):
-        sm, mx, reasons = [], None, set()
+        sm, mx, reasons, pw = [], None, set(), []
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         for ln in self.lines:
             parts = [x.strip() for x in ln.split(",")]
@@ -123,13 +123,25 @@ class ClockSampler:
             try:
                 sm.append(float(parts[1]))
                 mx = float(parts[2])
+                pw.append(float(parts[3]))
             except ValueError:
                 continue
             for nm, v in zip(names, parts[5:9]):
                 if v.lower() == "active":
                     reasons.add(nm)
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
-                "samples": len(sm)}
+                "samples": len(sm), "power_w_median": statistics.median(pw) if pw else None}
+
+
+def energy(clk, ms_per_call, flops_per_call):
+    """Board energy per call from the power samples of the timed region (the reference's
+    J-per-GEMM figure, test/power_consumption_test.cu:94-123, from nvidia-smi instead of NVML)."""
+    p = clk.get("power_w_median")
+    if not p:
+        return None
+    j = p * ms_per_call * 1e-3
+    return {"avg_board_power_w": p, "joules_per_call": j, "effective_gflop_per_joule": flops_per_call / j / 1e9,
+            "source": "nvidia-smi power.draw median over the timed region (whole board)"}
 
 
 def make_inputs(wl, dev, seed=0):
@@ -861,6 +873,7 @@ def main():
             "gpu_launches": launches,
             "roofline": roofline,
             "clocks": clk.summary(),
+            "energy": energy(clk.summary(), ms_step, flops_eff),
             "error": err,
             "e2e": e2e,
             "cpu_baseline": cpu,
