@@ -13,9 +13,8 @@
 //    128-column accumulator buffers, so a buffer's drain overlaps the next two halves'
 //    MMAs (about 1024 cycles) instead of one;
 //  * 20 warps: 8 split warps (two per TMEM lane quadrant, one per 32-k half of the
-//    step), 8 epilogue warps (per quadrant, one draining every N-half-0 buffer and one
-//    every N-half-1 buffer, so the two never read the quadrant's TMEM at the same time),
-//    a TMA producer warp and two MMA warps (one per N-half).
+//    step), 8 epilogue warps (two per quadrant, one per 64-column quarter of each
+//    half), a TMA producer warp and two MMA warps (one per N-half).
 //
 // Tensor memory (512 columns): accumulator buffer b at columns [128 b, 128 b + 128), b < 3,
 // used by half h of k-step s when (2 s + h) % 3 == b; operand stage t at
@@ -40,9 +39,6 @@ struct TmCfg {
     // 2 k-steps holds 2 operand stages while its MMAs run, so it takes 4 stages and 2 buffers
     static constexpr int SA = 4, SB = 3, ST = KC == 1 ? 2 : 4;
     static constexpr int ND = KC == 1 ? 3 : 2;
-    // half-use g = 2 chunk + half goes to buffer g % ND; the uses of one (buffer, half) pair
-    // repeat every PERIOD half-uses
-    static constexpr int PERIOD = (ND % 2) ? 2 * ND : ND;
     static_assert(KC == 1 || KC == 2, "k-chunk");
     static constexpr int NUM_THREADS = 640;
     static constexpr int SPLIT_WARPS = 8, EPI_WARP0 = 8, CTRL_WARP0 = 16;
@@ -97,11 +93,9 @@ __device__ __forceinline__ void tm_kernel_body(const Params& p) {
     uint64_t* b_empty = b_full + SB;   // MMAs reading the B stage completed
     uint64_t* t_full = b_empty + SB;   // hi/lo operand stage written to tensor memory
     uint64_t* t_empty = t_full + ST;   // MMAs reading the operand stage completed
-    // per (accumulator buffer b, N-half h), index 2 b + h: a buffer's uses alternate halves,
-    // so each barrier sees consecutive uses by one issuer and one epilogue group
-    uint64_t* d_full = t_empty + ST;           // use ready to drain
-    uint64_t* d_empty = d_full + 2 * Cfg::ND;  // use drained
-    uint64_t* drain_bar = d_empty + 2 * Cfg::ND;  // one per MMA issuer
+    uint64_t* d_full = t_empty + ST;   // accumulator buffer ready to drain
+    uint64_t* d_empty = d_full + Cfg::ND;  // accumulator buffer drained
+    uint64_t* drain_bar = d_empty + Cfg::ND;  // one per MMA issuer
     uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(drain_bar + 2);
     volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
 
@@ -121,9 +115,9 @@ __device__ __forceinline__ void tm_kernel_body(const Params& p) {
             ptx::mbar_init(&t_full[t], Cfg::SPLIT_WARPS);
             ptx::mbar_init(&t_empty[t], 2);  // both MMA issuers' commits
         }
-        for (int b = 0; b < 2 * Cfg::ND; ++b) {
+        for (int b = 0; b < Cfg::ND; ++b) {
             ptx::mbar_init(&d_full[b], 1);
-            ptx::mbar_init(&d_empty[b], 4);  // the four epilogue warps of that N-half
+            ptx::mbar_init(&d_empty[b], 8);
         }
         ptx::mbar_init(&drain_bar[0], 1);
         ptx::mbar_init(&drain_bar[1], 1);
@@ -223,7 +217,7 @@ __device__ __forceinline__ void tm_kernel_body(const Params& p) {
         // ---------------------------------------------------------------- epilogue
         ptx::setmaxnreg_inc<Cfg::EPI_REGS>();
         const int q = warp & 3;
-        const int hh = (warp - Cfg::EPI_WARP0) >> 2;  // the N-half whose 128 columns this warp drains
+        const int cq = (warp - Cfg::EPI_WARP0) >> 2;  // 64-column quarter within each half
         const int row_in_tile = q * 32 + lane;
         const uint32_t lane_addr = static_cast<uint32_t>(q * 32) << 16;
         uint32_t gc = 0;
@@ -235,39 +229,45 @@ __device__ __forceinline__ void tm_kernel_body(const Params& p) {
                 nsteps = ud.s1 - ud.s0;
                 // beta != 0: C of this thread's row into L2 (kept there) while the tile's k-steps run
                 const int row = ud.tm * Cfg::BM + row_in_tile;
-                if (ud.beta != 0.0f && !ud.partial && row < ud.m)
-                    prefetch_row<Cfg::HALF_N>(ud.c, ud.ldc, output_op(p), row, ud.tn * Cfg::BN + hh * Cfg::HALF_N, ud.n);
+                if (ud.beta != 0.0f && !ud.partial && row < ud.m) {
+#pragma unroll
+                    for (int h = 0; h < 2; ++h)
+                        prefetch_row<64>(ud.c, ud.ldc, output_op(p), row, ud.tn * Cfg::BN + h * Cfg::HALF_N + cq * 64,
+                                         ud.n);
+                }
             }
-            uint64_t acc2[64];  // 128 columns of half hh, in pairs
+            uint64_t acc2[64];  // [half][32 column pairs]
 #pragma unroll
             for (int j = 0; j < 64; ++j) acc2[j] = 0ull;
             for (int i = 0; i < nsteps; i += KC) {
-                // half hh of k-chunk gc: half-use g = 2 gc + hh, buffer g % ND, use g / PERIOD of
-                // the (buffer, half) pair
-                const uint32_t g = 2 * gc + hh, buf = g % Cfg::ND, bh = 2 * buf + hh;
-                if (!ptx::mbar_wait(&d_full[bh], (g / Cfg::PERIOD) & 1u, abort_flag, limit)) {
-                    fail(kErrEpilogueTimeout);
-                    goto epi_done;
-                }
-                ptx::tc_fence_after();
 #pragma unroll
-                for (int j0 = 0; j0 < Cfg::HALF_N; j0 += 32) {
-                    uint32_t r0[16], r1[16];
-                    const uint32_t ta = tmem_base + lane_addr + buf * Cfg::HALF_N + j0;
-                    ptx::tmem_ld_32x32b_x16(ta, r0);
-                    ptx::tmem_ld_32x32b_x16(ta + 16, r1);
-                    ptx::tmem_ld_wait();
-#pragma unroll
-                    for (int e = 0; e < 8; ++e) {
-                        uint64_t& a0 = acc2[j0 / 2 + e];
-                        uint64_t& a1 = acc2[j0 / 2 + 8 + e];
-                        a0 = ptx::f2_add(a0, (static_cast<uint64_t>(r0[2 * e + 1]) << 32) | r0[2 * e]);
-                        a1 = ptx::f2_add(a1, (static_cast<uint64_t>(r1[2 * e + 1]) << 32) | r1[2 * e]);
+                for (int h = 0; h < 2; ++h) {
+                    // half h of k-chunk gc is use (2 gc + h) / ND of buffer (2 gc + h) % ND
+                    const uint32_t g = 2 * gc + h, buf = g % Cfg::ND;
+                    if (!ptx::mbar_wait(&d_full[buf], (g / Cfg::ND) & 1u, abort_flag, limit)) {
+                        fail(kErrEpilogueTimeout);
+                        goto epi_done;
                     }
+                    ptx::tc_fence_after();
+#pragma unroll
+                    for (int j0 = 0; j0 < 64; j0 += 32) {
+                        uint32_t r0[16], r1[16];
+                        const uint32_t ta = tmem_base + lane_addr + buf * Cfg::HALF_N + cq * 64 + j0;
+                        ptx::tmem_ld_32x32b_x16(ta, r0);
+                        ptx::tmem_ld_32x32b_x16(ta + 16, r1);
+                        ptx::tmem_ld_wait();
+#pragma unroll
+                        for (int e = 0; e < 8; ++e) {
+                            uint64_t& a0 = acc2[h * 32 + j0 / 2 + e];
+                            uint64_t& a1 = acc2[h * 32 + j0 / 2 + 8 + e];
+                            a0 = ptx::f2_add(a0, (static_cast<uint64_t>(r0[2 * e + 1]) << 32) | r0[2 * e]);
+                            a1 = ptx::f2_add(a1, (static_cast<uint64_t>(r1[2 * e + 1]) << 32) | r1[2 * e]);
+                        }
+                    }
+                    ptx::tc_fence_before();
+                    __syncwarp();
+                    if (lane == 0) ptx::mbar_arrive(&d_empty[buf]);
                 }
-                ptx::tc_fence_before();
-                __syncwarp();
-                if (lane == 0) ptx::mbar_arrive(&d_empty[bh]);
                 ++gc;
             }
             {
@@ -276,16 +276,20 @@ __device__ __forceinline__ void tm_kernel_body(const Params& p) {
                 get_unit<Cfg>(p, u, ud);
                 const int row = ud.tm * Cfg::BM + row_in_tile;
                 if (row < ud.m) {
-                    const int col0 = ud.tn * Cfg::BN + hh * Cfg::HALF_N;
-                    if (ud.partial) {
-                        float* w = ud.partial + row;
 #pragma unroll
-                        for (int j = 0; j < Cfg::HALF_N; ++j) {
-                            const int col = col0 + j;
-                            if (col < ud.n) w[static_cast<size_t>(col) * ud.m] = acc(j);
+                    for (int h = 0; h < 2; ++h) {
+                        const int col0 = ud.tn * Cfg::BN + h * Cfg::HALF_N + cq * 64;
+                        if (ud.partial) {
+                            float* w = ud.partial + row;
+#pragma unroll
+                            for (int j = 0; j < 64; ++j) {
+                                const int col = col0 + j;
+                                if (col < ud.n) w[static_cast<size_t>(col) * ud.m] = acc(h * 64 + j);
+                            }
+                        } else {
+                            store_row<64>(ud.c, ud.ldc, output_op(p), row, col0, ud.n, ud.alpha, ud.beta,
+                                          [&](int j) { return acc(h * 64 + j); });
                         }
-                    } else {
-                        store_row<Cfg::HALF_N>(ud.c, ud.ldc, output_op(p), row, col0, ud.n, ud.alpha, ud.beta, acc);
                     }
                 }
             }
@@ -403,15 +407,7 @@ __device__ __forceinline__ void tm_kernel_body(const Params& p) {
                         bs = b;
                         bph = bp;
                     }
-                    {
-                        // the previous use of this buffer, half-use g - ND (the other half when ND is odd,
-                        // this half when ND is even): wait until the epilogue drained it
-                        const int g = static_cast<int>(2 * gc) + h, gp = g - Cfg::ND;
-                        if (gp >= 0) {
-                            const int hp = gp & 1;
-                            ok = ok && ptx::mbar_wait(&d_empty[2 * buf + hp], (gp / Cfg::PERIOD) & 1u, abort_flag, limit);
-                        }
-                    }
+                    ok = ok && ptx::mbar_wait(&d_empty[buf], (((2 * gc + h) / Cfg::ND) & 1u) ^ 1u, abort_flag, limit);
                     if (!ok) {
                         fail(kErrMmaTimeout);
                         goto mma_done;
@@ -447,7 +443,7 @@ __device__ __forceinline__ void tm_kernel_body(const Params& p) {
                         }
                     }
                     issued_any = true;
-                    ptx::umma_commit(&d_full[2 * buf + h]);
+                    ptx::umma_commit(&d_full[buf]);
 #pragma unroll
                     for (int j = 0; j < KC; ++j) {
                         if (j < c) {
