@@ -34,6 +34,10 @@ WORKLOADS = {
     # the large square SHGEMM
     "square16k": dict(m=16384, n=16384, k=16384, op_a=0, op_b=0, tc=0, alpha=1.0, beta=0.5, dist="wide",
                       desc="large square SHGEMM 16384^3 NN, fp16 compute, A N(0,1)*2^U(-15,15), B N(0,1), beta=0.5"),
+    # the same product with A transposed: the FP32 operand K-major (rows of k contiguous floats)
+    "square16k_tn": dict(m=16384, n=16384, k=16384, op_a=1, op_b=0, tc=0, alpha=1.0, beta=0.5, dist="wide",
+                         desc="large square SHGEMM 16384^3 TN, fp16 compute, A N(0,1)*2^U(-15,15), B N(0,1), "
+                              "beta=0.5"),
     # a smaller square case of the same kernel, for profiler captures (inputs still exceed L2)
     "square8k": dict(m=8192, n=8192, k=8192, op_a=0, op_b=0, tc=0, alpha=1.0, beta=0.5, dist="wide",
                      desc="square SHGEMM 8192^3 NN, fp16 compute, A N(0,1)*2^U(-15,15), B N(0,1), beta=0.5"),

@@ -69,6 +69,11 @@ struct alignas(64) TileGemmParams {
     int steps_per_slice;  // k-steps per slice
     int num_units;        // tiles_m * tiles_n * num_slices
     int group_m;          // rasterisation group along m
+    // Tensor-memory kernel, K-major FP32 operand: tmap_a is a 3-D view {32 floats, k / 32, m}
+    // whose box {32, 2, 128} lands each row's 64 floats of a k-step in two adjacent 128-byte
+    // segments (row r, k-half h at segment 2 r + h). 0: two 2-D boxes {32, 128}, one per
+    // k-half (segment 128 h + r).
+    int a_rows_paired;
 };
 
 // B_WIDE (TF32 compute only): the binary16 operand arrives already widened to FP32

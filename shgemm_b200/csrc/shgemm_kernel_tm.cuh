@@ -148,6 +148,13 @@ __device__ __forceinline__ void tm_kernel_body(const Params& p) {
         const int kh = warp >> 2;  // k 32 kh .. 32 kh + 31 of each step
         const int row = q * 32 + lane;
         const uint32_t lane_addr = static_cast<uint32_t>(q * 32) << 16;
+        // K-major raw tile: the 128-byte segment holding this row's k-half kh and its swizzle
+        // phase. Lanes 4-7 of every 8 read the two chunks of each pair in swapped order: in the
+        // paired layout rows r and r + 4 share a phase, and the swap keeps their loads on
+        // different banks (in the per-half layout it only permutes already distinct chunks).
+        const int seg = p.a_rows_paired ? 2 * row + kh : kh * Cfg::BM + row;
+        const int sw = seg & 7;
+        const int fl = (lane >> 2) & 1;
         int as = 0, ts = 0;
         uint32_t aph = 0, tph = 0;
         for (int u = blockIdx.x; u < num_units; u += gridDim.x) {
@@ -168,15 +175,19 @@ __device__ __forceinline__ void tm_kernel_body(const Params& p) {
                     for (int c = 0; c < 2; ++c) {  // k-block kk = 2 kh + c of 16 k
                         float v[16];
                         if constexpr (A_KMAJOR) {
-                            // raw sub-tile kh: [128 rows][32 floats], 128-byte swizzle; chunks 4c .. 4c+3
-                            const uint8_t* rp = ast + kh * (Cfg::BM * 128) + row * 128;
+                            // 32 floats of the segment, 128-byte swizzle; chunks 4c .. 4c+3
+                            const uint8_t* rp = ast + seg * 128;
+                            float4 x[4];
+#pragma unroll
+                            for (int j = 0; j < 4; ++j)
+                                x[j] = *reinterpret_cast<const float4*>(rp + ((((4 * c + j) ^ fl) ^ sw) << 4));
 #pragma unroll
                             for (int j = 0; j < 4; ++j) {
-                                const float4 x = *reinterpret_cast<const float4*>(rp + (((4 * c + j) ^ (row & 7)) << 4));
-                                v[4 * j] = x.x;
-                                v[4 * j + 1] = x.y;
-                                v[4 * j + 2] = x.z;
-                                v[4 * j + 3] = x.w;
+                                const float4 y = fl ? x[j ^ 1] : x[j];
+                                v[4 * j] = y.x;
+                                v[4 * j + 1] = y.y;
+                                v[4 * j + 2] = y.z;
+                                v[4 * j + 3] = y.w;
                             }
                         } else {
                             // raw [64 k][128 m] floats, 512-byte rows: a warp reads 128 contiguous bytes per k
@@ -319,10 +330,15 @@ __device__ __forceinline__ void tm_kernel_body(const Params& p) {
                         uint8_t* a_dst = a_base + as * Cfg::A_STAGE;
                         ptx::mbar_arrive_expect_tx(&a_full[as], Cfg::A_STAGE);
                         if constexpr (A_KMAJOR) {
+                            if (p.a_rows_paired) {
+                                // one box of 128 rows x 256 bytes: whole row segments per request
+                                ptx::tma_load_3d(a_dst, ud.tmap_a, &a_full[as], 0, 2 * st, ud.tm * Cfg::BM);
+                            } else {
 #pragma unroll
-                            for (int sub = 0; sub < 2; ++sub)
-                                ptx::tma_load_2d(a_dst + sub * (Cfg::BM * 128), ud.tmap_a, &a_full[as], kc + 32 * sub,
-                                                 ud.tm * Cfg::BM);
+                                for (int sub = 0; sub < 2; ++sub)
+                                    ptx::tma_load_2d(a_dst + sub * (Cfg::BM * 128), ud.tmap_a, &a_full[as],
+                                                     kc + 32 * sub, ud.tm * Cfg::BM);
+                            }
                         } else {
                             ptx::tma_load_2d(a_dst, ud.tmap_a, &a_full[as], ud.tm * Cfg::BM, kc);
                         }

@@ -265,11 +265,13 @@ def test_split_k_deterministic_and_matches(h, tc, op_a, op_b):
 
 
 @pytest.mark.parametrize("op_a", [0, 1])
-@pytest.mark.parametrize("mnk", [(1000, 700, 3000), (128, 256, 64), (385, 513, 1111)])
+@pytest.mark.parametrize("mnk", [(1000, 700, 3000), (128, 256, 64), (385, 513, 1111), (1000, 700, 2080), (385, 513, 1024)])
 def test_tensor_memory_kernel_matches_shared_memory_kernel(h, op_a, mnk):
     """The 128x256 binary16 kernel that keeps hi/lo in tensor memory computes the same
     products in the same order as the shared-memory operand kernel: bit-identical C,
-    and within the parity bar of the restated reference."""
+    and within the parity bar of the restated reference. With op_a = T and k a multiple
+    of 32 (2080: an odd count of 32-wide halves, the last step half past k) the FP32
+    operand arrives through the paired 3-D box; other k take the two 2-D boxes."""
     import shgemm_b200 as sg
 
     m, n, k = mnk
