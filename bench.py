@@ -51,6 +51,10 @@ WORKLOADS = {
     "sketch": dict(m=4096, n=256, k=1 << 20, op_a=1, op_b=0, tc=0, alpha=1.0, beta=0.0, dist="sketch",
                    desc="left sketch Y = Omega^T A, A 2^20 x 4096 FP32 (low rank + noise), Omega 2^20 x 256 "
                         "binary16 N(0,1/256), split-K, fp16 compute", op_c=1, bound="hbm"),
+    # the sketch at 1/8 of its length (A 2 GiB, still 16x L2), for profiler captures
+    "sketch128k": dict(m=4096, n=256, k=1 << 17, op_a=1, op_b=0, tc=0, alpha=1.0, beta=0.0, dist="sketch",
+                       op_c=1, desc="left sketch Y = Omega^T A, A 2^17 x 4096 FP32 (low rank + noise), "
+                                    "Omega 2^17 x 256 binary16", bound="hbm"),
     # 512 uneven right sketches in one graph-captured grouped launch
     "grouped": dict(m=0, n=0, k=0, op_a=0, op_b=0, tc=0, alpha=1.0, beta=0.0, dist="grouped", count=512, bound="hbm",
                     desc="grouped batch of 512 uneven right sketches Y_i = A_i Omega_i, m_i log-U[64,8192], "
@@ -734,6 +738,9 @@ def main():
     if wl["tc"] == 1 and wl["op_b"] == 0:
         # room for the widened FP32 copy of B (the TF32 route that loads B unconverted)
         h.set_workspace_size(max(64 << 20, n * ((k + 3) // 4 * 4) * 4 + (1 << 20)))
+    if wl["tc"] == 0 and wl["op_b"] == 0 and ldb * 2 >= (1 << 20):
+        # room for B re-laid out as contiguous k-blocks (columns >= 1 MiB apart) plus the split-K partials
+        h.set_workspace_size((64 << 20) + n * ((k + 63) // 64 * 64) * 2)
     # one-off autotune of the shape's bucket (not timed); C is overwritten by it, then restored
     tuned = None
     if not args.no_autotune and op_c == 0:

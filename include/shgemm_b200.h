@@ -117,8 +117,11 @@ int shgemm_b200_set_debug_mode(shgemm_b200_handle_t handle, unsigned on);
  * op_c == SHGEMM_OP_T stores C transposed. TF32 calls with a K-contiguous B whose
  * 128 x 256 tiles fill the GPU and whose widened B (n * round4(k) floats) fits the handle
  * workspace widen B there first and run the TF32 kernel that loads it unconverted
- * (not while capturing). *level_out (may be NULL) receives the
- * kernel level used, like the reference's return value. */
+ * (not while capturing). Binary16 calls whose K-contiguous B has columns >= 1 MiB apart
+ * (ldb >= 512 Ki) and run on 128 x 256 tiles re-lay B out in the workspace as contiguous
+ * 64-deep k-blocks first, when it holds n * round64(k) * 2 bytes besides the split-K
+ * partials (a wide column pitch otherwise halves the load rate). *level_out (may be NULL)
+ * receives the kernel level used, like the reference's return value. */
 int shgemm_b200_shgemm(shgemm_b200_handle_t handle, int op_a, int op_b, size_t m, size_t n, size_t k,
                        const float* alpha, const float* a, size_t lda, const void* b, size_t ldb,
                        const float* beta, float* c, size_t ldc, int compute_type, int op_c, int* level_out);

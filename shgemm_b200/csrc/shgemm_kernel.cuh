@@ -74,6 +74,12 @@ struct alignas(64) TileGemmParams {
     // segments (row r, k-half h at segment 2 r + h). 0: two 2-D boxes {32, 128}, one per
     // k-half (segment 128 h + r).
     int a_rows_paired;
+    // Tensor-memory kernel: every FP32 tile is read by one unit only (a single tile column),
+    // so its loads carry an evict-first L2 hint and leave L2 to the shared binary16 tiles.
+    int a_read_once;
+    // Tensor-memory kernel: tmap_b is a 3-D view {64 k, n, k / 64} of the binary16 operand
+    // re-laid out as contiguous k-blocks; a step loads box (0, 256 tn, step).
+    int b_blocked;
 };
 
 // B_WIDE (TF32 compute only): the binary16 operand arrives already widened to FP32

@@ -310,6 +310,7 @@ __device__ __forceinline__ void tm_kernel_body(const Params& p) {
         ptx::setmaxnreg_dec<Cfg::CTRL_REGS>();
         if (warp == Cfg::CTRL_WARP0 && lane == 0) {
             // ------------------------------------------------------------ TMA producer
+            const uint64_t pol_a = ptx::l2_policy_evict_first();
             int as = 0, bs = 0;
             uint32_t aph = 0, bph = 0;
             uint32_t a_issued = 0, a_par = 0, b_issued = 0, b_par = 0;  // per stage: load in flight, its parity
@@ -332,15 +333,27 @@ __device__ __forceinline__ void tm_kernel_body(const Params& p) {
                         if constexpr (A_KMAJOR) {
                             if (p.a_rows_paired) {
                                 // one box of 128 rows x 256 bytes: whole row segments per request
-                                ptx::tma_load_3d(a_dst, ud.tmap_a, &a_full[as], 0, 2 * st, ud.tm * Cfg::BM);
+                                if (p.a_read_once)
+                                    ptx::tma_load_3d_hint(a_dst, ud.tmap_a, &a_full[as], 0, 2 * st, ud.tm * Cfg::BM,
+                                                          pol_a);
+                                else
+                                    ptx::tma_load_3d(a_dst, ud.tmap_a, &a_full[as], 0, 2 * st, ud.tm * Cfg::BM);
                             } else {
 #pragma unroll
-                                for (int sub = 0; sub < 2; ++sub)
-                                    ptx::tma_load_2d(a_dst + sub * (Cfg::BM * 128), ud.tmap_a, &a_full[as],
-                                                     kc + 32 * sub, ud.tm * Cfg::BM);
+                                for (int sub = 0; sub < 2; ++sub) {
+                                    if (p.a_read_once)
+                                        ptx::tma_load_2d_hint(a_dst + sub * (Cfg::BM * 128), ud.tmap_a, &a_full[as],
+                                                              kc + 32 * sub, ud.tm * Cfg::BM, pol_a);
+                                    else
+                                        ptx::tma_load_2d(a_dst + sub * (Cfg::BM * 128), ud.tmap_a, &a_full[as],
+                                                         kc + 32 * sub, ud.tm * Cfg::BM);
+                                }
                             }
                         } else {
-                            ptx::tma_load_2d(a_dst, ud.tmap_a, &a_full[as], ud.tm * Cfg::BM, kc);
+                            if (p.a_read_once)
+                                ptx::tma_load_2d_hint(a_dst, ud.tmap_a, &a_full[as], ud.tm * Cfg::BM, kc, pol_a);
+                            else
+                                ptx::tma_load_2d(a_dst, ud.tmap_a, &a_full[as], ud.tm * Cfg::BM, kc);
                         }
                         a_issued |= 1u << as;
                         a_par = (a_par & ~(1u << as)) | (aph << as);
@@ -354,7 +367,10 @@ __device__ __forceinline__ void tm_kernel_body(const Params& p) {
                         goto producer_done;
                     }
                     ptx::mbar_arrive_expect_tx(&b_full[bs], Cfg::B_STAGE);
-                    ptx::tma_load_2d(b_base + bs * Cfg::B_STAGE, ud.tmap_b, &b_full[bs], kc, ud.tn * Cfg::BN);
+                    if (p.b_blocked)
+                        ptx::tma_load_3d(b_base + bs * Cfg::B_STAGE, ud.tmap_b, &b_full[bs], 0, ud.tn * Cfg::BN, st);
+                    else
+                        ptx::tma_load_2d(b_base + bs * Cfg::B_STAGE, ud.tmap_b, &b_full[bs], kc, ud.tn * Cfg::BN);
                     b_issued |= 1u << bs;
                     b_par = (b_par & ~(1u << bs)) | (bph << bs);
                     if (++bs == SB) {

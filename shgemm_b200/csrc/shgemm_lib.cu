@@ -86,21 +86,28 @@ bool make_tmap(CUtensorMap* map, CUtensorMapDataType dtype, const void* base, ui
     return r == CUDA_SUCCESS;
 }
 
+// 3-D tiled tensor map: dim0 contiguous, dims 1 and 2 with byte strides s1, s2; box {b0, b1, b2}.
+bool make_tmap_3d(CUtensorMap* map, CUtensorMapDataType dtype, const void* base, uint64_t d0, uint64_t d1,
+                  uint64_t d2, uint64_t s1, uint64_t s2, uint32_t b0, uint32_t b1, uint32_t b2, CUtensorMapSwizzle swz) {
+    EncodeTiledFn fn = encode_fn();
+    if (!fn) return false;
+    cuuint64_t dims[3] = {d0, d1, d2};
+    cuuint64_t strides[2] = {s1, s2};
+    cuuint32_t box[3] = {b0, b1, b2};
+    cuuint32_t estr[3] = {1, 1, 1};
+    CUresult r = fn(map, dtype, 3, const_cast<void*>(base), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                    swz, CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS;
+}
+
 // K-major FP32 operand (k x m, column stride `ld_bytes`) as a 3-D view {32 floats, k / 32,
 // m} with box {32, 2, 128} and a 128-byte swizzle: one load brings 128 rows x 64 floats, each
 // row's two 128-byte halves adjacent in shared memory. k must be a multiple of 32 so that the
 // view never reaches past a row into the next one.
 bool make_tmap_a_paired(CUtensorMap* map, const float* base, uint64_t k, uint64_t m, uint64_t ld_bytes) {
-    EncodeTiledFn fn = encode_fn();
-    if (!fn || k % 32 != 0) return false;
-    cuuint64_t dims[3] = {32, k / 32, m};
-    cuuint64_t strides[2] = {128, ld_bytes};
-    cuuint32_t box[3] = {32, 2, 128};
-    cuuint32_t estr[3] = {1, 1, 1};
-    CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, const_cast<float*>(base), dims, strides, box, estr,
-                    CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
-                    CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-    return r == CUDA_SUCCESS;
+    if (k % 32 != 0) return false;
+    return make_tmap_3d(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, base, 32, k / 32, m, 128, ld_bytes, 32, 2, 128,
+                        CU_TENSOR_MAP_SWIZZLE_128B);
 }
 
 // Width (m) of one TMA box of an M-major FP32 operand: the binary16 kernels load a 128-row
@@ -109,6 +116,9 @@ bool make_tmap_a_paired(CUtensorMap* map, const float* base, uint64_t k, uint64_
 constexpr uint32_t a_mmajor_box(int tc, bool b_wide = false) { return tc == kFP16 ? 64 : (b_wide ? 32 : 128); }
 
 using TileKernelFn = void (*)(TileGemmParams);
+
+// Column pitch of a K-major binary16 operand from which it is re-laid out as k-blocks.
+constexpr size_t kBlockBMinPitchBytes = size_t(1) << 20;
 
 template <int TC, int BN, bool AK, bool BK>
 void* tile_kernel_ptr() {
@@ -208,6 +218,35 @@ __global__ void widen_b_kernel(const __half* __restrict__ src, uint64_t ldb, flo
          idx += static_cast<size_t>(gridDim.x) * blockDim.x) {
         const size_t r = idx % k, c = idx / k;
         dst[r + c * ld_dst] = __half2float(src[r + c * ldb]);
+    }
+}
+
+// Re-lays a k x n binary16 K-contiguous operand (leading dimension ldb, 16-byte aligned
+// columns) out as k-blocks: dst[(kb * n + col) * 64 + j] = src[col * ldb + 64 kb + j], zero
+// where 64 kb + j >= k. One 64-deep step of a 256-column tile is then one contiguous 32 KB
+// run instead of 256 rows a leading dimension apart. A thread moves 16 bytes; a warp reads
+// 512 contiguous bytes of one column.
+__global__ void block_b_kernel(const __half* __restrict__ src, uint64_t ldb, __half* __restrict__ dst, int k, int n,
+                               int kblocks) {
+    const size_t total = static_cast<size_t>(n) * kblocks * 8;
+    for (size_t idx = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; idx < total;
+         idx += static_cast<size_t>(gridDim.x) * blockDim.x) {
+        const int c8 = static_cast<int>(idx & 7);
+        const size_t rest = idx >> 3;
+        const int kb = static_cast<int>(rest % kblocks);
+        const int col = static_cast<int>(rest / kblocks);
+        const size_t k0 = static_cast<size_t>(kb) * 64 + c8 * 8;
+        const __half* s = src + static_cast<size_t>(col) * ldb + k0;
+        uint4 v;
+        if (k0 + 8 <= static_cast<size_t>(k)) {
+            v = *reinterpret_cast<const uint4*>(s);
+        } else {
+            __half t[8];
+#pragma unroll
+            for (int j = 0; j < 8; ++j) t[j] = (k0 + j < static_cast<size_t>(k)) ? s[j] : __float2half(0.0f);
+            v = *reinterpret_cast<const uint4*>(t);
+        }
+        *reinterpret_cast<uint4*>(dst + (static_cast<size_t>(kb) * n + col) * 64 + c8 * 8) = v;
     }
 }
 
@@ -753,12 +792,31 @@ static int run_tiled(shgemm_b200_handle_t h, int op_a, int op_b, size_t m, size_
                      int op_c, int* level_out, float* splitk_ws, size_t splitk_bytes,
                      const shgemm_b200_tuned_config* force = nullptr) {
     int group_m = 8;
-    const Plan pl = force ? plan_from_tuned(*force, m, n, k, tc, splitk_bytes)
-                          : make_plan(h, op_a, op_b, m, n, k, tc, splitk_bytes, &group_m);
-    if (force) group_m = force->group_m;
     const bool a_kmajor = (op_a == kOpT);
     const bool b_kmajor = (op_b == kOpN);
     const int bk = (tc == kFP16) ? 64 : 32;
+    auto plan_with = [&](size_t ws_bytes) {
+        return force ? plan_from_tuned(*force, m, n, k, tc, ws_bytes)
+                     : make_plan(h, op_a, op_b, m, n, k, tc, ws_bytes, &group_m);
+    };
+    // A binary16 K-major operand whose columns lie >= 1 MiB apart puts each of a tile's 256
+    // columns on a page of its own: every 64-deep step then needs 256 address translations
+    // on top of the FP32 tile's, more than an SM's translation caches keep while streaming
+    // (the loads run at about half speed). When the workspace has room, such a B is re-laid
+    // out once per call as contiguous k-blocks (block_b_kernel) ahead of the split-K partials.
+    const size_t kblocks = (k + 63) / 64;
+    const size_t bblk_bytes = (kblocks * n * 128 + 255) / 256 * 256;
+    bool block_b = tc == kFP16 && b_kmajor && h->tile_kernel == 0 && ldb * 2 >= kBlockBMinPitchBytes &&
+                   splitk_bytes >= bblk_bytes && kblocks < (1u << 31);
+    Plan pl{};
+    if (block_b) {
+        pl = plan_with(splitk_bytes - bblk_bytes);
+        if (pl.bn != 256) block_b = false;
+    }
+    if (!block_b) pl = plan_with(splitk_bytes);
+    if (force) group_m = force->group_m;
+    float* part_ws = block_b ? splitk_ws + bblk_bytes / sizeof(float) : splitk_ws;
+    __half* b_blk = reinterpret_cast<__half*>(splitk_ws);
     // binary16 compute with 128 x 256 tiles and a K-major B: the tensor-memory operand kernel
     const bool use_tm = tc == kFP16 && pl.bn == 256 && b_kmajor && h->tile_kernel == 0;
 
@@ -782,7 +840,10 @@ static int run_tiled(shgemm_b200_handle_t h, int op_a, int op_b, size_t m, size_
                        bk, CU_TENSOR_MAP_SWIZZLE_NONE);
     if (!ok) return SHGEMM_STATUS_NOT_SUPPORTED;
     if (tc == kFP16) {
-        if (b_kmajor)
+        if (block_b)  // k-blocks {64 k, n columns, kblocks}: one 64 x 256 tile step is 32 KB contiguous
+            ok = make_tmap_3d(&P.tmap_b, CU_TENSOR_MAP_DATA_TYPE_FLOAT16, b_blk, 64, n, kblocks, 128, n * 128, 64,
+                              pl.bn, 1, CU_TENSOR_MAP_SWIZZLE_128B);
+        else if (b_kmajor)
             ok = make_tmap(&P.tmap_b, CU_TENSOR_MAP_DATA_TYPE_FLOAT16, b, k, n, ldb * 2, 64, pl.bn,
                            CU_TENSOR_MAP_SWIZZLE_128B);
         else
@@ -800,7 +861,7 @@ static int run_tiled(shgemm_b200_handle_t h, int op_a, int op_b, size_t m, size_
 
     P.c = c;
     P.ldc = ldc;
-    P.workspace = splitk_ws;
+    P.workspace = part_ws;
     P.error_flag = h->error_word;
     P.wait_limit_ns = static_cast<uint64_t>(h->wait_limit_ms) * 1000000ull;
     P.m = static_cast<int>(m);
@@ -815,6 +876,8 @@ static int run_tiled(shgemm_b200_handle_t h, int op_a, int op_b, size_t m, size_
     P.steps_per_slice = pl.steps_per_slice;
     P.num_units = pl.tiles_m * pl.tiles_n * pl.slices;
     P.group_m = group_m;
+    P.a_read_once = use_tm && pl.tiles_n == 1;
+    P.b_blocked = block_b ? 1 : 0;
 
     const KernelEntry e = use_tm ? tm_kernel_table(a_kmajor, h->k_chunk / 64) : kernel_table(tc, pl.bn, a_kmajor, b_kmajor);
     const int threads = use_tm ? TmCfg<true>::NUM_THREADS : 512;
@@ -826,6 +889,14 @@ static int run_tiled(shgemm_b200_handle_t h, int op_a, int op_b, size_t m, size_
                     m, n, k, op_a == kOpN ? "N" : "T", op_b == kOpN ? "N" : "T", tc == kTF32 ? "TF32" : "FP16",
                     pl.level, pl.bn, pl.slices, use_tm ? h->k_chunk : bk, grid, use_tm ? ", operands in TMEM" : "");
     }
+    if (block_b) {
+        const size_t total = kblocks * n * 8;
+        const int blocks = static_cast<int>(std::min<size_t>((total + 255) / 256, size_t(h->num_sms) * 16));
+        block_b_kernel<<<blocks, 256, 0, h->stream>>>(static_cast<const __half*>(b), ldb, b_blk, static_cast<int>(k),
+                                                      static_cast<int>(n), static_cast<int>(kblocks));
+        h->launches++;
+        if (launch_status() != SHGEMM_STATUS_OK) return SHGEMM_STATUS_LAUNCH_FAILED;
+    }
     void* args[] = {&P};
     cudaError_t err = cudaLaunchKernel(e.fn, dim3(grid), dim3(threads), args, e.smem, h->stream);
     h->launches++;
@@ -836,8 +907,7 @@ static int run_tiled(shgemm_b200_handle_t h, int op_a, int op_b, size_t m, size_
     if (pl.slices > 1) {
         const size_t mn = m * n;
         const int blocks = static_cast<int>(std::min<size_t>((mn + 255) / 256, size_t(h->num_sms) * 8));
-        splitk_reduce_kernel<<<blocks, 256, 0, h->stream>>>(splitk_ws, pl.slices, P.m, P.n, c, ldc, op_c, alpha,
-                                                            beta);
+        splitk_reduce_kernel<<<blocks, 256, 0, h->stream>>>(part_ws, pl.slices, P.m, P.n, c, ldc, op_c, alpha, beta);
         h->launches++;
         if (launch_status() != SHGEMM_STATUS_OK) return SHGEMM_STATUS_LAUNCH_FAILED;
     }

@@ -290,6 +290,35 @@ def test_tensor_memory_kernel_matches_shared_memory_kernel(h, op_a, mnk):
     assert np.array_equal(c_tm.view(np.uint32), c_sm.view(np.uint32))
 
 
+@pytest.mark.parametrize("op_a", [0, 1])
+@pytest.mark.parametrize("k", [1000, 8224])
+def test_wide_pitch_b_k_blocks(h, op_a, k):
+    """A binary16 operand whose columns lie >= 1 MiB apart is re-laid out as contiguous
+    k-blocks in the workspace before the tensor-memory kernel runs (ragged last block
+    zero-filled, n below one tile, split-K at k = 8224): C is bit-identical to the same
+    values stored with a compact leading dimension, which loads B in place."""
+    import shgemm_b200 as sg
+
+    m, n = 300, 136
+    rng = np.random.default_rng(k + op_a)
+    inp = K.make_inputs(rng, m, n, k, op_a, 0, 0, dist="wide")
+    ld_wide = (1 << 19) + 8  # 1 MiB + 16 bytes between columns
+    wide = np.zeros(n * ld_wide, dtype=np.float16)
+    wide.reshape(n, ld_wide)[:, :k] = inp["B"].reshape(n, k)
+    inp_w = dict(inp, B=wide, ldb=ld_wide)
+    sg.enable_kernel_level_fixing(h, 1)  # 128 x 256 tiles: the tensor-memory kernel
+    try:
+        c_compact, _ = K.run_gpu(h, oracle.FP16, op_a, 0, m, n, k, 1.0, inp, 0.5, 0)
+        c_wide, _ = K.run_gpu(h, oracle.FP16, op_a, 0, m, n, k, 1.0, inp_w, 0.5, 0)
+    finally:
+        sg.disable_kernel_level_fixing(h)
+    assert np.array_equal(c_compact.view(np.uint32), c_wide.view(np.uint32))
+    orc = K.run_oracle(oracle.FP16, op_a, 0, m, n, k, 1.0, inp, 0.5, 0, chunk=0)
+    ref = K.fp64(op_a, 0, m, n, k, 1.0, inp, 0.5, 0)
+    sgc = K.sgemm(op_a, 0, m, n, k, 1.0, inp, 0.5, 0)
+    K.assert_parity(K.parity_report(c_wide, orc, ref, sgc, m, n, inp["ldc"], 0))
+
+
 @pytest.mark.parametrize("dist", ["uniform", "wide", "positive"])
 @pytest.mark.parametrize("op_a", [0, 1])
 def test_k_chunk_128(h, dist, op_a):
