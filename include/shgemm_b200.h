@@ -59,7 +59,9 @@ enum {
                                       accumulator in the tensor-memory kernel: 64 (default) or
                                       128 (measured: ~1.2x the 64-k error on mixed-sign data,
                                       ~2.2x on all-positive data, within 2x FP32 SGEMM's error);
-                                      the other kernels always drain every 64 */
+                                      the other kernels always drain every 64 */,
+    SHGEMM_CFG_HOST_BLOCK_COLS = 9 /* columns of C per block of shgemm_b200_shgemm_host:
+                                      0 (default) = a multiple of 256 giving about 8 blocks */
 };
 
 /* ------------------------------------------------------------------------
@@ -125,6 +127,25 @@ int shgemm_b200_set_debug_mode(shgemm_b200_handle_t handle, unsigned on);
 int shgemm_b200_shgemm(shgemm_b200_handle_t handle, int op_a, int op_b, size_t m, size_t n, size_t k,
                        const float* alpha, const float* a, size_t lda, const void* b, size_t ldb,
                        const float* beta, float* c, size_t ldc, int compute_type, int op_c, int* level_out);
+
+/* SHGEMM on host buffers (no reference counterpart: the reference takes device
+ * pointers only). Same arguments, status codes and results as shgemm_b200_shgemm,
+ * but a, b and c are host addresses. A is copied to the device once; C is then
+ * produced in column blocks (SHGEMM_CFG_HOST_BLOCK_COLS) through two device slots,
+ * block j's B and C columns going up while block j-1 computes and block j-2's C
+ * comes back, so both PCIe directions overlap the tensor work. Host buffers should
+ * be page-locked (cudaHostAlloc / cudaHostRegister); pageable memory gives correct
+ * results without the overlap. Device staging (A plus two blocks) belongs to the
+ * handle and grows when a call needs more, the only allocation this entry point
+ * makes (refused with SHGEMM_STATUS_NOT_SUPPORTED while the stream is capturing);
+ * shgemm_b200_release_host_staging frees it. Asynchronous like every call here:
+ * synchronise the handle's stream before reading c or reusing a or b. */
+int shgemm_b200_shgemm_host(shgemm_b200_handle_t handle, int op_a, int op_b, size_t m, size_t n, size_t k,
+                            const float* alpha, const float* a, size_t lda, const void* b, size_t ldb,
+                            const float* beta, float* c, size_t ldc, int compute_type, int op_c, int* level_out);
+
+/* Frees the handle's host-entry staging (after synchronising its streams). */
+int shgemm_b200_release_host_staging(shgemm_b200_handle_t handle);
 
 /* mtk::shgemm::hsgemm (include/shgemm/shgemm.hpp:121-157): A binary16, B FP32,
  * computed through the same transposition identity as the reference. */

@@ -17,7 +17,7 @@ import os
 __all__ = [
     "op_n", "op_t", "fp16", "tf32", "P0", "P1", "ShgemmError", "Handle", "create", "destroy",
     "set_cuda_stream", "enable_kernel_level_fixing", "disable_kernel_level_fixing", "set_debug_mode",
-    "shgemm", "hsgemm", "library_path",
+    "shgemm", "hsgemm", "shgemm_host", "release_host_staging", "library_path",
 ]
 
 op_n, op_t = 0, 1          # operation_t (include/shgemm/shgemm.hpp:36-39)
@@ -26,6 +26,7 @@ P0, P1 = 0, 1              # detail::kernel_level (include/shgemm/shgemm.hpp:30-
 
 CFG_SPLIT_K, CFG_WAIT_LIMIT_MS, CFG_GROUP_M, CFG_GROUPED_B_FP32, CFG_AUTOTUNE, CFG_TILE_KERNEL, CFG_K_CHUNK = (
     2, 3, 4, 5, 6, 7, 8)
+CFG_HOST_BLOCK_COLS = 9
 
 STATUS = {0: "OK", 1: "INVALID_VALUE", 2: "NOT_SUPPORTED", 3: "ALLOC_FAILED", 4: "LAUNCH_FAILED",
           5: "TIMEOUT", 6: "CUDA_ERROR", 7: "SCRATCH_TOO_SMALL"}
@@ -81,6 +82,8 @@ def lib() -> ctypes.CDLL:
         "shgemm_b200_set_debug_mode": [vp, ctypes.c_uint],
         "shgemm_b200_shgemm": [vp, i, i, sz, sz, sz, pf, vp, sz, vp, sz, pf, vp, sz, i, i, pi],
         "shgemm_b200_hsgemm": [vp, i, i, sz, sz, sz, pf, vp, sz, vp, sz, pf, vp, sz, i, i, pi],
+        "shgemm_b200_shgemm_host": [vp, i, i, sz, sz, sz, pf, vp, sz, vp, sz, pf, vp, sz, i, i, pi],
+        "shgemm_b200_release_host_staging": [vp],
         "shgemm_b200_set_config": [vp, i, ctypes.c_longlong],
         "shgemm_b200_get_config": [vp, i, ctypes.POINTER(ctypes.c_longlong)],
         "shgemm_b200_set_workspace_size": [vp, sz],
@@ -281,6 +284,44 @@ def hsgemm(handle: Handle, op_a: int, op_b: int, m: int, n: int, k: int, alpha: 
                                   ctypes.byref(be), _addr(c), ldc, compute_type, op_c, ctypes.byref(lv))
     _check(st, "hsgemm")
     return lv.value
+
+
+# ---------------------------------------------------------------- host buffers
+def _host_addr(x) -> int:
+    """Host address of a CPU torch tensor, a C-contiguous numpy array or an integer pointer."""
+    if x is None:
+        return 0
+    if isinstance(x, int):
+        return x
+    if hasattr(x, "data_ptr"):
+        if getattr(x, "is_cuda", False):
+            raise ValueError("shgemm_host takes host buffers; use shgemm for device memory")
+        return x.data_ptr()
+    if hasattr(x, "ctypes"):
+        return x.ctypes.data
+    raise TypeError(f"expected a host tensor, a numpy array or an address, got {type(x)!r}")
+
+
+def shgemm_host(handle: Handle, op_a: int, op_b: int, m: int, n: int, k: int, alpha: float, a, lda: int, b, ldb: int,
+                beta: float, c, ldc: int, compute_type: int, op_c: int = op_n) -> int:
+    """shgemm with A, B and C in host memory; copies overlap the computation.
+
+    A goes to the device once, then C is computed in column blocks whose B/C uploads,
+    computation and C download overlap on separate streams. Pass page-locked buffers
+    (torch `pin_memory=True`) for the overlap. Asynchronous on the handle's stream:
+    synchronise it before reading C. Returns the kernel level of the first block.
+    """
+    al, be, lv = ctypes.c_float(alpha), ctypes.c_float(beta), ctypes.c_int(0)
+    st = lib().shgemm_b200_shgemm_host(handle.ptr, op_a, op_b, m, n, k, ctypes.byref(al), _host_addr(a), lda,
+                                       _host_addr(b), ldb, ctypes.byref(be), _host_addr(c), ldc, compute_type, op_c,
+                                       ctypes.byref(lv))
+    _check(st, "shgemm_host")
+    return lv.value
+
+
+def release_host_staging(handle: Handle) -> None:
+    """Frees the device staging that shgemm_host keeps in the handle."""
+    _check(lib().shgemm_b200_release_host_staging(handle.ptr), "release_host_staging")
 
 
 # ---------------------------------------------------------------- allocation-free path

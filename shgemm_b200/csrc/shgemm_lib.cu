@@ -49,6 +49,13 @@ struct shgemm_b200_handle {
     int k_chunk = 64;       // SHGEMM_CFG_K_CHUNK
     std::mutex tune_mu;
     std::map<uint64_t, shgemm_b200_tuned_config> tuned;
+    // host-buffer entry: device staging (A and two column blocks of B and C), one stream per
+    // copy direction, events start / in[2] / computed[2] / out[2]
+    void* host_stage = nullptr;
+    size_t host_stage_bytes = 0;
+    cudaStream_t host_in = nullptr, host_out = nullptr;
+    cudaEvent_t host_ev[7] = {};
+    long long host_block_cols = 0;  // SHGEMM_CFG_HOST_BLOCK_COLS
 };
 
 namespace {
@@ -644,6 +651,11 @@ int shgemm_b200_create(shgemm_b200_handle_t* out, int device) {
 int shgemm_b200_destroy(shgemm_b200_handle_t h) {
     if (!h) return SHGEMM_STATUS_INVALID_VALUE;
     DeviceGuard g(h->device);
+    shgemm_b200_release_host_staging(h);
+    for (cudaEvent_t& e : h->host_ev)
+        if (e) cudaEventDestroy(e);
+    if (h->host_in) cudaStreamDestroy(h->host_in);
+    if (h->host_out) cudaStreamDestroy(h->host_out);
     if (h->grouped_copied) {
         cudaEventSynchronize(h->grouped_copied);
         cudaEventDestroy(h->grouped_copied);
@@ -705,6 +717,10 @@ int shgemm_b200_set_config(shgemm_b200_handle_t h, int key, long long v) {
             if (v != 64 && v != 128) return SHGEMM_STATUS_INVALID_VALUE;
             h->k_chunk = static_cast<int>(v);
             return SHGEMM_STATUS_OK;
+        case SHGEMM_CFG_HOST_BLOCK_COLS:
+            if (v < 0 || v >= (1ll << 31)) return SHGEMM_STATUS_INVALID_VALUE;
+            h->host_block_cols = v;
+            return SHGEMM_STATUS_OK;
         default:
             return SHGEMM_STATUS_INVALID_VALUE;
     }
@@ -720,6 +736,7 @@ int shgemm_b200_get_config(shgemm_b200_handle_t h, int key, long long* v) {
         case SHGEMM_CFG_AUTOTUNE: *v = h->autotune_mode; return SHGEMM_STATUS_OK;
         case SHGEMM_CFG_TILE_KERNEL: *v = h->tile_kernel; return SHGEMM_STATUS_OK;
         case SHGEMM_CFG_K_CHUNK: *v = h->k_chunk; return SHGEMM_STATUS_OK;
+        case SHGEMM_CFG_HOST_BLOCK_COLS: *v = h->host_block_cols; return SHGEMM_STATUS_OK;
         default: return SHGEMM_STATUS_INVALID_VALUE;
     }
 }
@@ -1272,6 +1289,143 @@ int shgemm_b200_hsgemm(shgemm_b200_handle_t h, int op_a, int op_b, size_t m, siz
         return SHGEMM_STATUS_INVALID_VALUE;
     return shgemm_b200_shgemm(h, inv(op_b), inv(op_a), n, m, k, alpha, b, ldb, a, lda, beta, c, ldc, tc, inv(op_c),
                               level_out);
+}
+
+int shgemm_b200_release_host_staging(shgemm_b200_handle_t h) {
+    if (!h) return SHGEMM_STATUS_INVALID_VALUE;
+    if (!h->host_stage) return SHGEMM_STATUS_OK;
+    DeviceGuard g(h->device);
+    if (cudaStreamSynchronize(h->stream) != cudaSuccess) return SHGEMM_STATUS_CUDA_ERROR;
+    if (h->host_in) cudaStreamSynchronize(h->host_in);
+    if (h->host_out) cudaStreamSynchronize(h->host_out);
+    cudaFree(h->host_stage);
+    h->host_stage = nullptr;
+    h->host_stage_bytes = 0;
+    return SHGEMM_STATUS_OK;
+}
+
+// Host-buffer SHGEMM. A goes to the device once; C is then produced in column blocks that
+// alternate between two staging slots: the copy-in stream brings block j's B columns (and C
+// columns when beta != 0) while the handle's stream computes block j - 1 with the device
+// entry point and the copy-out stream returns block j - 2, so both copy directions overlap
+// the tensor work. Events order the three streams; the handle's stream waits for the last
+// copy-out, so synchronising it covers the whole call.
+int shgemm_b200_shgemm_host(shgemm_b200_handle_t h, int op_a, int op_b, size_t m, size_t n, size_t k,
+                            const float* alpha_ptr, const float* a, size_t lda, const void* b, size_t ldb,
+                            const float* beta_ptr, float* c, size_t ldc, int tc, int op_c, int* level_out) {
+    if (!h || !alpha_ptr || !beta_ptr) return SHGEMM_STATUS_INVALID_VALUE;
+    if ((op_a != kOpN && op_a != kOpT) || (op_b != kOpN && op_b != kOpT) || (op_c != kOpN && op_c != kOpT) ||
+        (tc != kFP16 && tc != kTF32))
+        return SHGEMM_STATUS_INVALID_VALUE;
+    if (m == 0 || n == 0) {
+        if (level_out) *level_out = SHGEMM_LEVEL_P0;
+        return SHGEMM_STATUS_OK;
+    }
+    const size_t a_rows = (op_a == kOpN) ? m : k, a_cols = (op_a == kOpN) ? k : m;
+    const size_t b_rows = (op_b == kOpN) ? k : n;
+    const size_t c_rows = (op_c == kOpN) ? m : n;
+    if (!c || ldc < c_rows) return SHGEMM_STATUS_INVALID_VALUE;
+    if (k > 0 && (!a || !b || lda < std::max<size_t>(1, a_rows) || ldb < std::max<size_t>(1, b_rows)))
+        return SHGEMM_STATUS_INVALID_VALUE;
+    if (m >= (1u << 31) || n >= (1u << 31) || k >= (1u << 31)) return SHGEMM_STATUS_NOT_SUPPORTED;
+    const float alpha = *alpha_ptr, beta = *beta_ptr;
+    DeviceGuard g(h->device);
+
+    // column blocks: a multiple of the 256-wide tile, about eight per call by default
+    size_t nb = h->host_block_cols > 0 ? static_cast<size_t>(h->host_block_cols)
+                                       : std::max<size_t>(256, round_up((n + 7) / 8, 256));
+    nb = std::min(nb, n);
+    const size_t nblocks = (n + nb - 1) / nb;
+    // device layouts: 16-byte aligned leading dimensions, each region 256-byte aligned
+    const size_t lda_d = round_up(std::max<size_t>(a_rows, 1), 4);
+    const size_t a_bytes = round_up(lda_d * a_cols * 4, 256);
+    const size_t ldb_d = (op_b == kOpN) ? round_up(std::max<size_t>(k, 1), 8) : round_up(nb, 8);
+    const size_t b_blk = round_up(((op_b == kOpN) ? ldb_d * nb : ldb_d * k) * 2, 256);
+    const size_t ldc_d = (op_c == kOpN) ? round_up(m, 4) : round_up(nb, 4);
+    const size_t c_blk = round_up(((op_c == kOpN) ? ldc_d * nb : ldc_d * m) * 4, 256);
+    const size_t need = a_bytes + 2 * (b_blk + c_blk);
+
+    if (!h->host_in) {
+        if (cudaStreamCreateWithFlags(&h->host_in, cudaStreamNonBlocking) != cudaSuccess ||
+            cudaStreamCreateWithFlags(&h->host_out, cudaStreamNonBlocking) != cudaSuccess) {
+            cudaGetLastError();
+            return SHGEMM_STATUS_CUDA_ERROR;
+        }
+        for (cudaEvent_t& e : h->host_ev)
+            if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) {
+                cudaGetLastError();
+                return SHGEMM_STATUS_CUDA_ERROR;
+            }
+    }
+    if (need > h->host_stage_bytes) {  // grow the staging (the one allocation of this entry point)
+        cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+        if (cudaStreamIsCapturing(h->stream, &cap) != cudaSuccess || cap != cudaStreamCaptureStatusNone)
+            return SHGEMM_STATUS_NOT_SUPPORTED;
+        const int st = shgemm_b200_release_host_staging(h);
+        if (st != SHGEMM_STATUS_OK) return st;
+        if (cudaMalloc(&h->host_stage, need) != cudaSuccess) {
+            cudaGetLastError();
+            h->host_stage = nullptr;
+            return SHGEMM_STATUS_ALLOC_FAILED;
+        }
+        h->host_stage_bytes = need;
+    }
+    char* base = static_cast<char*>(h->host_stage);
+    float* a_d = reinterpret_cast<float*>(base);
+    __half* b_s[2] = {reinterpret_cast<__half*>(base + a_bytes), reinterpret_cast<__half*>(base + a_bytes + b_blk)};
+    float* c_s[2] = {reinterpret_cast<float*>(base + a_bytes + 2 * b_blk),
+                     reinterpret_cast<float*>(base + a_bytes + 2 * b_blk + c_blk)};
+    cudaEvent_t ev_start = h->host_ev[0], *ev_in = h->host_ev + 1, *ev_comp = h->host_ev + 3, *ev_out = h->host_ev + 5;
+    const __half* bh = static_cast<const __half*>(b);
+
+    // the copy streams start after everything already queued on the handle's stream
+    cudaEventRecord(ev_start, h->stream);
+    cudaStreamWaitEvent(h->host_in, ev_start, 0);
+    cudaStreamWaitEvent(h->host_out, ev_start, 0);
+    if (k > 0)
+        cudaMemcpy2DAsync(a_d, lda_d * 4, a, lda * 4, a_rows * 4, a_cols, cudaMemcpyHostToDevice, h->host_in);
+    int level = SHGEMM_LEVEL_P0;
+    for (size_t j = 0; j < nblocks; ++j) {
+        const int slot = static_cast<int>(j & 1);
+        const size_t c0 = j * nb, nbj = std::min(nb, n - c0);
+        if (j >= 2) cudaStreamWaitEvent(h->host_in, ev_out[slot], 0);  // block j - 2 has left the slot
+        if (k > 0) {
+            if (op_b == kOpN)
+                cudaMemcpy2DAsync(b_s[slot], ldb_d * 2, bh + c0 * ldb, ldb * 2, k * 2, nbj, cudaMemcpyHostToDevice,
+                                  h->host_in);
+            else
+                cudaMemcpy2DAsync(b_s[slot], ldb_d * 2, bh + c0, ldb * 2, nbj * 2, k, cudaMemcpyHostToDevice,
+                                  h->host_in);
+        }
+        if (beta != 0.0f) {
+            if (op_c == kOpN)
+                cudaMemcpy2DAsync(c_s[slot], ldc_d * 4, c + c0 * ldc, ldc * 4, m * 4, nbj, cudaMemcpyHostToDevice,
+                                  h->host_in);
+            else
+                cudaMemcpy2DAsync(c_s[slot], ldc_d * 4, c + c0, ldc * 4, nbj * 4, m, cudaMemcpyHostToDevice,
+                                  h->host_in);
+        }
+        cudaEventRecord(ev_in[slot], h->host_in);
+        cudaStreamWaitEvent(h->stream, ev_in[slot], 0);
+        int lvl = SHGEMM_LEVEL_P0;
+        const int st = shgemm_b200_shgemm(h, op_a, op_b, m, nbj, k, &alpha, a_d, lda_d, b_s[slot], ldb_d, &beta,
+                                          c_s[slot], ldc_d, tc, op_c, &lvl);
+        if (st != SHGEMM_STATUS_OK) return st;
+        if (j == 0) level = lvl;
+        cudaEventRecord(ev_comp[slot], h->stream);
+        cudaStreamWaitEvent(h->host_out, ev_comp[slot], 0);
+        if (op_c == kOpN)
+            cudaMemcpy2DAsync(c + c0 * ldc, ldc * 4, c_s[slot], ldc_d * 4, m * 4, nbj, cudaMemcpyDeviceToHost,
+                              h->host_out);
+        else
+            cudaMemcpy2DAsync(c + c0, ldc * 4, c_s[slot], ldc_d * 4, nbj * 4, m, cudaMemcpyDeviceToHost, h->host_out);
+        cudaEventRecord(ev_out[slot], h->host_out);
+    }
+    cudaStreamWaitEvent(h->stream, ev_out[(nblocks - 1) & 1], 0);
+    if (nblocks > 1) cudaStreamWaitEvent(h->stream, ev_out[nblocks & 1], 0);
+    if (cudaGetLastError() != cudaSuccess) return SHGEMM_STATUS_CUDA_ERROR;
+    if (level_out) *level_out = level;
+    return SHGEMM_STATUS_OK;
 }
 
 static int eval_dgemm_impl(shgemm_b200_handle_t h, int op_a, int op_b, size_t m, size_t n, size_t k, const void* a,
