@@ -61,7 +61,7 @@ enum {
                                       ~2.2x on all-positive data, within 2x FP32 SGEMM's error);
                                       the other kernels always drain every 64 */,
     SHGEMM_CFG_HOST_BLOCK_COLS = 9 /* columns of C per block of shgemm_b200_shgemm_host:
-                                      0 (default) = a multiple of 256 giving about 8 blocks */
+                                      0 (default) = a multiple of 256 giving about 16 blocks */
 };
 
 /* ------------------------------------------------------------------------
@@ -131,11 +131,11 @@ int shgemm_b200_shgemm(shgemm_b200_handle_t handle, int op_a, int op_b, size_t m
 /* SHGEMM on host buffers (no reference counterpart: the reference takes device
  * pointers only). Same arguments, status codes and results as shgemm_b200_shgemm,
  * but a, b and c are host addresses. A is copied to the device once; C is then
- * produced in column blocks (SHGEMM_CFG_HOST_BLOCK_COLS) through two device slots,
+ * produced in column blocks (SHGEMM_CFG_HOST_BLOCK_COLS) through three device slots,
  * block j's B and C columns going up while block j-1 computes and block j-2's C
  * comes back, so both PCIe directions overlap the tensor work. Host buffers should
  * be page-locked (cudaHostAlloc / cudaHostRegister); pageable memory gives correct
- * results without the overlap. Device staging (A plus two blocks) belongs to the
+ * results without the overlap. Device staging (A plus three blocks) belongs to the
  * handle and grows when a call needs more, the only allocation this entry point
  * makes (refused with SHGEMM_STATUS_NOT_SUPPORTED while the stream is capturing);
  * shgemm_b200_release_host_staging frees it. Asynchronous like every call here:

@@ -49,12 +49,12 @@ struct shgemm_b200_handle {
     int k_chunk = 64;       // SHGEMM_CFG_K_CHUNK
     std::mutex tune_mu;
     std::map<uint64_t, shgemm_b200_tuned_config> tuned;
-    // host-buffer entry: device staging (A and two column blocks of B and C), one stream per
-    // copy direction, events start / in[2] / computed[2] / out[2]
+    // host-buffer entry: device staging (A and three column-block slots of B and C), one
+    // stream per copy direction, events start / in[3] / computed[3] / out[3]
     void* host_stage = nullptr;
     size_t host_stage_bytes = 0;
     cudaStream_t host_in = nullptr, host_out = nullptr;
-    cudaEvent_t host_ev[7] = {};
+    cudaEvent_t host_ev[10] = {};
     long long host_block_cols = 0;  // SHGEMM_CFG_HOST_BLOCK_COLS
 };
 
@@ -1305,11 +1305,12 @@ int shgemm_b200_release_host_staging(shgemm_b200_handle_t h) {
 }
 
 // Host-buffer SHGEMM. A goes to the device once; C is then produced in column blocks that
-// alternate between two staging slots: the copy-in stream brings block j's B columns (and C
+// rotate through three staging slots: the copy-in stream brings block j's B columns (and C
 // columns when beta != 0) while the handle's stream computes block j - 1 with the device
 // entry point and the copy-out stream returns block j - 2, so both copy directions overlap
-// the tensor work. Events order the three streams; the handle's stream waits for the last
-// copy-out, so synchronising it covers the whole call.
+// the tensor work; the third slot lets block j + 1 go up before block j - 2 has come back
+// (with two, the upload stream waited for every download). Events order the three streams;
+// the handle's stream waits for the last copy-outs, so synchronising it covers the call.
 int shgemm_b200_shgemm_host(shgemm_b200_handle_t h, int op_a, int op_b, size_t m, size_t n, size_t k,
                             const float* alpha_ptr, const float* a, size_t lda, const void* b, size_t ldb,
                             const float* beta_ptr, float* c, size_t ldc, int tc, int op_c, int* level_out) {
@@ -1331,9 +1332,11 @@ int shgemm_b200_shgemm_host(shgemm_b200_handle_t h, int op_a, int op_b, size_t m
     const float alpha = *alpha_ptr, beta = *beta_ptr;
     DeviceGuard g(h->device);
 
-    // column blocks: a multiple of the 256-wide tile, about eight per call by default
+    // column blocks: a multiple of the 256-wide tile, about sixteen per call by default (the
+    // last block's compute and download are the part no upload hides)
+    constexpr int kSlots = 3;
     size_t nb = h->host_block_cols > 0 ? static_cast<size_t>(h->host_block_cols)
-                                       : std::max<size_t>(256, round_up((n + 7) / 8, 256));
+                                       : std::max<size_t>(256, round_up((n + 15) / 16, 256));
     nb = std::min(nb, n);
     const size_t nblocks = (n + nb - 1) / nb;
     // device layouts: 16-byte aligned leading dimensions, each region 256-byte aligned
@@ -1343,7 +1346,7 @@ int shgemm_b200_shgemm_host(shgemm_b200_handle_t h, int op_a, int op_b, size_t m
     const size_t b_blk = round_up(((op_b == kOpN) ? ldb_d * nb : ldb_d * k) * 2, 256);
     const size_t ldc_d = (op_c == kOpN) ? round_up(m, 4) : round_up(nb, 4);
     const size_t c_blk = round_up(((op_c == kOpN) ? ldc_d * nb : ldc_d * m) * 4, 256);
-    const size_t need = a_bytes + 2 * (b_blk + c_blk);
+    const size_t need = a_bytes + kSlots * (b_blk + c_blk);
 
     if (!h->host_in) {
         if (cudaStreamCreateWithFlags(&h->host_in, cudaStreamNonBlocking) != cudaSuccess ||
@@ -1372,10 +1375,14 @@ int shgemm_b200_shgemm_host(shgemm_b200_handle_t h, int op_a, int op_b, size_t m
     }
     char* base = static_cast<char*>(h->host_stage);
     float* a_d = reinterpret_cast<float*>(base);
-    __half* b_s[2] = {reinterpret_cast<__half*>(base + a_bytes), reinterpret_cast<__half*>(base + a_bytes + b_blk)};
-    float* c_s[2] = {reinterpret_cast<float*>(base + a_bytes + 2 * b_blk),
-                     reinterpret_cast<float*>(base + a_bytes + 2 * b_blk + c_blk)};
-    cudaEvent_t ev_start = h->host_ev[0], *ev_in = h->host_ev + 1, *ev_comp = h->host_ev + 3, *ev_out = h->host_ev + 5;
+    __half* b_s[kSlots];
+    float* c_s[kSlots];
+    for (int sl = 0; sl < kSlots; ++sl) {
+        b_s[sl] = reinterpret_cast<__half*>(base + a_bytes + sl * b_blk);
+        c_s[sl] = reinterpret_cast<float*>(base + a_bytes + kSlots * b_blk + sl * c_blk);
+    }
+    cudaEvent_t ev_start = h->host_ev[0], *ev_in = h->host_ev + 1, *ev_comp = ev_in + kSlots,
+                *ev_out = ev_comp + kSlots;
     const __half* bh = static_cast<const __half*>(b);
 
     // the copy streams start after everything already queued on the handle's stream
@@ -1386,9 +1393,9 @@ int shgemm_b200_shgemm_host(shgemm_b200_handle_t h, int op_a, int op_b, size_t m
         cudaMemcpy2DAsync(a_d, lda_d * 4, a, lda * 4, a_rows * 4, a_cols, cudaMemcpyHostToDevice, h->host_in);
     int level = SHGEMM_LEVEL_P0;
     for (size_t j = 0; j < nblocks; ++j) {
-        const int slot = static_cast<int>(j & 1);
+        const int slot = static_cast<int>(j % kSlots);
         const size_t c0 = j * nb, nbj = std::min(nb, n - c0);
-        if (j >= 2) cudaStreamWaitEvent(h->host_in, ev_out[slot], 0);  // block j - 2 has left the slot
+        if (j >= kSlots) cudaStreamWaitEvent(h->host_in, ev_out[slot], 0);  // the slot's last block is home
         if (k > 0) {
             if (op_b == kOpN)
                 cudaMemcpy2DAsync(b_s[slot], ldb_d * 2, bh + c0 * ldb, ldb * 2, k * 2, nbj, cudaMemcpyHostToDevice,
@@ -1421,8 +1428,7 @@ int shgemm_b200_shgemm_host(shgemm_b200_handle_t h, int op_a, int op_b, size_t m
             cudaMemcpy2DAsync(c + c0, ldc * 4, c_s[slot], ldc_d * 4, nbj * 4, m, cudaMemcpyDeviceToHost, h->host_out);
         cudaEventRecord(ev_out[slot], h->host_out);
     }
-    cudaStreamWaitEvent(h->stream, ev_out[(nblocks - 1) & 1], 0);
-    if (nblocks > 1) cudaStreamWaitEvent(h->stream, ev_out[nblocks & 1], 0);
+    for (size_t sl = 0; sl < std::min<size_t>(nblocks, kSlots); ++sl) cudaStreamWaitEvent(h->stream, ev_out[sl], 0);
     if (cudaGetLastError() != cudaSuccess) return SHGEMM_STATUS_CUDA_ERROR;
     if (level_out) *level_out = level;
     return SHGEMM_STATUS_OK;
