@@ -144,6 +144,12 @@ int shgemm_b200_shgemm_host(shgemm_b200_handle_t handle, int op_a, int op_b, siz
                             const float* alpha, const float* a, size_t lda, const void* b, size_t ldb,
                             const float* beta, float* c, size_t ldc, int compute_type, int op_c, int* level_out);
 
+/* hsgemm on host buffers (A binary16, B FP32): shgemm_b200_shgemm_host through the
+ * same transposition identity as shgemm_b200_hsgemm. */
+int shgemm_b200_hsgemm_host(shgemm_b200_handle_t handle, int op_a, int op_b, size_t m, size_t n, size_t k,
+                            const float* alpha, const void* a, size_t lda, const float* b, size_t ldb,
+                            const float* beta, float* c, size_t ldc, int compute_type, int op_c, int* level_out);
+
 /* Frees the handle's host-entry staging (after synchronising its streams). */
 int shgemm_b200_release_host_staging(shgemm_b200_handle_t handle);
 

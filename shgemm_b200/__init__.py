@@ -17,7 +17,7 @@ import os
 __all__ = [
     "op_n", "op_t", "fp16", "tf32", "P0", "P1", "ShgemmError", "Handle", "create", "destroy",
     "set_cuda_stream", "enable_kernel_level_fixing", "disable_kernel_level_fixing", "set_debug_mode",
-    "shgemm", "hsgemm", "shgemm_host", "release_host_staging", "library_path",
+    "shgemm", "hsgemm", "shgemm_host", "hsgemm_host", "release_host_staging", "library_path",
 ]
 
 op_n, op_t = 0, 1          # operation_t (include/shgemm/shgemm.hpp:36-39)
@@ -84,6 +84,7 @@ def lib() -> ctypes.CDLL:
         "shgemm_b200_hsgemm": [vp, i, i, sz, sz, sz, pf, vp, sz, vp, sz, pf, vp, sz, i, i, pi],
         "shgemm_b200_shgemm_host": [vp, i, i, sz, sz, sz, pf, vp, sz, vp, sz, pf, vp, sz, i, i, pi],
         "shgemm_b200_release_host_staging": [vp],
+        "shgemm_b200_hsgemm_host": [vp, i, i, sz, sz, sz, pf, vp, sz, vp, sz, pf, vp, sz, i, i, pi],
         "shgemm_b200_set_config": [vp, i, ctypes.c_longlong],
         "shgemm_b200_get_config": [vp, i, ctypes.POINTER(ctypes.c_longlong)],
         "shgemm_b200_set_workspace_size": [vp, sz],
@@ -316,6 +317,17 @@ def shgemm_host(handle: Handle, op_a: int, op_b: int, m: int, n: int, k: int, al
                                        _host_addr(b), ldb, ctypes.byref(be), _host_addr(c), ldc, compute_type, op_c,
                                        ctypes.byref(lv))
     _check(st, "shgemm_host")
+    return lv.value
+
+
+def hsgemm_host(handle: Handle, op_a: int, op_b: int, m: int, n: int, k: int, alpha: float, a, lda: int, b, ldb: int,
+                beta: float, c, ldc: int, compute_type: int, op_c: int = op_n) -> int:
+    """hsgemm (A binary16, B FP32) with A, B and C in host memory; see shgemm_host."""
+    al, be, lv = ctypes.c_float(alpha), ctypes.c_float(beta), ctypes.c_int(0)
+    st = lib().shgemm_b200_hsgemm_host(handle.ptr, op_a, op_b, m, n, k, ctypes.byref(al), _host_addr(a), lda,
+                                       _host_addr(b), ldb, ctypes.byref(be), _host_addr(c), ldc, compute_type, op_c,
+                                       ctypes.byref(lv))
+    _check(st, "hsgemm_host")
     return lv.value
 
 

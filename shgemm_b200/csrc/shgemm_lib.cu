@@ -1434,6 +1434,17 @@ int shgemm_b200_shgemm_host(shgemm_b200_handle_t h, int op_a, int op_b, size_t m
     return SHGEMM_STATUS_OK;
 }
 
+int shgemm_b200_hsgemm_host(shgemm_b200_handle_t h, int op_a, int op_b, size_t m, size_t n, size_t k,
+                            const float* alpha, const void* a, size_t lda, const float* b, size_t ldb,
+                            const float* beta, float* c, size_t ldc, int tc, int op_c, int* level_out) {
+    // the same transposition identity as shgemm_b200_hsgemm, on the host-buffer path
+    auto inv = [](int op) { return op == kOpN ? kOpT : kOpN; };
+    if ((op_a != kOpN && op_a != kOpT) || (op_b != kOpN && op_b != kOpT) || (op_c != kOpN && op_c != kOpT))
+        return SHGEMM_STATUS_INVALID_VALUE;
+    return shgemm_b200_shgemm_host(h, inv(op_b), inv(op_a), n, m, k, alpha, b, ldb, a, lda, beta, c, ldc, tc,
+                                   inv(op_c), level_out);
+}
+
 static int eval_dgemm_impl(shgemm_b200_handle_t h, int op_a, int op_b, size_t m, size_t n, size_t k, const void* a,
                            size_t lda, const void* b, size_t ldb, double* c64, bool a_is_float) {
     if (!h || !a || !b || !c64 || m == 0 || n == 0) return SHGEMM_STATUS_INVALID_VALUE;

@@ -136,3 +136,31 @@ def test_host_rejects_device_tensor(h):
     a = torch.zeros(16, device="cuda")
     with pytest.raises(ValueError):
         sg.shgemm_host(h, 0, 0, 4, 4, 4, 1.0, a, 4, a, 4, 0.0, a, 4, oracle.FP16)
+
+
+@pytest.mark.parametrize("op_a,op_b", [(0, 0), (1, 1)])
+def test_hsgemm_host_matches_device(h, op_a, op_b):
+    """hsgemm (A binary16, B FP32) on host buffers, two blocks: bit-identical to the
+    device hsgemm under the same fixed plan."""
+    import torch
+
+    import shgemm_b200 as sg
+
+    rng = np.random.default_rng(41 + op_a)
+    m, n, k = 384, 200, 520
+    lda = m if op_a == 0 else k
+    ldb = k if op_b == 0 else n
+    Ah = rng.uniform(-1, 1, lda * (k if op_a == 0 else m)).astype(np.float16)
+    Bf = rng.uniform(-1, 1, ldb * (n if op_b == 0 else k)).astype(np.float32)
+    inp = dict(A=Bf, B=Ah, C=rng.uniform(-1, 1, m * n).astype(np.float32), lda=ldb, ldb=lda, ldc=m)
+    _same_plan(h)
+    h.set_config(sg.CFG_HOST_BLOCK_COLS, 256)  # the internal shgemm's n is this call's m: blocks 256 + 128
+    try:
+        c_dev, _ = K.run_gpu(h, oracle.FP16, op_a, op_b, m, n, k, 1.0, inp, 0.5, 0, hs=True)
+        Ch = torch.from_numpy(inp["C"].copy()).pin_memory()
+        sg.hsgemm_host(h, op_a, op_b, m, n, k, 1.0, Ah, lda, Bf, ldb, 0.5, Ch, m, oracle.FP16)
+        torch.cuda.synchronize()
+        assert h.check_error() == 0
+    finally:
+        _default_plan(h)
+    assert np.array_equal(c_dev.view(np.uint32), Ch.numpy().view(np.uint32))
