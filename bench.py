@@ -41,6 +41,9 @@ WORKLOADS = {
     # a smaller square case of the same kernel, for profiler captures (inputs still exceed L2)
     "square8k": dict(m=8192, n=8192, k=8192, op_a=0, op_b=0, tc=0, alpha=1.0, beta=0.5, dist="wide",
                      desc="square SHGEMM 8192^3 NN, fp16 compute, A N(0,1)*2^U(-15,15), B N(0,1), beta=0.5"),
+    # square8k with A transposed (K-major FP32 operand), for profiler captures of that load path
+    "square8k_tn": dict(m=8192, n=8192, k=8192, op_a=1, op_b=0, tc=0, alpha=1.0, beta=0.5, dist="wide",
+                        desc="square SHGEMM 8192^3 TN, fp16 compute, A N(0,1)*2^U(-15,15), B N(0,1), beta=0.5"),
     # a still smaller square case: with square8k it shows how DRAM traffic scales with the problem
     "square4k": dict(m=4096, n=4096, k=4096, op_a=0, op_b=0, tc=0, alpha=1.0, beta=0.5, dist="wide",
                      desc="square SHGEMM 4096^3 NN, fp16 compute, A N(0,1)*2^U(-15,15), B N(0,1), beta=0.5"),
