@@ -74,3 +74,17 @@ def test_library_is_sm100a_only():
     out = subprocess.run(["cuobjdump", "--list-elf", shgemm_b200.library_path()], capture_output=True,
                          text=True).stdout
     assert "sm_100a" in out
+
+
+def test_host_entry_points_validate_without_gpu():
+    """The host-buffer entry points reject a missing handle before any CUDA call."""
+    import shgemm_b200
+
+    L = shgemm_b200.lib()
+    one = ctypes.c_float(1.0)
+    lvl = ctypes.c_int(-7)
+    for fn in (L.shgemm_b200_shgemm_host, L.shgemm_b200_hsgemm_host):
+        st = fn(None, 0, 0, 4, 4, 4, ctypes.byref(one), None, 4, None, 4, ctypes.byref(one), None, 4, 0, 0,
+                ctypes.byref(lvl))
+        assert st == 1  # SHGEMM_STATUS_INVALID_VALUE
+    assert L.shgemm_b200_release_host_staging(None) == 1
