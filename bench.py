@@ -78,6 +78,22 @@ WORKLOADS = {
 }
 
 
+def max_over_ranks(ms: float, dist, device) -> float:
+    """Length of a timed region as the maximum over ranks (each rank timed its own device)."""
+    if dist is None:
+        return ms
+    import torch
+
+    t = torch.tensor([ms], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def aggregate_tflops(world: int, flops_per_rank: float, ms: float) -> float:
+    """Whole-job TFLOP/s: every replica's work over the slowest rank's time."""
+    return world * flops_per_rank / (ms * 1e-3) / 1e12
+
+
 def load_peaks():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
@@ -778,15 +794,11 @@ def main():
     launches = h.launch_count() - launches0
     if dist:
         dist.barrier()
-    ms_total = ev0.elapsed_time(ev1)
-    t = torch.tensor([ms_total], device=dev, dtype=torch.float64)
-    if dist:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms_total = float(t.item())
+    ms_total = max_over_ranks(ev0.elapsed_time(ev1), dist, dev)
     ms_step = ms_total / args.steps
     flops_eff = 2.0 * m * n * k
     flops_issued = 4.0 * m * n * k
-    value = world * flops_eff * args.steps / (ms_total * 1e-3) / 1e12
+    value = aggregate_tflops(world, flops_eff * args.steps, ms_total)
     if h.check_error() != 0:
         raise RuntimeError("device-side timeout in the timed region")
 
@@ -829,10 +841,8 @@ def main():
             e2e_step()
         e1.record(stream)
         torch.cuda.synchronize(dev)
-        te = torch.tensor([e0.elapsed_time(e1)], device=dev, dtype=torch.float64)
-        if dist:
-            dist.all_reduce(te, op=dist.ReduceOp.MAX)
-        e2e = {"value": world * flops_eff * e2e_steps / (float(te.item()) * 1e-3) / 1e12, "unit": "TFLOP/s",
+        te = max_over_ranks(e0.elapsed_time(e1), dist, dev)
+        e2e = {"value": aggregate_tflops(world, flops_eff * e2e_steps, te), "unit": "TFLOP/s",
                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h), "steps": e2e_steps,
                "path": "shgemm_b200_shgemm_host on page-locked host buffers (copies overlapped with compute)"}
         sg.release_host_staging(h)
