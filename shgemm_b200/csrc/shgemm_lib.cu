@@ -1417,7 +1417,14 @@ int shgemm_b200_shgemm_host(shgemm_b200_handle_t h, int op_a, int op_b, size_t m
         int lvl = SHGEMM_LEVEL_P0;
         const int st = shgemm_b200_shgemm(h, op_a, op_b, m, nbj, k, &alpha, a_d, lda_d, b_s[slot], ldb_d, &beta,
                                           c_s[slot], ldc_d, tc, op_c, &lvl);
-        if (st != SHGEMM_STATUS_OK) return st;
+        if (st != SHGEMM_STATUS_OK) {
+            // join the copy streams before returning, so that nothing of this call is still
+            // reading or writing the staging when the next call on the handle reuses it
+            cudaEventRecord(ev_in[slot], h->host_in);
+            cudaStreamWaitEvent(h->stream, ev_in[slot], 0);
+            for (size_t sl = 0; sl < std::min<size_t>(j, kSlots); ++sl) cudaStreamWaitEvent(h->stream, ev_out[sl], 0);
+            return st;
+        }
         if (j == 0) level = lvl;
         cudaEventRecord(ev_comp[slot], h->stream);
         cudaStreamWaitEvent(h->host_out, ev_comp[slot], 0);
