@@ -128,6 +128,25 @@ int shgemm_b200_shgemm(shgemm_b200_handle_t handle, int op_a, int op_b, size_t m
                        const float* alpha, const float* a, size_t lda, const void* b, size_t ldb,
                        const float* beta, float* c, size_t ldc, int compute_type, int op_c, int* level_out);
 
+/* mtk::shgemm::shgemm with alpha and beta in DEVICE memory (the reference reads them on the
+ * host at call time, src/shgemm.cu:532,600,603; no counterpart there). alpha_dev and beta_dev
+ * are 4-byte aligned device addresses of one float each; the kernels read them when they
+ * run, so a launch captured in a CUDA graph picks up whatever the caller stored there before
+ * each replay. Everything else as shgemm_b200_shgemm, including that C is not read when
+ * *beta_dev == 0; autotuning on first use (SHGEMM_CFG_AUTOTUNE = 2) is skipped, since it
+ * needs beta == 0 known on the host. */
+int shgemm_b200_shgemm_device_scalars(shgemm_b200_handle_t handle, int op_a, int op_b, size_t m, size_t n, size_t k,
+                                      const float* alpha_dev, const float* a, size_t lda, const void* b, size_t ldb,
+                                      const float* beta_dev, float* c, size_t ldc, int compute_type, int op_c,
+                                      int* level_out);
+
+/* hsgemm with device-resident alpha and beta: shgemm_b200_shgemm_device_scalars through
+ * the transposition identity of include/shgemm/shgemm.hpp:121-157. */
+int shgemm_b200_hsgemm_device_scalars(shgemm_b200_handle_t handle, int op_a, int op_b, size_t m, size_t n, size_t k,
+                                      const float* alpha_dev, const void* a, size_t lda, const float* b, size_t ldb,
+                                      const float* beta_dev, float* c, size_t ldc, int compute_type, int op_c,
+                                      int* level_out);
+
 /* SHGEMM on host buffers (no reference counterpart: the reference takes device
  * pointers only). Same arguments, status codes and results as shgemm_b200_shgemm,
  * but a, b and c are host addresses. A is copied to the device once; C is then
@@ -206,6 +225,12 @@ int shgemm_b200_get_config(shgemm_b200_handle_t handle, int key, long long* valu
  * src/shgemm.cu:417). Allocation happens here, never inside shgemm calls. */
 int shgemm_b200_set_workspace_size(shgemm_b200_handle_t handle, size_t bytes);
 
+/* The handle's workspace: its device address and size in bytes (the reference's
+ * w_ptr and max_working_memory_num_elements, include/shgemm/shgemm.hpp:46-92,
+ * src/shgemm.cu:417). Valid until the next shgemm_b200_set_workspace_size or
+ * shgemm_b200_destroy; calls on the handle overwrite its contents. */
+int shgemm_b200_get_workspace(shgemm_b200_handle_t handle, void** ptr, size_t* bytes);
+
 /* Synchronises the handle's stream and reports (then clears) the device-side
  * error word: SHGEMM_STATUS_TIMEOUT when a kernel gave up a bounded wait
  * (*device_code = which role), SHGEMM_STATUS_CUDA_ERROR on a CUDA error.
@@ -253,17 +278,26 @@ int shgemm_b200_eval_error(shgemm_b200_handle_t handle, size_t m, size_t n, cons
  * workspace is allocated). It computes what shgemm_b200_shgemm computes (same
  * kernels, same deterministic split-K), on the current device and the given
  * stream, and allocates nothing: the split-K partials live in a 16 MiB
- * file-scope device array of the library (held on every GPU that loads the
- * library until the process exits) and the error word in another.
+ * file-scope device array of the library and the error word in another. The
+ * driver reserves the arrays on a device when the library's device code is
+ * loaded there -- with CUDA's lazy module loading (the default), during the
+ * first call on that device -- and keeps them until the process exits.
+ * MTK_SHGEMM_KERNEL_LEVEL and MTK_SHGEMM_DEBUG apply as in shgemm_b200_create.
  *  - Limit: m * n <= shgemm_b200_noalloc_scratch_bytes() / 8 (two slices of
  *    FP32 partials); larger problems return SHGEMM_STATUS_SCRATCH_TOO_SMALL.
  *    Operands must be 16-byte aligned with 16-byte aligned leading dimensions
  *    (no staging), else SHGEMM_STATUS_NOT_SUPPORTED.
  *  - The first call on a device sets that device up (resolves the arrays'
- *    device addresses, raises kernel shared-memory limits); make it before any
- *    stream capture.
+ *    device addresses, raises kernel shared-memory limits) and may make the
+ *    driver load the library's device code and reserve the arrays. Make it at
+ *    start-up, while device memory can still be reserved (before a memory
+ *    manager claims the rest, outside allocator callbacks), and before any
+ *    stream capture: one warm-up call on each device is enough.
  *  - Every call shares the arrays: calls that overlap on the GPU (different
  *    streams, or different host threads) race on the partials. Serialise them.
+ *  - The error word is shared too and sticky: a bounded wait that gave up in any
+ *    call stays recorded until shgemm_b200_noalloc_check_error reads and clears
+ *    it. Check after each call whose result you depend on.
  * ------------------------------------------------------------------------ */
 int shgemm_b200_shgemm_noalloc(void* cuda_stream, int op_a, int op_b, size_t m, size_t n, size_t k,
                                const float* alpha, const float* a, size_t lda, const void* b, size_t ldb,
@@ -272,8 +306,9 @@ int shgemm_b200_shgemm_noalloc(void* cuda_stream, int op_a, int op_b, size_t m, 
 /* Size of the allocation-free path's scratch array in bytes. No counterpart in the reference. */
 size_t shgemm_b200_noalloc_scratch_bytes(void);
 
-/* Synchronises `cuda_stream` and reports the allocation-free path's device error
- * word (as shgemm_b200_check_error does for a handle). No counterpart in the reference. */
+/* Synchronises `cuda_stream` and reports (then clears) the allocation-free path's
+ * device error word, as shgemm_b200_check_error does for a handle. No counterpart
+ * in the reference. */
 int shgemm_b200_noalloc_check_error(void* cuda_stream, int* device_code);
 
 /* ------------------------------------------------------------------------
@@ -328,6 +363,11 @@ typedef struct {
     size_t peak_resident_bytes;             /* max over time of the admitted A + Omega + Y bytes */
     size_t resident_bytes;
     unsigned long long queued, in_flight;   /* now */
+    /* Device-side timing (CUDA events on the server's streams), completed batches only:
+     * kernel_busy_s = time during which at least one grouped SHGEMM launch was running
+     * (the union of their intervals), omega_s = summed time of the Omega generation. */
+    double kernel_busy_s, omega_s;
+    unsigned long long launches;            /* kernels enqueued: grouped launches + Omega generations */
 } shgemm_b200_server_stats;
 
 /* Starts a server thread on `device` that admits requests first-come first-served

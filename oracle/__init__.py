@@ -58,12 +58,17 @@ def lib() -> ctypes.CDLL:
         L.oracle_split.argtypes = [i, p, sz, p, p]
         L.oracle_shgemm.restype = i
         L.oracle_shgemm.argtypes = [i, i, i, sz, sz, sz, f, p, sz, p, sz, f, p, sz, i, sz]
+        L.oracle_shgemm_tcmodel.restype = i
+        L.oracle_shgemm_tcmodel.argtypes = [i, i, i, sz, sz, sz, f, p, sz, p, sz, f, p, sz, i, sz]
         L.oracle_dgemm_ref.restype = i
         L.oracle_dgemm_ref.argtypes = [i, i, sz, sz, sz, d, p, sz, p, sz, d, p, sz, i, p]
         L.oracle_sgemm.restype = i
         L.oracle_sgemm.argtypes = [i, i, sz, sz, sz, f, p, sz, p, sz, f, p, sz, i]
         L.oracle_num_threads.restype = i
         L.oracle_num_threads.argtypes = []
+        for fn in (L.oracle_cpu_sgemm, L.oracle_cpu_dgemm):
+            fn.restype = None
+            fn.argtypes = [sz, sz, sz, p, sz, p, sz, p, sz]
         _lib = L
     return _lib
 
@@ -104,26 +109,36 @@ def split(tc: int, x) -> tuple[np.ndarray, np.ndarray]:
     return hi, lo
 
 
-def shgemm(tc, op_a, op_b, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, op_c=OP_N, chunk=0):
+IDEAL, TCMODEL = "ideal", "tcmodel"
+
+
+def shgemm(tc, op_a, op_b, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, op_c=OP_N, chunk=0, model=IDEAL):
     """Restated reference SHGEMM on column-major flat buffers; C is updated in place.
 
-    ``B`` holds binary16 values (np.float16 or their uint16 bits).
+    ``B`` holds binary16 values (np.float16 or their uint16 bits). ``model``: IDEAL sums
+    each hi fragment exactly and accumulates lo exactly (oracle_shgemm); TCMODEL models
+    the reference's tensor-core accumulation -- hi fragments truncated to FP32 before
+    their round-to-nearest add, lo in a truncating FP32 accumulator over all k
+    (oracle_shgemm_tcmodel, src/wmmae_shgemm.hpp:86-124).
     """
     A = _f32(A)
     B = _u16(B)
     assert C.dtype == np.float32 and C.flags.c_contiguous
-    rc = lib().oracle_shgemm(tc, op_a, op_b, m, n, k, alpha, _ptr(A), lda, _ptr(B), ldb,
-                             beta, _ptr(C), ldc, op_c, chunk)
+    fn = lib().oracle_shgemm if model == IDEAL else lib().oracle_shgemm_tcmodel
+    if model not in (IDEAL, TCMODEL):
+        raise ValueError(model)
+    rc = fn(tc, op_a, op_b, m, n, k, alpha, _ptr(A), lda, _ptr(B), ldb, beta, _ptr(C), ldc, op_c, chunk)
     if rc != 0:
         raise MemoryError("oracle_shgemm: allocation failed")
     return C
 
 
-def hsgemm(tc, op_a, op_b, m, n, k, alpha, A_half, lda, B_float, ldb, beta, C, ldc, op_c=OP_N, chunk=0):
+def hsgemm(tc, op_a, op_b, m, n, k, alpha, A_half, lda, B_float, ldb, beta, C, ldc, op_c=OP_N, chunk=0,
+           model=IDEAL):
     """HSGEMM through the transposition identity of include/shgemm/shgemm.hpp:121-157."""
     inv = lambda op: OP_T if op == OP_N else OP_N  # noqa: E731
     return shgemm(tc, inv(op_b), inv(op_a), n, m, k, alpha, B_float, ldb, A_half, lda,
-                  beta, C, ldc, inv(op_c), chunk)
+                  beta, C, ldc, inv(op_c), chunk, model)
 
 
 def dgemm_ref(op_a, op_b, m, n, k, alpha, A, lda, B, ldb, beta=0.0, Cin=None, ldc=0, op_c=OP_N):
@@ -147,6 +162,17 @@ def sgemm(op_a, op_b, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, op_c=OP_N):
                             _ptr(C), ldc, op_c)
     if rc != 0:
         raise MemoryError("oracle_sgemm: allocation failed")
+    return C
+
+
+def cpu_gemm(A, B, m, n, k, dtype=np.float64) -> np.ndarray:
+    """Plain OpenMP GEMM C = A B (column-major flat buffers, A m x k, B k x n) in FP32 or
+    FP64: the timed CPU baseline, not a checker. Returns C flat (ld = m)."""
+    A = np.ascontiguousarray(A, dtype=dtype)
+    B = np.ascontiguousarray(B, dtype=dtype)
+    C = np.empty(m * n, dtype=dtype)
+    fn = lib().oracle_cpu_dgemm if dtype == np.float64 else lib().oracle_cpu_sgemm
+    fn(m, n, k, _ptr(A), m, _ptr(B), k, _ptr(C), m)
     return C
 
 

@@ -27,6 +27,11 @@
  *    for tf32 in the reference; the B200 kernel's k-chunk when modelling it).
  *    Products of split values are exact in FP64; a fragment sum is modelled as
  *    the exact sum rounded once to FP32.
+ *    That is oracle_shgemm, the idealised form. oracle_shgemm_tcmodel models
+ *    the tensor core's accumulation as the reference meets it instead: each
+ *    hi fragment sum truncated (rounded toward zero) to FP32 before its
+ *    round-to-nearest add, and lo kept in an FP32 accumulator across all k
+ *    that takes each fragment's sum with truncation.
  *  - fold, tcec store_matrix_sync at src/shgemm.cu:87-99: c = hi + lo * 2^-11.
  *  - epilogue, src/dmem_accessor.hpp:267-271 (beta != 0) and 199-214
  *    (beta == 0, C is not read): alpha * c + beta * C.
@@ -190,6 +195,66 @@ int oracle_shgemm(int tc, int op_a, int op_b, size_t m, size_t n, size_t k, floa
     return 0;
 }
 
+/* FP32 value of a double rounded toward zero (the tensor core's truncating
+ * accumulation is modelled as exact products and sums rounded this way). */
+static inline float rz_f32(double d) {
+    float f = (float)d; /* round to nearest */
+    if (isfinite(f) && fabs((double)f) > fabs(d)) f = nextafterf(f, 0.0f);
+    return f;
+}
+
+/*
+ * Restated reference SHGEMM with the tensor core's accumulation modelled as the
+ * reference meets it (src/wmmae_shgemm.hpp:86-124), rather than exactly:
+ *  - hi: per k-fragment of `chunk` (16 for fp16, 8 for tf32: one mma_sync), the
+ *    product is formed on the tensor core from a zero accumulator -- modelled as
+ *    the exact fragment sum rounded toward zero to FP32 -- and added to the FP32
+ *    running sum with a round-to-nearest add (src/wmmae_shgemm.hpp:89-97,106-114);
+ *  - lo: accumulated on the tensor core across ALL k, D_lo = A_lo B + D_lo
+ *    (src/wmmae_shgemm.hpp:116-121) -- modelled as an FP32 accumulator to which
+ *    each fragment's exact sum is added with rounding toward zero;
+ *  - fold c = hi + lo * 2^-11 (tcec store, call site src/shgemm.cu:87-99), then the
+ *    same epilogue as oracle_shgemm.
+ * Products of split values with binary16 values are exact in FP64.
+ */
+int oracle_shgemm_tcmodel(int tc, int op_a, int op_b, size_t m, size_t n, size_t k, float alpha,
+                          const float* A, size_t lda, const uint16_t* B, size_t ldb, float beta,
+                          float* C, size_t ldc, int op_c, size_t chunk) {
+    if (chunk == 0) chunk = (tc == TC_FP16) ? 16 : 8;
+    float* a = (float*)malloc(sizeof(float) * (m * k + 1));
+    float* ahi = (float*)malloc(sizeof(float) * (m * k + 1));
+    float* alo = (float*)malloc(sizeof(float) * (m * k + 1));
+    float* b = (float*)malloc(sizeof(float) * (n * k + 1));
+    if (!a || !ahi || !alo || !b) { free(a); free(ahi); free(alo); free(b); return 1; }
+    pack_a(op_a, m, k, A, lda, a);
+    oracle_split(tc, a, m * k, ahi, alo);
+    pack_b_f16(op_b, k, n, B, ldb, b);
+#pragma omp parallel for collapse(2) schedule(static)
+    for (size_t j = 0; j < n; j++) {
+        for (size_t i = 0; i < m; i++) {
+            const float* ah = ahi + i * k;
+            const float* al = alo + i * k;
+            const float* bj = b + j * k;
+            float acc = 0.0f, lo = 0.0f;
+            for (size_t k0 = 0; k0 < k; k0 += chunk) {
+                const size_t k1 = (k0 + chunk < k) ? k0 + chunk : k;
+                double s = 0.0, t = 0.0;
+                for (size_t kk = k0; kk < k1; kk++) {
+                    s += (double)ah[kk] * (double)bj[kk];
+                    t += (double)al[kk] * (double)bj[kk];
+                }
+                acc = acc + rz_f32(s);
+                lo = rz_f32((double)lo + t);
+            }
+            const float c = acc + lo * (1.0f / 2048.0f);
+            float* cp = C + c_index(op_c, i, j, ldc);
+            *cp = epilogue(c, alpha, beta, cp);
+        }
+    }
+    free(a); free(ahi); free(alo); free(b);
+    return 0;
+}
+
 /*
  * FP64 GEMM of the same FP32 / binary16 inputs (the error reference):
  * C64 = alpha * op(A) * op(B) + beta * Cin, all in double.  Cin may be NULL
@@ -251,6 +316,38 @@ int oracle_sgemm(int op_a, int op_b, size_t m, size_t n, size_t k, float alpha,
     }
     free(a); free(b);
     return 0;
+}
+
+/*
+ * Plain OpenMP GEMMs in FP32 and FP64 for the timed CPU baseline (not checkers):
+ * C = A B, column-major, A m x k (lda), B k x n (ldb), C m x n (ldc), C overwritten.
+ * Threads split the columns of C; each walks k in blocks of 256 so the block of A
+ * stays in cache, with the innermost loop down a column (contiguous, vectorisable).
+ */
+#define CPU_GEMM_KB 256
+#define CPU_GEMM_BODY(T)                                                           \
+    _Pragma("omp parallel for schedule(dynamic, 4)")                               \
+    for (size_t j = 0; j < n; j++) {                                               \
+        T* cj = C + j * ldc;                                                       \
+        for (size_t i = 0; i < m; i++) cj[i] = (T)0;                               \
+        for (size_t k0 = 0; k0 < k; k0 += CPU_GEMM_KB) {                           \
+            const size_t k1 = (k0 + CPU_GEMM_KB < k) ? k0 + CPU_GEMM_KB : k;       \
+            for (size_t kk = k0; kk < k1; kk++) {                                  \
+                const T b = B[kk + j * ldb];                                       \
+                const T* ak = A + kk * lda;                                        \
+                for (size_t i = 0; i < m; i++) cj[i] += ak[i] * b;                 \
+            }                                                                      \
+        }                                                                          \
+    }
+
+void oracle_cpu_sgemm(size_t m, size_t n, size_t k, const float* A, size_t lda, const float* B, size_t ldb,
+                      float* C, size_t ldc) {
+    CPU_GEMM_BODY(float)
+}
+
+void oracle_cpu_dgemm(size_t m, size_t n, size_t k, const double* A, size_t lda, const double* B, size_t ldb,
+                      double* C, size_t ldc) {
+    CPU_GEMM_BODY(double)
 }
 
 /* Number of OpenMP threads the oracle runs with (for the CPU-baseline report). */

@@ -17,7 +17,8 @@ import os
 __all__ = [
     "op_n", "op_t", "fp16", "tf32", "P0", "P1", "ShgemmError", "Handle", "create", "destroy",
     "set_cuda_stream", "enable_kernel_level_fixing", "disable_kernel_level_fixing", "set_debug_mode",
-    "shgemm", "hsgemm", "shgemm_host", "hsgemm_host", "release_host_staging", "library_path",
+    "shgemm", "hsgemm", "shgemm_device_scalars", "hsgemm_device_scalars", "shgemm_host", "hsgemm_host",
+    "release_host_staging", "library_path",
 ]
 
 op_n, op_t = 0, 1          # operation_t (include/shgemm/shgemm.hpp:36-39)
@@ -82,12 +83,15 @@ def lib() -> ctypes.CDLL:
         "shgemm_b200_set_debug_mode": [vp, ctypes.c_uint],
         "shgemm_b200_shgemm": [vp, i, i, sz, sz, sz, pf, vp, sz, vp, sz, pf, vp, sz, i, i, pi],
         "shgemm_b200_hsgemm": [vp, i, i, sz, sz, sz, pf, vp, sz, vp, sz, pf, vp, sz, i, i, pi],
+        "shgemm_b200_shgemm_device_scalars": [vp, i, i, sz, sz, sz, vp, vp, sz, vp, sz, vp, vp, sz, i, i, pi],
+        "shgemm_b200_hsgemm_device_scalars": [vp, i, i, sz, sz, sz, vp, vp, sz, vp, sz, vp, vp, sz, i, i, pi],
         "shgemm_b200_shgemm_host": [vp, i, i, sz, sz, sz, pf, vp, sz, vp, sz, pf, vp, sz, i, i, pi],
         "shgemm_b200_release_host_staging": [vp],
         "shgemm_b200_hsgemm_host": [vp, i, i, sz, sz, sz, pf, vp, sz, vp, sz, pf, vp, sz, i, i, pi],
         "shgemm_b200_set_config": [vp, i, ctypes.c_longlong],
         "shgemm_b200_get_config": [vp, i, ctypes.POINTER(ctypes.c_longlong)],
         "shgemm_b200_set_workspace_size": [vp, sz],
+        "shgemm_b200_get_workspace": [vp, ctypes.POINTER(vp), ctypes.POINTER(sz)],
         "shgemm_b200_check_error": [vp, pi],
         "shgemm_b200_get_launch_count": [vp, ctypes.POINTER(ctypes.c_longlong)],
         "shgemm_b200_selftest_wait_timeout": [vp, ctypes.c_uint, pi],
@@ -190,6 +194,12 @@ class Handle:
     def set_workspace_size(self, nbytes: int) -> None:
         _check(lib().shgemm_b200_set_workspace_size(self.ptr, nbytes), "set_workspace_size")
 
+    def workspace(self) -> tuple[int, int]:
+        """(device address, bytes) of the handle's workspace (the reference's w_ptr)."""
+        p, n = ctypes.c_void_p(), ctypes.c_size_t()
+        _check(lib().shgemm_b200_get_workspace(self.ptr, ctypes.byref(p), ctypes.byref(n)), "get_workspace")
+        return int(p.value or 0), int(n.value)
+
     def check_error(self) -> int:
         """Synchronises and returns the device error code (0 = none)."""
         code = ctypes.c_int()
@@ -284,6 +294,29 @@ def hsgemm(handle: Handle, op_a: int, op_b: int, m: int, n: int, k: int, alpha: 
     st = lib().shgemm_b200_hsgemm(handle.ptr, op_a, op_b, m, n, k, ctypes.byref(al), _addr(a), lda, _addr(b), ldb,
                                   ctypes.byref(be), _addr(c), ldc, compute_type, op_c, ctypes.byref(lv))
     _check(st, "hsgemm")
+    return lv.value
+
+
+def shgemm_device_scalars(handle: Handle, op_a: int, op_b: int, m: int, n: int, k: int, alpha_dev, a, lda: int, b,
+                          ldb: int, beta_dev, c, ldc: int, compute_type: int, op_c: int = op_n) -> int:
+    """shgemm with alpha and beta read from device memory by the kernels (one float each,
+    e.g. 1-element CUDA tensors): a captured CUDA graph replays with whatever they hold."""
+    lv = ctypes.c_int(0)
+    st = lib().shgemm_b200_shgemm_device_scalars(handle.ptr, op_a, op_b, m, n, k, _addr(alpha_dev), _addr(a), lda,
+                                                 _addr(b), ldb, _addr(beta_dev), _addr(c), ldc, compute_type, op_c,
+                                                 ctypes.byref(lv))
+    _check(st, "shgemm_device_scalars")
+    return lv.value
+
+
+def hsgemm_device_scalars(handle: Handle, op_a: int, op_b: int, m: int, n: int, k: int, alpha_dev, a, lda: int, b,
+                          ldb: int, beta_dev, c, ldc: int, compute_type: int, op_c: int = op_n) -> int:
+    """hsgemm (A binary16, B FP32) with device-resident alpha and beta."""
+    lv = ctypes.c_int(0)
+    st = lib().shgemm_b200_hsgemm_device_scalars(handle.ptr, op_a, op_b, m, n, k, _addr(alpha_dev), _addr(a), lda,
+                                                 _addr(b), ldb, _addr(beta_dev), _addr(c), ldc, compute_type, op_c,
+                                                 ctypes.byref(lv))
+    _check(st, "hsgemm_device_scalars")
     return lv.value
 
 

@@ -41,8 +41,12 @@ void mtk::shgemm::create(mtk::shgemm::shgemmHandle_t& handle) {
 	if (kl && (kl[0] == '0' || kl[0] == '1') && kl[1] == '\0') {
 		handle.fixed_lernel_level = static_cast<mtk::shgemm::detail::kernel_level>(kl[0] - '0');
 	}
-	handle.max_working_memory_num_elements = (std::size_t(64) << 20) / sizeof(float);
-	handle.w_ptr = nullptr;
+	// The handle's live workspace, like the reference's cudaMalloc'd w_ptr (src/shgemm.cu:417).
+	void* w = nullptr;
+	std::size_t w_bytes = 0;
+	if (shgemm_b200_get_workspace(h, &w, &w_bytes) != SHGEMM_STATUS_OK) w_bytes = 0;
+	handle.w_ptr = w_bytes ? static_cast<float*>(w) : nullptr;
+	handle.max_working_memory_num_elements = handle.w_ptr ? w_bytes / sizeof(float) : 0;
 }
 
 void mtk::shgemm::destroy(mtk::shgemm::shgemmHandle_t& handle) {

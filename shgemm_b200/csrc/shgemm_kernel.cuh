@@ -64,6 +64,10 @@ struct alignas(64) TileGemmParams {
     int m, n, k;
     int op_c;
     float alpha, beta;
+    // Device-resident scalars (both null: alpha and beta above). Read when a tile's epilogue
+    // starts, so a captured launch picks up whatever the caller stored there since.
+    const float* alpha_dev;
+    const float* beta_dev;
     int tiles_m, tiles_n;
     int num_slices;       // split-K slices (1: the epilogue writes C)
     int steps_per_slice;  // k-steps per slice
@@ -173,6 +177,10 @@ struct alignas(64) GroupedParams {
     int* error_flag;
     uint64_t wait_limit_ns;
     int op_c;
+    // Device-resident scalars for every problem of the launch (both null: each problem's
+    // alpha and beta), read once by each epilogue warp when the kernel starts.
+    const float* alpha_dev;
+    const float* beta_dev;
 };
 
 // What one work unit (a 128 x bn tile of one problem over a range of k-steps) needs.
@@ -189,6 +197,22 @@ struct UnitDesc {
     float alpha, beta;
     bool maps_in_global;  // descriptors written by a copy before the launch
 };
+
+// Device-resident alpha and beta of a launch, read once per epilogue warp; `on` false when
+// the launch passes host scalars (each unit's alpha and beta then apply).
+struct DevScalarValues {
+    bool on;
+    float alpha, beta;
+};
+template <class Params>
+__device__ __forceinline__ DevScalarValues load_dev_scalars(const Params& p) {
+    DevScalarValues v{p.alpha_dev != nullptr, 0.0f, 0.0f};
+    if (v.on) {
+        v.alpha = *p.alpha_dev;
+        v.beta = *p.beta_dev;
+    }
+    return v;
+}
 
 template <class Cfg>
 __device__ __forceinline__ void get_unit(const TileGemmParams& p, int u, UnitDesc& d) {
@@ -886,6 +910,7 @@ __device__ __forceinline__ void tile_kernel_body(const Params& p) {
     } else {
         // ------------------------------------------------------------ epilogue
         ptx::setmaxnreg_inc<Cfg::EPI_REGS>();
+        const DevScalarValues dsc = load_dev_scalars(p);
         constexpr int HN = Cfg::HALF_N;
         const int q = warp & 3;                         // TMEM lane quadrant this warp may access
         const int half = (warp - Cfg::EPI_WARP0) >> 2;  // column half of the tile
@@ -902,7 +927,7 @@ __device__ __forceinline__ void tile_kernel_body(const Params& p) {
                 // beta != 0: C of this thread's row into L2 (kept there) while the tile's k-steps run
                 const int row = ud.tm * Cfg::BM + row_in_tile;
                 const int col0 = ud.tn * ud.bn + half * hn;
-                if (ud.beta != 0.0f && !ud.partial && row < ud.m)
+                if ((dsc.on ? dsc.beta : ud.beta) != 0.0f && !ud.partial && row < ud.m)
                     prefetch_row<HN>(ud.c, ud.ldc, output_op(p), row, col0, ud.n < col0 + hn ? ud.n : col0 + hn);
             }
             uint64_t acc2[HN / 2];  // running sums, packed in pairs of columns
@@ -955,7 +980,8 @@ __device__ __forceinline__ void tile_kernel_body(const Params& p) {
                     } else {
                         // columns of this warp's half only (a grouped problem's tile may be narrower)
                         const int n_end = ud.n < col0 + hn ? ud.n : col0 + hn;
-                        store_row<HN>(ud.c, ud.ldc, output_op(p), row, col0, n_end, ud.alpha, ud.beta, acc);
+                        store_row<HN>(ud.c, ud.ldc, output_op(p), row, col0, n_end, dsc.on ? dsc.alpha : ud.alpha,
+                                      dsc.on ? dsc.beta : ud.beta, acc);
                     }
                 }
             }

@@ -227,6 +227,7 @@ __device__ __forceinline__ void tm_kernel_body(const Params& p) {
     } else if (warp < Cfg::CTRL_WARP0) {
         // ---------------------------------------------------------------- epilogue
         ptx::setmaxnreg_inc<Cfg::EPI_REGS>();
+        const DevScalarValues dsc = load_dev_scalars(p);
         const int q = warp & 3;
         const int cq = (warp - Cfg::EPI_WARP0) >> 2;  // 64-column quarter within each half
         const int row_in_tile = q * 32 + lane;
@@ -240,7 +241,7 @@ __device__ __forceinline__ void tm_kernel_body(const Params& p) {
                 nsteps = ud.s1 - ud.s0;
                 // beta != 0: C of this thread's row into L2 (kept there) while the tile's k-steps run
                 const int row = ud.tm * Cfg::BM + row_in_tile;
-                if (ud.beta != 0.0f && !ud.partial && row < ud.m) {
+                if ((dsc.on ? dsc.beta : ud.beta) != 0.0f && !ud.partial && row < ud.m) {
 #pragma unroll
                     for (int h = 0; h < 2; ++h)
                         prefetch_row<64>(ud.c, ud.ldc, output_op(p), row, ud.tn * Cfg::BN + h * Cfg::HALF_N + cq * 64,
@@ -298,7 +299,8 @@ __device__ __forceinline__ void tm_kernel_body(const Params& p) {
                                 if (col < ud.n) w[static_cast<size_t>(col) * ud.m] = acc(h * 64 + j);
                             }
                         } else {
-                            store_row<64>(ud.c, ud.ldc, output_op(p), row, col0, ud.n, ud.alpha, ud.beta,
+                            store_row<64>(ud.c, ud.ldc, output_op(p), row, col0, ud.n, dsc.on ? dsc.alpha : ud.alpha,
+                                          dsc.on ? dsc.beta : ud.beta,
                                           [&](int j) { return acc(h * 64 + j); });
                         }
                     }

@@ -22,6 +22,20 @@
 
 using namespace shgemm_b200;
 
+// The tables of a grouped launch: the device copy the kernel reads and its pinned host
+// staging, each holding the problems, then the unit list, then the unit count at fixed
+// offsets, so that a captured graph's copy replays whatever the staging holds.
+struct GroupedTable {
+    void* dev = nullptr;
+    void* host = nullptr;
+    cudaEvent_t copied = nullptr;  // the last eager copy out of the staging
+    int max_problems = 0;
+    size_t units_off = 0, count_off = 0, bytes = 0;
+    int tc = -1, op_a = -1, op_b = -1, op_c = -1, b32 = -1;  // variant of the staged batch
+    int units = 0;
+    int copied_count = 0;  // problem slots the last enqueued copy covers
+};
+
 struct shgemm_b200_handle {
     int device = 0;
     int num_sms = 148;
@@ -35,14 +49,11 @@ struct shgemm_b200_handle {
     size_t workspace_bytes = 0;
     int* error_word = nullptr;
     std::atomic<long long> launches{0};
-    // grouped launches: problem table + unit list, device copy and pinned host staging
-    void* grouped_dev = nullptr;
-    void* grouped_host = nullptr;
-    cudaEvent_t grouped_copied = nullptr;
-    int grouped_tc = -1, grouped_op_a = -1, grouped_op_b = -1, grouped_op_c = -1, grouped_b32 = -1;
+    // grouped launches: the caller's batches (which captured graphs replay) and, apart from
+    // them, the one-problem table of eager TF32 calls that take the widened-B route
+    GroupedTable grouped;
+    GroupedTable single;
     int grouped_b_fp32 = 0;  // SHGEMM_CFG_GROUPED_B_FP32
-    int grouped_units = 0;
-    int grouped_copied_count = 0;  // problem slots the last enqueued copy covers
     // autotuner: best (tile N, split-K slices, rasterisation group) per shape bucket
     int autotune_mode = 1;  // SHGEMM_CFG_AUTOTUNE
     int tile_kernel = 0;    // SHGEMM_CFG_TILE_KERNEL
@@ -186,13 +197,34 @@ KernelEntry grouped_table(int tc, int ak, bool b_wide) {
 // Table layout (device copy and host staging): problems, then units, then the unit count.
 constexpr int kGroupedMaxProblems = 8192;
 constexpr int kGroupedMaxUnits = 1 << 16;
-constexpr size_t kGroupedUnitsOff = sizeof(GroupedProblem) * kGroupedMaxProblems;
-constexpr size_t kGroupedCountOff = kGroupedUnitsOff + sizeof(int2) * kGroupedMaxUnits;
-constexpr size_t kGroupedBytes = kGroupedCountOff + 256;
+
+bool table_alloc(GroupedTable& t, int max_problems) {
+    t.max_problems = max_problems;
+    t.units_off = sizeof(GroupedProblem) * static_cast<size_t>(max_problems);
+    t.count_off = t.units_off + sizeof(int2) * kGroupedMaxUnits;
+    t.bytes = t.count_off + 256;
+    if (cudaMalloc(&t.dev, t.bytes) != cudaSuccess || cudaMallocHost(&t.host, t.bytes) != cudaSuccess ||
+        cudaEventCreateWithFlags(&t.copied, cudaEventDisableTiming) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return true;
+}
+
+void table_free(GroupedTable& t) {
+    if (t.copied) {
+        cudaEventSynchronize(t.copied);
+        cudaEventDestroy(t.copied);
+    }
+    cudaFree(t.dev);
+    cudaFreeHost(t.host);
+    t = GroupedTable{};
+}
 
 // ------------------------------------------------------------------ small kernels
-// C = beta * C (k == 0: the product is empty).
-__global__ void scale_c_kernel(float* c, uint64_t ldc, int rows, int cols, float beta) {
+// C = beta * C (k == 0: the product is empty); beta from device memory when beta_dev is set.
+__global__ void scale_c_kernel(float* c, uint64_t ldc, int rows, int cols, float beta, const float* beta_dev) {
+    if (beta_dev) beta = *beta_dev;
     const size_t total = static_cast<size_t>(rows) * cols;
     for (size_t idx = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; idx < total;
          idx += static_cast<size_t>(gridDim.x) * blockDim.x) {
@@ -260,7 +292,10 @@ __global__ void block_b_kernel(const __half* __restrict__ src, uint64_t ldb, __h
 // Deterministic split-K reduction: slices summed in fixed order 0..S-1, then the
 // same alpha/beta epilogue as the tile kernel (C is not read when beta == 0).
 __global__ void splitk_reduce_kernel(const float* __restrict__ ws, int slices, int m, int n, float* c,
-                                     uint64_t ldc, int op_c, float alpha, float beta) {
+                                     uint64_t ldc, int op_c, float alpha, float beta, const float* alpha_dev,
+                                     const float* beta_dev) {
+    if (alpha_dev) alpha = *alpha_dev;
+    if (beta_dev) beta = *beta_dev;
     const size_t mn = static_cast<size_t>(m) * n;
     for (size_t idx = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; idx < mn;
          idx += static_cast<size_t>(gridDim.x) * blockDim.x) {
@@ -633,12 +668,11 @@ int shgemm_b200_create(shgemm_b200_handle_t* out, int device) {
                 KernelEntry e = grouped_table(tc, ak, bw != 0);
                 cudaFuncSetAttribute(e.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, e.smem);
             }
-    if (cudaGetLastError() != cudaSuccess || cudaMalloc(&h->grouped_dev, kGroupedBytes) != cudaSuccess ||
-        cudaMallocHost(&h->grouped_host, kGroupedBytes) != cudaSuccess ||
-        cudaEventCreateWithFlags(&h->grouped_copied, cudaEventDisableTiming) != cudaSuccess) {
+    if (cudaGetLastError() != cudaSuccess || !table_alloc(h->grouped, kGroupedMaxProblems) ||
+        !table_alloc(h->single, 1)) {
         cudaGetLastError();
-        cudaFree(h->grouped_dev);
-        cudaFreeHost(h->grouped_host);
+        table_free(h->grouped);
+        table_free(h->single);
         cudaFree(h->workspace);
         cudaFree(h->error_word);
         delete h;
@@ -656,12 +690,8 @@ int shgemm_b200_destroy(shgemm_b200_handle_t h) {
         if (e) cudaEventDestroy(e);
     if (h->host_in) cudaStreamDestroy(h->host_in);
     if (h->host_out) cudaStreamDestroy(h->host_out);
-    if (h->grouped_copied) {
-        cudaEventSynchronize(h->grouped_copied);
-        cudaEventDestroy(h->grouped_copied);
-    }
-    cudaFree(h->grouped_dev);
-    cudaFreeHost(h->grouped_host);
+    table_free(h->grouped);
+    table_free(h->single);
     cudaFree(h->workspace);
     cudaFree(h->error_word);
     delete h;
@@ -756,6 +786,13 @@ int shgemm_b200_set_workspace_size(shgemm_b200_handle_t h, size_t bytes) {
     return SHGEMM_STATUS_OK;
 }
 
+int shgemm_b200_get_workspace(shgemm_b200_handle_t h, void** ptr, size_t* bytes) {
+    if (!h || !ptr || !bytes) return SHGEMM_STATUS_INVALID_VALUE;
+    *ptr = h->workspace;
+    *bytes = h->workspace_bytes;
+    return SHGEMM_STATUS_OK;
+}
+
 int shgemm_b200_check_error(shgemm_b200_handle_t h, int* device_code) {
     if (!h) return SHGEMM_STATUS_INVALID_VALUE;
     DeviceGuard g(h->device);
@@ -804,10 +841,16 @@ int shgemm_b200_selftest_wait_timeout(shgemm_b200_handle_t h, unsigned limit_us,
 
 }  // extern "C"
 
+// Device-resident scalars for one call: each pointer, when set, replaces alpha or beta.
+struct DevScalars {
+    const float* alpha = nullptr;
+    const float* beta = nullptr;
+};
+
 static int run_tiled(shgemm_b200_handle_t h, int op_a, int op_b, size_t m, size_t n, size_t k, float alpha,
                      const float* a, size_t lda, const void* b, size_t ldb, float beta, float* c, size_t ldc, int tc,
                      int op_c, int* level_out, float* splitk_ws, size_t splitk_bytes,
-                     const shgemm_b200_tuned_config* force = nullptr) {
+                     const shgemm_b200_tuned_config* force = nullptr, DevScalars dev = DevScalars{}) {
     int group_m = 8;
     const bool a_kmajor = (op_a == kOpT);
     const bool b_kmajor = (op_b == kOpN);
@@ -887,6 +930,8 @@ static int run_tiled(shgemm_b200_handle_t h, int op_a, int op_b, size_t m, size_
     P.op_c = op_c;
     P.alpha = alpha;
     P.beta = beta;
+    P.alpha_dev = dev.alpha;
+    P.beta_dev = dev.beta;
     P.tiles_m = pl.tiles_m;
     P.tiles_n = pl.tiles_n;
     P.num_slices = pl.slices;
@@ -924,7 +969,8 @@ static int run_tiled(shgemm_b200_handle_t h, int op_a, int op_b, size_t m, size_
     if (pl.slices > 1) {
         const size_t mn = m * n;
         const int blocks = static_cast<int>(std::min<size_t>((mn + 255) / 256, size_t(h->num_sms) * 8));
-        splitk_reduce_kernel<<<blocks, 256, 0, h->stream>>>(part_ws, pl.slices, P.m, P.n, c, ldc, op_c, alpha, beta);
+        splitk_reduce_kernel<<<blocks, 256, 0, h->stream>>>(part_ws, pl.slices, P.m, P.n, c, ldc, op_c, alpha, beta,
+                                                            dev.alpha, dev.beta);
         h->launches++;
         if (launch_status() != SHGEMM_STATUS_OK) return SHGEMM_STATUS_LAUNCH_FAILED;
     }
@@ -950,10 +996,15 @@ static void launch_pack(shgemm_b200_handle_t h, const T* src, size_t ld_src, T* 
 // grouped launch replays whatever table the handle stages later), when the workspace
 // holds the widened B, and when 128 x 256 tiles fill the GPU (no split-K wanted);
 // otherwise SHGEMM_STATUS_NOT_SUPPORTED and the caller uses the tile kernel.
+// Stages a batch into table `t` and enqueues its copy and one grouped launch (defined with
+// the grouped entry points below).
+static int grouped_run(shgemm_b200_handle_t h, GroupedTable& t, bool b_wide, int op_a, int op_b, int tc, int op_c,
+                       const shgemm_b200_problem* probs, int count, DevScalars dev = DevScalars{});
+
 static int tf32_widened_b(shgemm_b200_handle_t h, int op_a, int op_b, size_t m, size_t n, size_t k, float alpha,
                           const float* a, size_t lda, const void* b, size_t ldb, float beta, float* c, size_t ldc,
-                          int op_c, int* level_out) {
-    if (op_b != kOpN || !h->grouped_dev || h->tile_kernel != 0 || h->fixed_level != SHGEMM_LEVEL_AUTO ||
+                          int op_c, int* level_out, DevScalars dev) {
+    if (op_b != kOpN || !h->single.dev || h->tile_kernel != 0 || h->fixed_level != SHGEMM_LEVEL_AUTO ||
         h->split_k > 1)
         return SHGEMM_STATUS_NOT_SUPPORTED;
     const size_t ldw = (k + 3) / 4 * 4;
@@ -983,20 +1034,18 @@ static int tf32_widened_b(shgemm_b200_handle_t h, int op_a, int op_b, size_t m, 
     q.ldc = ldc;
     q.alpha = alpha;
     q.beta = beta;
-    const int saved = h->grouped_b_fp32;
-    h->grouped_b_fp32 = 1;
-    const int st = shgemm_b200_shgemm_grouped(h, op_a, kOpN, kTF32, op_c, &q, 1);
-    h->grouped_b_fp32 = saved;
+    // the handle's own one-problem table: the caller's grouped staging, which a captured
+    // graph may replay, is left untouched
+    const int st = grouped_run(h, h->single, true, op_a, kOpN, kTF32, op_c, &q, 1, dev);
     if (st == SHGEMM_STATUS_OK && level_out) *level_out = SHGEMM_LEVEL_P1;
     return st;
 }
 
-extern "C" {
-
-int shgemm_b200_shgemm(shgemm_b200_handle_t h, int op_a, int op_b, size_t m, size_t n, size_t k,
-                       const float* alpha_ptr, const float* a, size_t lda, const void* b, size_t ldb,
-                       const float* beta_ptr, float* c, size_t ldc, int tc, int op_c, int* level_out) {
-    if (!h || !alpha_ptr || !beta_ptr) return SHGEMM_STATUS_INVALID_VALUE;
+// The dispatch behind shgemm_b200_shgemm (host scalars: alpha, beta) and
+// shgemm_b200_shgemm_device_scalars (dev.alpha / dev.beta device addresses, read by the kernels).
+static int shgemm_impl(shgemm_b200_handle_t h, int op_a, int op_b, size_t m, size_t n, size_t k, float alpha,
+                       const float* a, size_t lda, const void* b, size_t ldb, float beta, float* c, size_t ldc,
+                       int tc, int op_c, int* level_out, DevScalars dev) {
     if ((op_a != kOpN && op_a != kOpT) || (op_b != kOpN && op_b != kOpT) || (op_c != kOpN && op_c != kOpT) ||
         (tc != kFP16 && tc != kTF32))
         return SHGEMM_STATUS_INVALID_VALUE;
@@ -1011,13 +1060,13 @@ int shgemm_b200_shgemm(shgemm_b200_handle_t h, int op_a, int op_b, size_t m, siz
     if (k > 0 && (!a || !b || lda < std::max<size_t>(1, a_rows) || ldb < std::max<size_t>(1, b_rows)))
         return SHGEMM_STATUS_INVALID_VALUE;
     if (m >= (1u << 31) || n >= (1u << 31) || k >= (1u << 31)) return SHGEMM_STATUS_NOT_SUPPORTED;
-    const float alpha = *alpha_ptr, beta = *beta_ptr;
     DeviceGuard g(h->device);
 
     if (k == 0) {  // empty product: C = beta * C
         const size_t rows = c_rows, cols = (op_c == kOpN) ? n : m;
         const int blocks = static_cast<int>(std::min<size_t>((rows * cols + 255) / 256, 4096));
-        scale_c_kernel<<<blocks, 256, 0, h->stream>>>(c, ldc, static_cast<int>(rows), static_cast<int>(cols), beta);
+        scale_c_kernel<<<blocks, 256, 0, h->stream>>>(c, ldc, static_cast<int>(rows), static_cast<int>(cols), beta,
+                                                      dev.beta);
         h->launches++;
         if (level_out) *level_out = SHGEMM_LEVEL_P0;
         return launch_status();
@@ -1027,13 +1076,14 @@ int shgemm_b200_shgemm(shgemm_b200_handle_t h, int op_a, int op_b, size_t m, siz
     const bool pack_b = (reinterpret_cast<uintptr_t>(b) & 15) || (ldb * 2) % 16;
     if (!pack_a && !pack_b) {
         if (tc == kTF32) {
-            const int st = tf32_widened_b(h, op_a, op_b, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc, op_c, level_out);
+            const int st =
+                tf32_widened_b(h, op_a, op_b, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc, op_c, level_out, dev);
             if (st != SHGEMM_STATUS_NOT_SUPPORTED) return st;
         }
         // SHGEMM_CFG_AUTOTUNE = 2: an untuned bucket is tuned on this call's operands first
         // (C is overwritten by the candidates, harmless when beta == 0 and C is laid out op_n).
-        if (h->autotune_mode == 2 && beta == 0.0f && op_c == kOpN && h->fixed_level == SHGEMM_LEVEL_AUTO &&
-            h->split_k == 0) {
+        if (h->autotune_mode == 2 && beta == 0.0f && !dev.beta && op_c == kOpN &&
+            h->fixed_level == SHGEMM_LEVEL_AUTO && h->split_k == 0) {
             bool have;
             {
                 std::lock_guard<std::mutex> lk(h->tune_mu);
@@ -1047,7 +1097,7 @@ int shgemm_b200_shgemm(shgemm_b200_handle_t h, int op_a, int op_b, size_t m, siz
             cudaGetLastError();
         }
         return run_tiled(h, op_a, op_b, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc, tc, op_c, level_out,
-                         h->workspace, h->workspace_bytes);
+                         h->workspace, h->workspace_bytes, nullptr, dev);
     }
 
     // Staging path: copy the unaligned operand(s) slab by slab (k-slabs of a multiple
@@ -1097,12 +1147,51 @@ int shgemm_b200_shgemm(shgemm_b200_handle_t h, int op_a, int op_b, size_t m, siz
             ldb_s = ldb;
         }
         if (launch_status() != SHGEMM_STATUS_OK) return SHGEMM_STATUS_LAUNCH_FAILED;
+        DevScalars ds = dev;
+        if (k0 > 0) ds.beta = nullptr;  // later slabs accumulate: beta = 1
         const int st = run_tiled(h, op_a, op_b, m, n, kk, alpha, as, lda_s, bs, ldb_s, k0 == 0 ? beta : 1.0f, c,
-                                 ldc, tc, op_c, &level, nullptr, 0);
+                                 ldc, tc, op_c, &level, nullptr, 0, nullptr, ds);
         if (st != SHGEMM_STATUS_OK) return st;
     }
     if (level_out) *level_out = level;
     return SHGEMM_STATUS_OK;
+}
+
+extern "C" {
+
+int shgemm_b200_shgemm(shgemm_b200_handle_t h, int op_a, int op_b, size_t m, size_t n, size_t k,
+                       const float* alpha_ptr, const float* a, size_t lda, const void* b, size_t ldb,
+                       const float* beta_ptr, float* c, size_t ldc, int tc, int op_c, int* level_out) {
+    if (!h || !alpha_ptr || !beta_ptr) return SHGEMM_STATUS_INVALID_VALUE;
+    return shgemm_impl(h, op_a, op_b, m, n, k, *alpha_ptr, a, lda, b, ldb, *beta_ptr, c, ldc, tc, op_c, level_out,
+                       DevScalars{});
+}
+
+int shgemm_b200_shgemm_device_scalars(shgemm_b200_handle_t h, int op_a, int op_b, size_t m, size_t n, size_t k,
+                                      const float* alpha_dev, const float* a, size_t lda, const void* b, size_t ldb,
+                                      const float* beta_dev, float* c, size_t ldc, int tc, int op_c,
+                                      int* level_out) {
+    if (!h || !alpha_dev || !beta_dev) return SHGEMM_STATUS_INVALID_VALUE;
+    if ((reinterpret_cast<uintptr_t>(alpha_dev) & 3) || (reinterpret_cast<uintptr_t>(beta_dev) & 3))
+        return SHGEMM_STATUS_INVALID_VALUE;
+    DevScalars dev;
+    dev.alpha = alpha_dev;
+    dev.beta = beta_dev;
+    // alpha = 1, beta = 1 stand in on the host: the kernels read the device values, and with
+    // beta != 0 on the host side nothing assumes that C may be left unread
+    return shgemm_impl(h, op_a, op_b, m, n, k, 1.0f, a, lda, b, ldb, 1.0f, c, ldc, tc, op_c, level_out, dev);
+}
+
+int shgemm_b200_hsgemm_device_scalars(shgemm_b200_handle_t h, int op_a, int op_b, size_t m, size_t n, size_t k,
+                                      const float* alpha_dev, const void* a, size_t lda, const float* b, size_t ldb,
+                                      const float* beta_dev, float* c, size_t ldc, int tc, int op_c,
+                                      int* level_out) {
+    // the transposition identity of shgemm_b200_hsgemm (include/shgemm/shgemm.hpp:142-156)
+    auto inv = [](int op) { return op == kOpN ? kOpT : kOpN; };
+    if ((op_a != kOpN && op_a != kOpT) || (op_b != kOpN && op_b != kOpT) || (op_c != kOpN && op_c != kOpT))
+        return SHGEMM_STATUS_INVALID_VALUE;
+    return shgemm_b200_shgemm_device_scalars(h, inv(op_b), inv(op_a), n, m, k, alpha_dev, b, ldb, a, lda, beta_dev,
+                                             c, ldc, tc, inv(op_c), level_out);
 }
 
 // ---------------------------------------------------------------- autotuner
@@ -1524,28 +1613,28 @@ int grouped_tile_n(int tc, bool b_wide, size_t n) {
     return bn;
 }
 
-// Writes the problem table and the unit list of a batch into the pinned host staging.
-int grouped_stage(shgemm_b200_handle_t h, int op_a, int op_b, int tc, int op_c, const shgemm_b200_problem* probs,
-                  int count) {
+// Writes the problem table and the unit list of a batch into table t's pinned host staging.
+int grouped_stage(shgemm_b200_handle_t h, GroupedTable& t, bool b_wide, int op_a, int op_b, int tc, int op_c,
+                  const shgemm_b200_problem* probs, int count) {
     if (!h || count < 0 || (count > 0 && !probs)) return SHGEMM_STATUS_INVALID_VALUE;
     if ((op_a != kOpN && op_a != kOpT) || op_b != kOpN || (op_c != kOpN && op_c != kOpT) ||
         (tc != kFP16 && tc != kTF32))
         return op_b == kOpT ? SHGEMM_STATUS_NOT_SUPPORTED : SHGEMM_STATUS_INVALID_VALUE;
-    if (count > kGroupedMaxProblems) return SHGEMM_STATUS_NOT_SUPPORTED;
+    if (count > t.max_problems) return SHGEMM_STATUS_NOT_SUPPORTED;
     // The staging buffer may still be the source of a pending eager copy: wait for it
     // (not while capturing, where host waits are illegal; copies replayed from a
     // captured graph are the caller's to wait for).
     cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
     if (cudaStreamIsCapturing(h->stream, &cap) != cudaSuccess) cap = cudaStreamCaptureStatusNone;
-    if (cap == cudaStreamCaptureStatusNone && cudaEventSynchronize(h->grouped_copied) != cudaSuccess) {
+    if (cap == cudaStreamCaptureStatusNone && cudaEventSynchronize(t.copied) != cudaSuccess) {
         cudaGetLastError();
         return SHGEMM_STATUS_CUDA_ERROR;
     }
-    auto* host = static_cast<uint8_t*>(h->grouped_host);
+    auto* host = static_cast<uint8_t*>(t.host);
     auto* gp = reinterpret_cast<GroupedProblem*>(host);
-    auto* units = reinterpret_cast<int2*>(host + kGroupedUnitsOff);
+    auto* units = reinterpret_cast<int2*>(host + t.units_off);
     const int bk = tc == kFP16 ? 64 : 32;
-    const bool b_wide = tc == kTF32 && h->grouped_b_fp32 != 0;  // B given as FP32 (exact binary16 values)
+    b_wide = b_wide && tc == kTF32;  // B given as FP32 (exact binary16 values)
     const size_t b_elem = b_wide ? 4 : 2;
     struct Cost {
         long long cost;
@@ -1605,63 +1694,44 @@ int grouped_stage(shgemm_b200_handle_t h, int op_a, int op_b, int tc, int op_c, 
     // uneven k (greedy longest-processing-time order).
     std::stable_sort(list.begin(), list.end(), [](const Cost& x, const Cost& y) { return x.cost > y.cost; });
     for (size_t u = 0; u < list.size(); ++u) units[u] = list[u].unit;
-    *reinterpret_cast<int*>(host + kGroupedCountOff) = static_cast<int>(list.size());
-    h->grouped_tc = tc;
-    h->grouped_b32 = b_wide ? 1 : 0;
-    h->grouped_op_a = op_a;
-    h->grouped_op_b = op_b;
-    h->grouped_op_c = op_c;
-    h->grouped_units = static_cast<int>(list.size());
+    *reinterpret_cast<int*>(host + t.count_off) = static_cast<int>(list.size());
+    t.tc = tc;
+    t.b32 = b_wide ? 1 : 0;
+    t.op_a = op_a;
+    t.op_b = op_b;
+    t.op_c = op_c;
+    t.units = static_cast<int>(list.size());
     return SHGEMM_STATUS_OK;
 }
 
 }  // namespace
 
-extern "C" {
-
-int shgemm_b200_grouped_update(shgemm_b200_handle_t h, int op_a, int op_b, int compute_type, int op_c,
-                               const shgemm_b200_problem* problems, int count) {
-    if (!h) return SHGEMM_STATUS_INVALID_VALUE;
-    DeviceGuard g(h->device);
-    const int prev_tc = h->grouped_tc, prev_a = h->grouped_op_a, prev_c = h->grouped_op_c, prev_b = h->grouped_b32;
-    const int st = grouped_stage(h, op_a, op_b, compute_type, op_c, problems, count);
-    if (st != SHGEMM_STATUS_OK) return st;
-    // A captured launch was built for one kernel variant and copies a fixed number of
-    // problem slots: the batch must keep the variant and fit those slots.
-    if (prev_tc >= 0 && (prev_tc != compute_type || prev_a != op_a || prev_c != op_c || prev_b != h->grouped_b32))
-        return SHGEMM_STATUS_INVALID_VALUE;
-    if (count > h->grouped_copied_count) return SHGEMM_STATUS_INVALID_VALUE;
-    return SHGEMM_STATUS_OK;
-}
-
-int shgemm_b200_shgemm_grouped(shgemm_b200_handle_t h, int op_a, int op_b, int compute_type, int op_c,
-                               const shgemm_b200_problem* problems, int count) {
-    if (!h) return SHGEMM_STATUS_INVALID_VALUE;
-    DeviceGuard g(h->device);
-    const int st = grouped_stage(h, op_a, op_b, compute_type, op_c, problems, count);
+static int grouped_run(shgemm_b200_handle_t h, GroupedTable& t, bool b_wide, int op_a, int op_b, int tc, int op_c,
+                       const shgemm_b200_problem* probs, int count, DevScalars dev) {
+    const int st = grouped_stage(h, t, b_wide, op_a, op_b, tc, op_c, probs, count);
     if (st != SHGEMM_STATUS_OK) return st;
     // problems, units and count in two copies from the pinned staging (the tables are
     // fixed-offset so a captured graph replays with whatever the staging holds)
-    if (cudaMemcpyAsync(h->grouped_dev, h->grouped_host, sizeof(GroupedProblem) * static_cast<size_t>(count),
-                        cudaMemcpyHostToDevice, h->stream) != cudaSuccess ||
-        cudaMemcpyAsync(static_cast<uint8_t*>(h->grouped_dev) + kGroupedUnitsOff,
-                        static_cast<uint8_t*>(h->grouped_host) + kGroupedUnitsOff,
-                        kGroupedCountOff + sizeof(int) - kGroupedUnitsOff, cudaMemcpyHostToDevice, h->stream) !=
-            cudaSuccess)
+    if (cudaMemcpyAsync(t.dev, t.host, sizeof(GroupedProblem) * static_cast<size_t>(count), cudaMemcpyHostToDevice,
+                        h->stream) != cudaSuccess ||
+        cudaMemcpyAsync(static_cast<uint8_t*>(t.dev) + t.units_off, static_cast<uint8_t*>(t.host) + t.units_off,
+                        t.count_off + sizeof(int) - t.units_off, cudaMemcpyHostToDevice, h->stream) != cudaSuccess)
         return SHGEMM_STATUS_CUDA_ERROR;
-    h->grouped_copied_count = count;
+    t.copied_count = count;
     cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
     cudaStreamIsCapturing(h->stream, &cap);
-    if (cap == cudaStreamCaptureStatusNone) cudaEventRecord(h->grouped_copied, h->stream);
+    if (cap == cudaStreamCaptureStatusNone) cudaEventRecord(t.copied, h->stream);
     GroupedParams P;
     std::memset(&P, 0, sizeof(P));
-    P.problems = static_cast<const GroupedProblem*>(h->grouped_dev);
-    P.units = reinterpret_cast<const int2*>(static_cast<uint8_t*>(h->grouped_dev) + kGroupedUnitsOff);
-    P.num_units = reinterpret_cast<const int*>(static_cast<uint8_t*>(h->grouped_dev) + kGroupedCountOff);
+    P.problems = static_cast<const GroupedProblem*>(t.dev);
+    P.units = reinterpret_cast<const int2*>(static_cast<uint8_t*>(t.dev) + t.units_off);
+    P.num_units = reinterpret_cast<const int*>(static_cast<uint8_t*>(t.dev) + t.count_off);
     P.error_flag = h->error_word;
     P.wait_limit_ns = static_cast<uint64_t>(h->wait_limit_ms) * 1000000ull;
     P.op_c = op_c;
-    const KernelEntry e = grouped_table(compute_type, op_a == kOpT, h->grouped_b32 == 1);
+    P.alpha_dev = dev.alpha;
+    P.beta_dev = dev.beta;
+    const KernelEntry e = grouped_table(tc, op_a == kOpT, t.b32 == 1);
     void* args[] = {&P};
     // One CTA per SM whatever the batch: a captured launch stays valid for other batches.
     const cudaError_t err = cudaLaunchKernel(e.fn, dim3(h->num_sms), dim3(512), args, e.smem, h->stream);
@@ -1671,9 +1741,34 @@ int shgemm_b200_shgemm_grouped(shgemm_b200_handle_t h, int op_a, int op_b, int c
         return SHGEMM_STATUS_LAUNCH_FAILED;
     }
     if (h->debug_mode)
-        std::printf("[grouped] problems = %d, units = %d, compute_type = %s\n", count, h->grouped_units,
-                    compute_type == kTF32 ? "TF32" : "FP16");
+        std::printf("[grouped] problems = %d, units = %d, compute_type = %s\n", count, t.units,
+                    tc == kTF32 ? "TF32" : "FP16");
     return SHGEMM_STATUS_OK;
+}
+
+extern "C" {
+
+int shgemm_b200_grouped_update(shgemm_b200_handle_t h, int op_a, int op_b, int compute_type, int op_c,
+                               const shgemm_b200_problem* problems, int count) {
+    if (!h) return SHGEMM_STATUS_INVALID_VALUE;
+    DeviceGuard g(h->device);
+    GroupedTable& t = h->grouped;
+    const int prev_tc = t.tc, prev_a = t.op_a, prev_c = t.op_c, prev_b = t.b32;
+    const int st = grouped_stage(h, t, h->grouped_b_fp32 != 0, op_a, op_b, compute_type, op_c, problems, count);
+    if (st != SHGEMM_STATUS_OK) return st;
+    // A captured launch was built for one kernel variant and copies a fixed number of
+    // problem slots: the batch must keep the variant and fit those slots.
+    if (prev_tc >= 0 && (prev_tc != compute_type || prev_a != op_a || prev_c != op_c || prev_b != t.b32))
+        return SHGEMM_STATUS_INVALID_VALUE;
+    if (count > t.copied_count) return SHGEMM_STATUS_INVALID_VALUE;
+    return SHGEMM_STATUS_OK;
+}
+
+int shgemm_b200_shgemm_grouped(shgemm_b200_handle_t h, int op_a, int op_b, int compute_type, int op_c,
+                               const shgemm_b200_problem* problems, int count) {
+    if (!h) return SHGEMM_STATUS_INVALID_VALUE;
+    DeviceGuard g(h->device);
+    return grouped_run(h, h->grouped, h->grouped_b_fp32 != 0, op_a, op_b, compute_type, op_c, problems, count);
 }
 
 }  // extern "C"
@@ -1698,6 +1793,8 @@ static __device__ __align__(256) int g_noalloc_error;
 struct NoAllocDevice {
     bool ready = false;
     int num_sms = 0;
+    int fixed_level = SHGEMM_LEVEL_AUTO;  // MTK_SHGEMM_KERNEL_LEVEL, as shgemm_b200_create reads it
+    unsigned debug_mode = 0;              // MTK_SHGEMM_DEBUG
     float* scratch = nullptr;  // device address of g_noalloc_scratch on this device
     int* error_word = nullptr; // device address of g_noalloc_error on this device
 };
@@ -1747,6 +1844,10 @@ int noalloc_setup(int dev, NoAllocDevice*& out) {
             }
         }
         d.num_sms = sms;
+        const char* dbg = std::getenv("MTK_SHGEMM_DEBUG");
+        d.debug_mode = (dbg && dbg[0] == '1') ? 1u : 0u;
+        const char* lvl = std::getenv("MTK_SHGEMM_KERNEL_LEVEL");
+        if (lvl && (lvl[0] == '0' || lvl[0] == '1') && lvl[1] == '\0') d.fixed_level = lvl[0] - '0';
         d.scratch = static_cast<float*>(sp);
         d.error_word = static_cast<int*>(ep);
         d.ready = true;
@@ -1782,8 +1883,10 @@ int shgemm_b200_shgemm_noalloc(void* cuda_stream, int op_a, int op_b, size_t m, 
     h.workspace = d->scratch;
     h.workspace_bytes = kNoAllocScratchBytes;
     h.error_word = d->error_word;
-    // The error word keeps the previous call's value: clear it first.
-    if (cudaMemsetAsync(d->error_word, 0, sizeof(int), h.stream) != cudaSuccess) return SHGEMM_STATUS_CUDA_ERROR;
+    h.fixed_level = d->fixed_level;
+    h.debug_mode = d->debug_mode;
+    // The error word is sticky: a timeout stays recorded until shgemm_b200_noalloc_check_error
+    // reads and clears it, so a later call cannot hide an earlier one's failure.
     return shgemm_b200_shgemm(&h, op_a, op_b, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc, compute_type, op_c,
                               level_out);
 }
@@ -1798,6 +1901,7 @@ int shgemm_b200_noalloc_check_error(void* cuda_stream, int* device_code) {
     int code = 0;
     if (cudaMemcpy(&code, d->error_word, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess)
         return SHGEMM_STATUS_CUDA_ERROR;
+    if (code && cudaMemset(d->error_word, 0, sizeof(int)) != cudaSuccess) return SHGEMM_STATUS_CUDA_ERROR;
     if (device_code) *device_code = code;
     return code ? SHGEMM_STATUS_TIMEOUT : SHGEMM_STATUS_OK;
 }

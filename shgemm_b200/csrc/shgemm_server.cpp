@@ -106,7 +106,8 @@ struct Request {
 struct Slot {
     shgemm_b200_handle_t h = nullptr;
     cudaStream_t stream = nullptr;
-    cudaEvent_t done = nullptr;
+    // batch start, Omega generated (grouped launch starts), batch done: timing events
+    cudaEvent_t start = nullptr, mid = nullptr, done = nullptr;
     bool busy = false;
     std::vector<std::shared_ptr<Request>> reqs;
 };
@@ -131,6 +132,12 @@ struct shgemm_b200_server {
     unsigned long long n_submitted = 0, n_completed = 0, n_failed = 0, n_batches = 0, n_unfinished = 0;
     std::vector<double> latencies_ms;
     double flops_done = 0;
+    // device timing of completed batches, in ms after `ref` (recorded on an idle stream)
+    cudaStream_t ref_stream = nullptr;
+    cudaEvent_t ref = nullptr;
+    std::vector<std::pair<float, float>> kernel_iv;  // grouped launch intervals
+    double omega_ms = 0;
+    unsigned long long n_launches = 0;
     bool have_first = false;
     Clock::time_point first_submit, last_done;
 
@@ -211,7 +218,7 @@ bool shgemm_b200_server::launch_locked(Slot& s) {
         ready.pop_front();
     }
     if (s.reqs.empty()) return false;
-    bool ok = true;
+    bool ok = cudaEventRecord(s.start, s.stream) == cudaSuccess;
     for (auto& qp : s.reqs) {
         Request& q = *qp;
         q.state = SHGEMM_REQ_RUNNING;
@@ -222,6 +229,7 @@ bool shgemm_b200_server::launch_locked(Slot& s) {
             ok = shgemm_b200_generate_omega(s.stream, dst, q.ldb, q.r.k, q.r.n, q.r.omega_dist,
                                             q.r.omega_seed * 0x100000001B3ull + static_cast<unsigned long long>(j),
                                             q.r.omega_scale, fp32) == SHGEMM_STATUS_OK;
+            ++n_launches;
         }
         shgemm_b200_problem p{};
         p.m = q.r.m;
@@ -237,8 +245,10 @@ bool shgemm_b200_server::launch_locked(Slot& s) {
         p.beta = 0.0f;
         probs.push_back(p);
     }
+    ok = ok && cudaEventRecord(s.mid, s.stream) == cudaSuccess;
     ok = ok && shgemm_b200_shgemm_grouped(s.h, SHGEMM_OP_N, SHGEMM_OP_N, tc, SHGEMM_OP_N, probs.data(),
                                           static_cast<int>(probs.size())) == SHGEMM_STATUS_OK;
+    if (ok) ++n_launches;
     ok = ok && cudaEventRecord(s.done, s.stream) == cudaSuccess;
     if (!ok) {
         cudaGetLastError();
@@ -252,6 +262,16 @@ bool shgemm_b200_server::launch_locked(Slot& s) {
 
 bool shgemm_b200_server::complete_locked(Slot& s, bool ok) {
     const auto now = Clock::now();
+    if (ok && s.busy) {
+        float t0 = 0, t1 = 0, t2 = 0;
+        if (cudaEventElapsedTime(&t0, ref, s.start) == cudaSuccess &&
+            cudaEventElapsedTime(&t1, ref, s.mid) == cudaSuccess && cudaEventElapsedTime(&t2, ref, s.done) == cudaSuccess) {
+            omega_ms += t1 - t0;
+            kernel_iv.emplace_back(t1, t2);
+        } else {
+            cudaGetLastError();
+        }
+    }
     for (auto& qp : s.reqs) {
         Request& q = *qp;
         arena.release(q.om_off, q.om_bytes);
@@ -337,7 +357,9 @@ int shgemm_b200_server_create(shgemm_b200_server_t* out, int device, const shgem
     for (auto& sl : s->slots) {
         int st = shgemm_b200_create(&sl.h, device);
         if (st == SHGEMM_STATUS_OK && (cudaStreamCreateWithFlags(&sl.stream, cudaStreamNonBlocking) != cudaSuccess ||
-                                       cudaEventCreateWithFlags(&sl.done, cudaEventDisableTiming) != cudaSuccess))
+                                       cudaEventCreate(&sl.start) != cudaSuccess ||
+                                       cudaEventCreate(&sl.mid) != cudaSuccess ||
+                                       cudaEventCreate(&sl.done) != cudaSuccess))
             st = SHGEMM_STATUS_CUDA_ERROR;
         if (st == SHGEMM_STATUS_OK) st = shgemm_b200_set_stream(sl.h, sl.stream);
         if (st == SHGEMM_STATUS_OK && c.compute_type == SHGEMM_TC_TF32)
@@ -346,6 +368,8 @@ int shgemm_b200_server_create(shgemm_b200_server_t* out, int device, const shgem
             cudaGetLastError();
             for (auto& t : s->slots) {
                 if (t.h) shgemm_b200_destroy(t.h);
+                if (t.start) cudaEventDestroy(t.start);
+                if (t.mid) cudaEventDestroy(t.mid);
                 if (t.done) cudaEventDestroy(t.done);
                 if (t.stream) cudaStreamDestroy(t.stream);
             }
@@ -353,6 +377,23 @@ int shgemm_b200_server_create(shgemm_b200_server_t* out, int device, const shgem
             delete s;
             return st;
         }
+    }
+    if (cudaStreamCreateWithFlags(&s->ref_stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreate(&s->ref) != cudaSuccess || cudaEventRecord(s->ref, s->ref_stream) != cudaSuccess ||
+        cudaEventSynchronize(s->ref) != cudaSuccess) {
+        cudaGetLastError();
+        for (auto& t : s->slots) {
+            shgemm_b200_destroy(t.h);
+            cudaEventDestroy(t.start);
+            cudaEventDestroy(t.mid);
+            cudaEventDestroy(t.done);
+            cudaStreamDestroy(t.stream);
+        }
+        if (s->ref) cudaEventDestroy(s->ref);
+        if (s->ref_stream) cudaStreamDestroy(s->ref_stream);
+        s->arena.destroy();
+        delete s;
+        return SHGEMM_STATUS_CUDA_ERROR;
     }
     s->worker = std::thread([s] { s->run(); });
     *out = s;
@@ -368,9 +409,13 @@ int shgemm_b200_server_destroy(shgemm_b200_server_t s) {
     for (auto& t : s->slots) {
         if (t.stream) cudaStreamSynchronize(t.stream);
         if (t.h) shgemm_b200_destroy(t.h);
+        if (t.start) cudaEventDestroy(t.start);
+        if (t.mid) cudaEventDestroy(t.mid);
         if (t.done) cudaEventDestroy(t.done);
         if (t.stream) cudaStreamDestroy(t.stream);
     }
+    if (s->ref) cudaEventDestroy(s->ref);
+    if (s->ref_stream) cudaStreamDestroy(s->ref_stream);
     s->arena.destroy();
     delete s;
     return SHGEMM_STATUS_OK;
@@ -492,6 +537,26 @@ int shgemm_b200_server_get_stats(shgemm_b200_server_t s, shgemm_b200_server_stat
         out->max_ms = v.back();
         out->span_s = std::chrono::duration<double>(s->last_done - s->first_submit).count();
     }
+    // union of the grouped launches' intervals
+    std::vector<std::pair<float, float>> iv = s->kernel_iv;
+    std::sort(iv.begin(), iv.end());
+    double busy_ms = 0;
+    float cur0 = 0, cur1 = 0;
+    bool open = false;
+    for (const auto& x : iv) {
+        if (open && x.first <= cur1) {
+            cur1 = std::max(cur1, x.second);
+            continue;
+        }
+        if (open) busy_ms += cur1 - cur0;
+        cur0 = x.first;
+        cur1 = x.second;
+        open = true;
+    }
+    if (open) busy_ms += cur1 - cur0;
+    out->kernel_busy_s = busy_ms * 1e-3;
+    out->omega_s = s->omega_ms * 1e-3;
+    out->launches = s->n_launches;
     return SHGEMM_STATUS_OK;
 }
 
@@ -502,6 +567,9 @@ int shgemm_b200_server_reset_stats(shgemm_b200_server_t s) {
     s->n_submitted = 0;
     s->n_completed = s->n_failed = s->n_batches = 0;
     s->flops_done = 0;
+    s->kernel_iv.clear();
+    s->omega_ms = 0;
+    s->n_launches = 0;
     s->have_first = false;
     s->peak_resident = s->resident;
     return SHGEMM_STATUS_OK;

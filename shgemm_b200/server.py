@@ -33,7 +33,8 @@ class ServerStats(ctypes.Structure):
                 ("batches", ctypes.c_ulonglong), ("p50_ms", ctypes.c_double), ("p99_ms", ctypes.c_double),
                 ("mean_ms", ctypes.c_double), ("max_ms", ctypes.c_double), ("flops_completed", ctypes.c_double),
                 ("span_s", ctypes.c_double), ("peak_resident_bytes", ctypes.c_size_t),
-                ("resident_bytes", ctypes.c_size_t), ("queued", ctypes.c_ulonglong), ("in_flight", ctypes.c_ulonglong)]
+                ("resident_bytes", ctypes.c_size_t), ("queued", ctypes.c_ulonglong), ("in_flight", ctypes.c_ulonglong),
+                ("kernel_busy_s", ctypes.c_double), ("omega_s", ctypes.c_double), ("launches", ctypes.c_ulonglong)]
 
     def as_dict(self) -> dict:
         return {name: getattr(self, name) for name, _ in self._fields_}

@@ -51,6 +51,16 @@ int main() {
 
 	const float alpha = 1.0f, beta = 0.0f;
 	int failures = 0;
+	// The handle exposes its live workspace, as the reference's w_ptr does (src/shgemm.cu:417).
+	{
+		cudaPointerAttributes attr{};
+		const bool dev_mem = shgemm_handle.w_ptr != nullptr &&
+		                     cudaPointerGetAttributes(&attr, shgemm_handle.w_ptr) == cudaSuccess &&
+		                     attr.type == cudaMemoryTypeDevice;
+		std::printf("workspace w_ptr=%p elements=%zu device=%d\n", static_cast<void*>(shgemm_handle.w_ptr),
+				shgemm_handle.max_working_memory_num_elements, dev_mem ? 1 : 0);
+		failures += (!dev_mem || shgemm_handle.max_working_memory_num_elements == 0);
+	}
 	for (const auto compute_type : {mtk::shgemm::fp16, mtk::shgemm::tf32}) {
 		// SHGEMM (A = float, B = half)
 		const auto level = mtk::shgemm::shgemm(shgemm_handle, mtk::shgemm::op_n, mtk::shgemm::op_n, m, n, k, &alpha,

@@ -172,6 +172,60 @@ def test_grouped_graph_replay_with_new_tables(h):
         h.set_stream(torch.cuda.current_stream())
 
 
+def test_eager_tf32_call_between_replays_leaves_captured_batch_intact(cuda_device):
+    """An eager TF32 shgemm that takes the widened-B route (its own one-problem grouped
+    table) between two replays of a captured grouped launch on the same handle: the second
+    replay still computes the captured batch, and the eager call its own product."""
+    import torch
+
+    import shgemm_b200 as sg
+
+    hd = sg.Handle(0)
+    s = torch.cuda.Stream()
+    hd.set_stream(s)
+    try:
+        rng = np.random.default_rng(77)
+        shapes = [(300, 64, 512), (129, 256, 1000), (640, 32, 320)]
+        ins, dev, probs = _run_batch(hd, shapes, oracle.FP16, 0, rng)
+        with torch.cuda.stream(s):
+            sg.shgemm_grouped(hd, probs, sg.fp16)
+        s.synchronize()
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g, stream=s):
+            sg.shgemm_grouped(hd, probs, sg.fp16)
+        # eager TF32 call whose 128 x 256 tiles fill the GPU: widened B, one-problem table
+        m, n, k = 2048, 2560, 700
+        hd.set_workspace_size(max(64 << 20, n * (k + 3) // 4 * 4 * 4 + (1 << 20)))
+        inp = K.make_inputs(rng, m, n, k, 0, 0, 0, dist="uniform")
+        A = torch.from_numpy(inp["A"]).cuda()
+        B = torch.from_numpy(inp["B"].view(np.int16)).cuda().view(torch.float16)
+        Ce = torch.from_numpy(inp["C"].copy()).cuda()
+        before = hd.launch_count()
+        with torch.cuda.stream(s):
+            sg.shgemm(hd, 0, 0, m, n, k, 1.0, A, inp["lda"], B, inp["ldb"], 0.0, Ce, inp["ldc"], sg.tf32)
+        s.synchronize()
+        assert hd.launch_count() - before == 2  # widen + the TF32 grouped kernel: the route was taken
+        for (_, _, C) in dev:
+            C.zero_()
+        torch.cuda.synchronize()
+        with torch.cuda.stream(s):
+            g.replay()
+        torch.cuda.synchronize()
+        assert hd.check_error() == 0
+        for (mm, nn, kk), ip, (_, _, C) in zip(shapes, ins, dev):
+            orc = K.run_oracle(oracle.FP16, 0, 0, mm, nn, kk, 1.0, ip, 0.0, 0, chunk=0)
+            ref = K.fp64(0, 0, mm, nn, kk, 1.0, ip, 0.0, 0)
+            sgc = K.sgemm(0, 0, mm, nn, kk, 1.0, ip, 0.0, 0)
+            K.assert_parity(K.parity_report(C.cpu().numpy(), orc, ref, sgc, mm, nn, ip["ldc"], 0))
+        orc = K.run_oracle(oracle.TF32, 0, 0, m, n, k, 1.0, inp, 0.0, 0, chunk=0)
+        ref = K.fp64(0, 0, m, n, k, 1.0, inp, 0.0, 0)
+        sgc = K.sgemm(0, 0, m, n, k, 1.0, inp, 0.0, 0)
+        K.assert_parity(K.parity_report(Ce.cpu().numpy(), orc, ref, sgc, m, n, inp["ldc"], 0))
+        del g
+    finally:
+        hd.close()
+
+
 def test_grouped_rejects_unsupported(h):
     import torch
 

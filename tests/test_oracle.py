@@ -139,3 +139,64 @@ def test_wide_exponent_lo_term_underflow():
     # the value, with ever fewer bits: the error grows, as in the reference
     assert res[(-36, -15)] > res[(-15, 14)]
     assert res[(-100, -36)] > 0.5
+
+
+def test_tcmodel_truncates_each_hi_fragment():
+    """Known answer of the tensor-core model: one 16-k fragment whose exact sum is
+    1 + 3 * 2^-25 (three quarters of an FP32 ulp above 1). The idealised oracle rounds it
+    to nearest (1 + 2^-23); the model truncates it before the round-to-nearest add (1)."""
+    k = 16
+    A = np.zeros(k, np.float32)
+    B = np.zeros(k, np.float16)
+    A[0], B[0] = 1.0, 1.0
+    for j in (1, 2, 3):  # 2^-13 * 2^-12 = 2^-25, each exact in binary16 and in the product
+        A[j], B[j] = 2.0 ** -13, 2.0 ** -12
+    out = {}
+    for model in (oracle.IDEAL, oracle.TCMODEL):
+        C = np.zeros(1, np.float32)
+        oracle.shgemm(oracle.FP16, 0, 0, 1, 1, k, 1.0, A, 1, B, k, 0.0, C, 1, 0, 0, model)
+        out[model] = float(C[0])
+    assert out[oracle.IDEAL] == 1.0 + 2.0 ** -23
+    assert out[oracle.TCMODEL] == 1.0
+
+
+def test_tcmodel_lo_accumulator_truncates_across_k():
+    """Known answer for the lo term, carried across two 16-k fragments. a1 = 2^-25 splits
+    into hi = 0 (a binary16 tie, rounded to even) and lo = 2^-14; a2 = 3 * 2^-35 into hi = 0
+    and lo = 3 * 2^-24 (subnormal). With b = (1, 2^-14) the lo sum is 2^-14 + 1.5 ulp: the
+    idealised oracle rounds it to nearest (even: + 2 ulp), the truncating FP32 accumulator
+    of the model keeps + 1 ulp. The fold scales by 2^-11 exactly."""
+    k = 32
+    A = np.zeros(k, np.float32)
+    B = np.zeros(k, np.float16)
+    A[0], B[0] = 2.0 ** -25, 1.0
+    A[16], B[16] = 3 * 2.0 ** -35, 2.0 ** -14
+    hi, lo = oracle.split(oracle.FP16, A[[0, 16]])
+    assert hi[0] == 0.0 and hi[1] == 0.0 and lo[0] == 2.0 ** -14 and lo[1] == 3 * 2.0 ** -24
+    out = {}
+    for model in (oracle.IDEAL, oracle.TCMODEL):
+        C = np.zeros(1, np.float32)
+        oracle.shgemm(oracle.FP16, 0, 0, 1, 1, k, 1.0, A, 1, B, k, 0.0, C, 1, 0, 0, model)
+        out[model] = float(C[0])
+    assert out[oracle.IDEAL] == 2.0 ** -25 + 2.0 ** -47
+    assert out[oracle.TCMODEL] == 2.0 ** -25 + 2.0 ** -48
+
+
+@pytest.mark.parametrize("tc", [oracle.FP16, oracle.TF32])
+def test_tcmodel_error_close_to_idealised(tc):
+    """The modelled truncation costs little against the idealised sums, and both stay well
+    inside 2x FP32 SGEMM's error (the bar the CUDA path is held to)."""
+    rng = np.random.default_rng(12)
+    m, n, k = 48, 40, 2048
+    A, lda, B, ldb = _rand_case(rng, m, n, k, 0, 0)
+    ref = oracle.dgemm_ref(0, 0, m, n, k, 1.0, A, lda, B, ldb)
+    e = {}
+    for model in (oracle.IDEAL, oracle.TCMODEL):
+        C = np.zeros(m * n, np.float32)
+        oracle.shgemm(tc, 0, 0, m, n, k, 1.0, A, lda, B, ldb, 0.0, C, m, 0, 0, model)
+        e[model] = oracle.rel_fro(oracle.logical_c(C, m, n, m), ref)
+    S = np.zeros(m * n, np.float32)
+    oracle.sgemm(0, 0, m, n, k, 1.0, A, lda, B, ldb, 0.0, S, m, 0)
+    e_s = oracle.rel_fro(oracle.logical_c(S, m, n, m), ref)
+    assert 0.9 * e[oracle.IDEAL] <= e[oracle.TCMODEL] <= 1.5 * e[oracle.IDEAL]
+    assert e[oracle.TCMODEL] < 0.5 * e_s

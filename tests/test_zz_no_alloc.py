@@ -49,10 +49,18 @@ def test_noalloc_matches_handle_entry_on_two_calls(cuda_device, tc):
     orc = K.run_oracle(tc, 1, 0, m, n, k, 1.0, inp, 0.5, 0, chunk=0)
     ref64 = K.fp64(1, 0, m, n, k, 1.0, inp, 0.5, 0)
     sgc = K.sgemm(1, 0, m, n, k, 1.0, inp, 0.5, 0)
-    for _ in range(2):
-        C = torch.from_numpy(inp["C"].copy()).cuda()
+    C0 = torch.from_numpy(inp["C"].copy()).cuda()
+    Cs = [C0.clone(), C0.clone()]  # outputs made before any call, so the calls themselves allocate nothing
+    torch.cuda.synchronize()
+    for i in range(2):
+        C = Cs[i]
+        if i == 1:  # the first call did the one-time set-up; the second must not allocate at all
+            free0, torch0 = torch.cuda.mem_get_info()[0], torch.cuda.memory_allocated()
         sg.shgemm_noalloc(stream, 1, 0, m, n, k, 1.0, A, inp["lda"], B, inp["ldb"], 0.5, C, inp["ldc"], tc)
         assert sg.noalloc_check_error(stream) == 0
+        if i == 1:
+            assert torch.cuda.mem_get_info()[0] == free0
+            assert torch.cuda.memory_allocated() == torch0
         out = C.cpu().numpy()
         # the tolerance of the parity tests, against the oracle and the FP64 product ...
         K.assert_parity(K.parity_report(out, orc, ref64, sgc, m, n, inp["ldc"], 0))
