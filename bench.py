@@ -79,6 +79,10 @@ WORKLOADS = {
                     desc="grouped batch of 512 uneven right sketches Y_i = A_i Omega_i, m_i log-U[64,8192], "
                          "k_i log-U[256,16384], n_i in {32,64,128,256}, A_i rank n_i/2 (sigma_j = j^-1.5) + N(0,1e-4), "
                          "Omega_i Rademacher/sqrt(n_i), fp16 compute, one CUDA-graph-captured launch"),
+    # the reference's power test: square 2^10 .. 2^14 NN, TF32 and fp16, ~10 s loops under NVML
+    "energy": dict(m=0, n=0, k=0, op_a=0, op_b=0, tc=0, alpha=1.0, beta=0.0, dist="energy",
+                   desc="energy per call: square SHGEMM m = n = k = 2^10 .. 2^14 NN, inputs uniform (0, 1], "
+                        "tf32 and fp16 compute, a ~10 s loop per shape with NVML power sampled every 50 ms"),
     # the same batch in TF32 compute, Omega_i handed over widened to FP32 (as the sketch server keeps it)
     "grouped_tf32": dict(m=0, n=0, k=0, op_a=0, op_b=0, tc=1, alpha=1.0, beta=0.0, dist="grouped", count=512,
                          bound="hbm", b_fp32=True,
@@ -218,6 +222,38 @@ def energy(clk, ms_per_call, flops_per_call):
             "source": "nvidia-smi power.draw median over the timed region (whole board)"}
 
 
+class _Null:
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        return False
+
+
+def nvml_monitor(device_index):
+    """An NVML power monitor of the device (energy counter + 50 ms samples), or None."""
+    try:
+        from shgemm_b200 import energy as en
+
+        return en.PowerMonitor(device_index, 50.0)
+    except Exception:
+        return None
+
+
+def nvml_energy(mon, calls, flops_per_call):
+    """Energy per call of a timed region from the NVML monitor that ran over it (the
+    reference's J-per-GEMM figure, test/power_consumption_test.cu:94-123)."""
+    if mon is None:
+        return None
+    try:
+        r = mon.result()
+    except Exception:
+        return None
+    j = r["joules"] / calls
+    return {"avg_board_power_w": r["avg_w"], "joules_per_call": j, "effective_gflop_per_joule": flops_per_call / j / 1e9,
+            "source": r["source"] + " over the timed region (whole board)", "samples": r["samples"]}
+
+
 def traffic_for(key):
     """DRAM bytes per launch from a committed ncu summary (profiles/traffic.json), if captured."""
     f = os.path.join(ROOT, "profiles", "traffic.json")
@@ -349,7 +385,8 @@ def square_case(args, wl, ctx, traffic_key, tf32_error=False, e2e=True):
     launches0 = h.launch_count()
     ev0 = torch.cuda.Event(enable_timing=True)
     ev1 = torch.cuda.Event(enable_timing=True)
-    with ClockSampler(ctx.local) as clk:
+    mon = nvml_monitor(ctx.local)
+    with ClockSampler(ctx.local) as clk, (mon or _Null()):
         ev0.record(stream)
         for _ in range(args.steps):
             step()
@@ -455,7 +492,8 @@ def square_case(args, wl, ctx, traffic_key, tf32_error=False, e2e=True):
     return {"value": value, "ms_per_step": ms_step, "steps": args.steps, "level": level, "tuned": tuned,
             "issued_tflops": ctx.world * flops_issued * args.steps / (ms_total * 1e-3) / 1e12,
             "gpu_launches": launches, "roofline": roofline, "clocks": clocks,
-            "energy": energy(clocks, ms_step, flops_eff), "error": err, "tf32": tf32, "e2e": e2e_d}
+            "energy": nvml_energy(mon, args.steps, flops_eff) or energy(clocks, ms_step, flops_eff),
+            "error": err, "tf32": tf32, "e2e": e2e_d}
 
 
 # ---------------------------------------------------------------- grouped batch
@@ -1179,6 +1217,19 @@ def main():
         cpu = cpu_baseline(wl) if ctx.rank == 0 and ctx.world == 1 and not args.no_cpu else None
         line = served_line(args, wl, ctx, s, cpu)
         line.update(nested)
+    elif wl["dist"] == "energy":
+        import shgemm_b200 as sg
+        from shgemm_b200 import energy
+
+        h = sg.Handle(ctx.local)
+        rows = energy.power_sweep(h, seconds=args.duration or 10.0, device_index=ctx.local)
+        h.close()
+        top = [r for r in rows if r["m"] == 16384 and r["compute_type"] == "fp16"]
+        line = {"metric": METRIC, "value": top[0]["tflops"] if top else None, "unit": "TFLOP/s",
+                "n_gpus": ctx.world, "steps": sum(r["calls"] for r in rows), "warmup": 16, "ms_per_step": None,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": dtype_of(0),
+                "data": "synthetic (uniform (0, 1], seed 0)", "config": {"workload": wl["desc"]},
+                "energy_table": rows}
     elif wl["dist"] == "grouped":
         g = grouped_case(args, wl, ctx)
         cpu = None
