@@ -357,6 +357,9 @@ def square_case(args, wl, ctx, traffic_key, tf32_error=False, e2e=True):
     C0 = C.clone() if wl["beta"] != 0 else None
 
     h.set_config(sg.CFG_K_CHUNK, args.k_chunk)
+    if args.group_m:
+        h.set_config(sg.CFG_GROUP_M, args.group_m)
+    h.set_config(sg.CFG_TM_STAGES, args.stages)
     if (wl["tc"] == 1 or tf32_error) and wl["op_b"] == 0:
         # room for the widened FP32 copy of B (the TF32 route that loads B unconverted)
         h.set_workspace_size(max(64 << 20, n * ((k + 3) // 4 * 4) * 4 + (1 << 20)))
@@ -563,7 +566,13 @@ def grouped_case(args, wl, ctx, steps=None):
             gprobs.append((m, n, k, A, lda, Bw.reshape(-1), ldb4, C, ldc, al, be))
         h.set_config(sg.CFG_GROUPED_B_FP32, 1)
 
-    # capture the grouped launch once, replay it per step
+    # tile N per n bucket tuned on this batch (not timed), then the launch captured once and
+    # replayed per step
+    tiles = None
+    if not args.no_autotune:
+        h.autotune_grouped(gprobs, wl["tc"])
+        tiles = {f"n in [{1 << L}, {2 << L})": h.autotune_grouped_lookup(1 << L, wl["tc"], 0, bool(wl.get("b_fp32")))
+                 for L in sorted({int(n).bit_length() - 1 for (_, n, _) in shapes})}
     with torch.cuda.stream(stream):
         sg.shgemm_grouped(h, gprobs, wl["tc"])
     stream.synchronize()
@@ -636,6 +645,7 @@ def grouped_case(args, wl, ctx, steps=None):
     return {
         "value": value, "unit": "TFLOP/s", "ms_per_step": ms_step, "steps": steps, "workload": wl["desc"],
         "problems": len(shapes), "total_flops_2mnk": flops, "algorithmic_bytes": bytes_min,
+        "autotuned_tile_n": tiles,
         "per_call_baseline": {"value": per_call_tflops, "unit": "TFLOP/s", "ms_per_step": ms_pc,
                               "launches_per_step": len(shapes),
                               "what": "the same problems as one shgemm call (one launch) each, back to back"},
@@ -1191,6 +1201,10 @@ def main():
     ap.add_argument("--no-nested", action="store_true", help="headline: skip the grouped and square results")
     ap.add_argument("--k-chunk", type=int, default=64, choices=[64, 128],
                     help="k between FP32 drains in the tensor-memory kernel (SHGEMM_CFG_K_CHUNK)")
+    ap.add_argument("--group-m", type=int, default=0,
+                    help="plain workloads: tile rasterisation group along m (with --no-autotune)")
+    ap.add_argument("--stages", type=int, default=0, choices=[0, 1],
+                    help="tensor-memory kernel operand ring (SHGEMM_CFG_TM_STAGES, with --no-autotune)")
     ap.add_argument("--rate", type=float, default=None, help="served: arrivals per second")
     ap.add_argument("--duration", type=float, default=None, help="served: seconds of arrivals")
     args = ap.parse_args()

@@ -21,6 +21,7 @@ extern "C" {
 #endif
 
 typedef struct shgemm_b200_handle* shgemm_b200_handle_t;
+struct shgemm_b200_problem; /* one problem of a grouped launch (below) */
 
 /* operation_t (include/shgemm/shgemm.hpp:36-39) */
 enum { SHGEMM_OP_N = 0, SHGEMM_OP_T = 1 };
@@ -60,8 +61,10 @@ enum {
                                       128 (measured: ~1.2x the 64-k error on mixed-sign data,
                                       ~2.2x on all-positive data, within 2x FP32 SGEMM's error);
                                       the other kernels always drain every 64 */,
-    SHGEMM_CFG_HOST_BLOCK_COLS = 9 /* columns of C per block of shgemm_b200_shgemm_host:
+    SHGEMM_CFG_HOST_BLOCK_COLS = 9, /* columns of C per block of shgemm_b200_shgemm_host:
                                       0 (default) = a multiple of 256 giving about 16 blocks */
+    SHGEMM_CFG_TM_STAGES = 10      /* operand ring of the tensor-memory kernel when no tuned entry
+                                      applies: 0 (default) = 4 FP32 A + 3 binary16 B stages, 1 = 3 + 4 */
 };
 
 /* ------------------------------------------------------------------------
@@ -69,28 +72,47 @@ enum {
  * compile time, src/shgemm.cu:429-488, and picks one of two levels per call,
  * src/shgemm.cu:643-656). A shape bucket is (compute type, op_a, op_b,
  * floor(log2 m), floor(log2 n), floor(log2 k)); its entry names the tile N,
- * the split-K slice count and the tile rasterisation group. The k-chunk of the
- * FP32 drain is not tuned: it is one k-step (64 binary16 / 32 TF32 k), the
- * longest interval that keeps the tensor core's truncation within the error bar.
+ * the split-K slice count, the tile rasterisation group and, for the 128 x 256
+ * binary16 tiles of the tensor-memory kernel, the operand ring (stage counts) and
+ * the k-chunk of the FP32 drain. A 128-k chunk is only chosen when it is faster
+ * AND passes an accuracy gate: on sampled blocks of C its relative error against
+ * an FP64 product of the same operands is at most 1.25x that of the 64-k chunk.
  * ------------------------------------------------------------------------ */
 typedef struct {
     int tile_n;   /* 64, 128 or 256 (binary16); 64 or 128 (TF32) */
     int slices;   /* split-K slices, 1 = none */
     int group_m;  /* tiles along m per rasterisation group */
     float time_us;
+    int stages;   /* tensor-memory kernel ring: 0 = 4 FP32 A + 3 binary16 B stages, 1 = 3 + 4 */
+    int k_chunk;  /* tensor-memory kernel: k between FP32 drains, 64 or 128 */
 } shgemm_b200_tuned_config;
 
 /* Times every candidate configuration on the given operands (C is overwritten with
  * A B: the runs use alpha = 1, beta = 0), stores the fastest for the shape's bucket
  * and returns it in *best. Synchronises the handle's stream; not while capturing.
- * Operands must be TMA-addressable (16-byte aligned, 16-byte leading dimensions). */
+ * Operands must be TMA-addressable (16-byte aligned, 16-byte leading dimensions).
+ * The accuracy gate allocates and frees two small device buffers. */
 int shgemm_b200_autotune(shgemm_b200_handle_t handle, int op_a, int op_b, size_t m, size_t n, size_t k,
                          const float* a, size_t lda, const void* b, size_t ldb, float* c, size_t ldc,
                          int compute_type, shgemm_b200_tuned_config* best);
 /* The entry for a shape's bucket: SHGEMM_STATUS_OK and *cfg, or SHGEMM_STATUS_INVALID_VALUE if none. */
 int shgemm_b200_autotune_lookup(shgemm_b200_handle_t handle, int op_a, int op_b, size_t m, size_t n, size_t k,
                                 int compute_type, shgemm_b200_tuned_config* cfg);
-/* Writes / reads the table as text, one bucket per line. Loading adds to the table. */
+/* Tunes the tile N of grouped launches per n bucket, floor(log2 n), on a real batch
+ * (problems as for shgemm_b200_shgemm_grouped; their C is overwritten by the timing
+ * runs, which are eager grouped launches on the handle's stream): for every bucket the
+ * batch holds, every tile N the kernel allows is timed with the other buckets at their
+ * current choice, and the fastest is kept. Later grouped launches of the same compute
+ * type, op_a and B format use the entries; buckets without one keep the default rule
+ * (the smallest power of two >= n). *tuned (may be NULL) receives the number of
+ * buckets tuned. Not while capturing. */
+int shgemm_b200_autotune_grouped(shgemm_b200_handle_t handle, int op_a, int op_b, int compute_type, int op_c,
+                                 const struct shgemm_b200_problem* problems, int count, int* tuned);
+/* The grouped entry for one n bucket: SHGEMM_STATUS_OK and *tile_n, or SHGEMM_STATUS_INVALID_VALUE if none.
+ * b_fp32: the B format (SHGEMM_CFG_GROUPED_B_FP32). */
+int shgemm_b200_autotune_grouped_lookup(shgemm_b200_handle_t handle, int op_a, int compute_type, int b_fp32, size_t n,
+                                        int* tile_n);
+/* Writes / reads the table as text, one bucket per line (plain and grouped entries). Loading adds to the table. */
 int shgemm_b200_autotune_save(shgemm_b200_handle_t handle, const char* path);
 int shgemm_b200_autotune_load(shgemm_b200_handle_t handle, const char* path);
 int shgemm_b200_autotune_clear(shgemm_b200_handle_t handle);

@@ -27,7 +27,7 @@ P0, P1 = 0, 1              # detail::kernel_level (include/shgemm/shgemm.hpp:30-
 
 CFG_SPLIT_K, CFG_WAIT_LIMIT_MS, CFG_GROUP_M, CFG_GROUPED_B_FP32, CFG_AUTOTUNE, CFG_TILE_KERNEL, CFG_K_CHUNK = (
     2, 3, 4, 5, 6, 7, 8)
-CFG_HOST_BLOCK_COLS = 9
+CFG_HOST_BLOCK_COLS, CFG_TM_STAGES = 9, 10
 
 STATUS = {0: "OK", 1: "INVALID_VALUE", 2: "NOT_SUPPORTED", 3: "ALLOC_FAILED", 4: "LAUNCH_FAILED",
           5: "TIMEOUT", 6: "CUDA_ERROR", 7: "SCRATCH_TOO_SMALL"}
@@ -49,10 +49,11 @@ class TunedConfig(ctypes.Structure):
     """shgemm_b200_tuned_config: the autotuner's choice for a shape bucket (include/shgemm_b200.h)."""
 
     _fields_ = [("tile_n", ctypes.c_int), ("slices", ctypes.c_int), ("group_m", ctypes.c_int),
-                ("time_us", ctypes.c_float)]
+                ("time_us", ctypes.c_float), ("stages", ctypes.c_int), ("k_chunk", ctypes.c_int)]
 
     def as_dict(self) -> dict:
-        return {"tile_n": self.tile_n, "slices": self.slices, "group_m": self.group_m, "time_us": self.time_us}
+        return {"tile_n": self.tile_n, "slices": self.slices, "group_m": self.group_m, "time_us": self.time_us,
+                "stages": self.stages, "k_chunk": self.k_chunk}
 
 
 class ShgemmError(RuntimeError):
@@ -107,6 +108,8 @@ def lib() -> ctypes.CDLL:
         "shgemm_b200_autotune_save": [vp, ctypes.c_char_p],
         "shgemm_b200_autotune_load": [vp, ctypes.c_char_p],
         "shgemm_b200_autotune_clear": [vp],
+        "shgemm_b200_autotune_grouped": [vp, i, i, i, i, ctypes.POINTER(Problem), i, pi],
+        "shgemm_b200_autotune_grouped_lookup": [vp, i, i, i, sz, pi],
     }
     for name, args in sig.items():
         fn = getattr(L, name)
@@ -222,6 +225,21 @@ class Handle:
         cfg = TunedConfig()
         st = lib().shgemm_b200_autotune_lookup(self.ptr, op_a, op_b, m, n, k, compute_type, ctypes.byref(cfg))
         return cfg.as_dict() if st == 0 else None
+
+    def autotune_grouped(self, problems, compute_type: int, op_a: int = 0, op_b: int = 0, op_c: int = 0) -> int:
+        """Tunes the tile N of grouped launches per n bucket on this batch (its C is overwritten);
+        returns the number of buckets tuned."""
+        arr = _problem_array(problems)
+        n = ctypes.c_int()
+        _check(lib().shgemm_b200_autotune_grouped(self.ptr, op_a, op_b, compute_type, op_c, arr, len(problems),
+                                                  ctypes.byref(n)), "autotune_grouped")
+        return n.value
+
+    def autotune_grouped_lookup(self, n: int, compute_type: int, op_a: int = 0, b_fp32: bool = False):
+        """The tuned tile N of grouped problems with this n's bucket, or None."""
+        bn = ctypes.c_int()
+        st = lib().shgemm_b200_autotune_grouped_lookup(self.ptr, op_a, compute_type, int(b_fp32), n, ctypes.byref(bn))
+        return bn.value if st == 0 else None
 
     def autotune_save(self, path: str) -> None:
         _check(lib().shgemm_b200_autotune_save(self.ptr, os.fsencode(path)), "autotune_save")

@@ -27,7 +27,8 @@
 namespace shgemm_b200 {
 
 // KC: k-steps of 64 per FP32 drain (1: every 64 k; 2: every 128 k).
-template <bool A_KMAJOR, int KC = 1>
+// SV: operand ring variant (0: 4 raw FP32 A stages and 3 binary16 B stages; 1: 3 and 4).
+template <bool A_KMAJOR, int KC = 1, int SV = 0>
 struct TmCfg {
     static constexpr int BM = 128;
     static constexpr int BN = 256;
@@ -37,7 +38,8 @@ struct TmCfg {
     static constexpr int B_STAGE = BN * BK * 2;  // [256 n][64 k] binary16, 128-byte swizzle
     // raw A, B and tensor-memory operand stages; 128-column accumulator buffers: a chunk of
     // 2 k-steps holds 2 operand stages while its MMAs run, so it takes 4 stages and 2 buffers
-    static constexpr int SA = 4, SB = 3, ST = KC == 1 ? 2 : 4;
+    static constexpr int SA = SV == 0 ? 4 : 3, SB = SV == 0 ? 3 : 4, ST = KC == 1 ? 2 : 4;
+    static_assert(SV == 0 || SV == 1, "stage variant");
     static constexpr int ND = KC == 1 ? 3 : 2;
     static_assert(KC == 1 || KC == 2, "k-chunk");
     static constexpr int NUM_THREADS = 640;
@@ -76,9 +78,9 @@ __device__ __forceinline__ void split16_f16(const float (&v)[16], uint32_t (&hw)
     }
 }
 
-template <bool A_KMAJOR, int KC, class Params>
+template <bool A_KMAJOR, int KC, int SV, class Params>
 __device__ __forceinline__ void tm_kernel_body(const Params& p) {
-    using Cfg = TmCfg<A_KMAJOR, KC>;
+    using Cfg = TmCfg<A_KMAJOR, KC, SV>;
     constexpr int SA = Cfg::SA, SB = Cfg::SB, ST = Cfg::ST;
 
     extern __shared__ uint8_t smem_raw[];
@@ -509,9 +511,9 @@ __device__ __forceinline__ void tm_kernel_body(const Params& p) {
     if (warp == Cfg::CTRL_WARP0) ptx::tmem_dealloc(tmem_base, Cfg::TMEM_COLS);
 }
 
-template <bool A_KMAJOR, int KC>
+template <bool A_KMAJOR, int KC, int SV>
 __global__ void __launch_bounds__(640, 1) shgemm_tm_kernel(const __grid_constant__ TileGemmParams p) {
-    tm_kernel_body<A_KMAJOR, KC>(p);
+    tm_kernel_body<A_KMAJOR, KC, SV>(p);
 }
 
 }  // namespace shgemm_b200

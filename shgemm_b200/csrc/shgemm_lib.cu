@@ -58,6 +58,7 @@ struct shgemm_b200_handle {
     int autotune_mode = 1;  // SHGEMM_CFG_AUTOTUNE
     int tile_kernel = 0;    // SHGEMM_CFG_TILE_KERNEL
     int k_chunk = 64;       // SHGEMM_CFG_K_CHUNK
+    int tm_stages = 0;      // SHGEMM_CFG_TM_STAGES
     std::mutex tune_mu;
     std::map<uint64_t, shgemm_b200_tuned_config> tuned;
     // host-buffer entry: device staging (A and three column-block slots of B and C), one
@@ -166,14 +167,18 @@ KernelEntry kernel_table(int tc, int bn, int ak, int bk) {
 }
 
 // Tensor-memory operand kernels (binary16 compute, 128 x 256 tiles, B K-major).
-template <bool AK, int KC>
+template <bool AK, int KC, int SV>
 KernelEntry tm_entry() {
-    return {reinterpret_cast<void*>(&shgemm_tm_kernel<AK, KC>), TmCfg<AK, KC>::SMEM_BYTES};
+    return {reinterpret_cast<void*>(&shgemm_tm_kernel<AK, KC, SV>), TmCfg<AK, KC, SV>::SMEM_BYTES};
 }
-// kc: k-steps of 64 per FP32 drain (1 or 2)
-KernelEntry tm_kernel_table(bool ak, int kc) {
-    if (kc == 2) return ak ? tm_entry<true, 2>() : tm_entry<false, 2>();
-    return ak ? tm_entry<true, 1>() : tm_entry<false, 1>();
+// kc: k-steps of 64 per FP32 drain (1 or 2); sv: operand ring variant (0 or 1)
+KernelEntry tm_kernel_table(bool ak, int kc, int sv) {
+    if (sv == 1) {
+        if (kc == 2) return ak ? tm_entry<true, 2, 1>() : tm_entry<false, 2, 1>();
+        return ak ? tm_entry<true, 1, 1>() : tm_entry<false, 1, 1>();
+    }
+    if (kc == 2) return ak ? tm_entry<true, 2, 0>() : tm_entry<false, 2, 0>();
+    return ak ? tm_entry<true, 1, 0>() : tm_entry<false, 1, 0>();
 }
 
 template <int TC, int BN, bool AK, bool BW>
@@ -482,6 +487,8 @@ struct Plan {
     int total_steps;
     int slices;
     int steps_per_slice;
+    int kc;  // tensor-memory kernel: k-steps of 64 per FP32 drain (0: the handle's SHGEMM_CFG_K_CHUNK)
+    int sv;  // tensor-memory kernel: operand ring variant (-1: the handle's SHGEMM_CFG_TM_STAGES)
 };
 
 double wave_efficiency(long long units, int sms) {
@@ -509,6 +516,12 @@ uint64_t tune_key(int tc, int op_a, int op_b, size_t m, size_t n, size_t k) {
            (static_cast<uint64_t>(op_b) << 25) | (static_cast<uint64_t>(ilog2(m)) << 16) |
            (static_cast<uint64_t>(ilog2(n)) << 8) | static_cast<uint64_t>(ilog2(k));
 }
+// Grouped launches: the tile N of the problems in one n bucket, floor(log2 n).
+constexpr uint64_t kTuneGrouped = uint64_t(1) << 30;
+uint64_t tune_key_grouped(int tc, int op_a, int b_fp32, int log2n) {
+    return kTuneGrouped | (static_cast<uint64_t>(tc) << 27) | (static_cast<uint64_t>(op_a) << 26) |
+           (static_cast<uint64_t>(b_fp32) << 25) | (static_cast<uint64_t>(log2n) << 8);
+}
 
 // A tuned configuration applied to a shape: the tile N and the slice count it names,
 // the slices capped by what the workspace holds and by the k-steps there are.
@@ -527,12 +540,15 @@ Plan plan_from_tuned(const shgemm_b200_tuned_config& t, size_t m, size_t n, size
     slices = std::min({slices, std::max(fit, 1), p.total_steps});
     p.steps_per_slice = (p.total_steps + slices - 1) / slices;
     p.slices = (p.total_steps + p.steps_per_slice - 1) / p.steps_per_slice;
+    p.kc = t.k_chunk == 128 ? 2 : 0;  // a 64-k entry leaves the handle's SHGEMM_CFG_K_CHUNK in force
+    p.sv = t.stages == 1 ? 1 : 0;
     return p;
 }
 
 Plan make_plan_for(int num_sms, int fixed_level, long long split_k, size_t m, size_t n, size_t k, int tc,
                    size_t ws_bytes) {
     Plan p{};
+    p.sv = -1;
     const int bk = (tc == kFP16) ? 64 : 32;
     p.total_steps = static_cast<int>((k + bk - 1) / bk);
     p.tiles_m = static_cast<int>((m + 127) / 128);
@@ -656,12 +672,12 @@ int shgemm_b200_create(shgemm_b200_handle_t* out, int device) {
                         return SHGEMM_STATUS_NOT_SUPPORTED;
                     }
                 }
-    for (int ak = 0; ak < 2; ++ak) {
-        for (int kc = 1; kc <= 2; ++kc) {
-            KernelEntry e = tm_kernel_table(ak != 0, kc);
-            cudaFuncSetAttribute(e.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, e.smem);
-        }
-    }
+    for (int ak = 0; ak < 2; ++ak)
+        for (int kc = 1; kc <= 2; ++kc)
+            for (int sv = 0; sv < 2; ++sv) {
+                KernelEntry e = tm_kernel_table(ak != 0, kc, sv);
+                cudaFuncSetAttribute(e.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, e.smem);
+            }
     for (int tc = 0; tc < 2; ++tc)
         for (int ak = 0; ak < 2; ++ak)
             for (int bw = 0; bw < 2; ++bw) {
@@ -751,6 +767,10 @@ int shgemm_b200_set_config(shgemm_b200_handle_t h, int key, long long v) {
             if (v < 0 || v >= (1ll << 31)) return SHGEMM_STATUS_INVALID_VALUE;
             h->host_block_cols = v;
             return SHGEMM_STATUS_OK;
+        case SHGEMM_CFG_TM_STAGES:
+            if (v != 0 && v != 1) return SHGEMM_STATUS_INVALID_VALUE;
+            h->tm_stages = static_cast<int>(v);
+            return SHGEMM_STATUS_OK;
         default:
             return SHGEMM_STATUS_INVALID_VALUE;
     }
@@ -767,6 +787,7 @@ int shgemm_b200_get_config(shgemm_b200_handle_t h, int key, long long* v) {
         case SHGEMM_CFG_TILE_KERNEL: *v = h->tile_kernel; return SHGEMM_STATUS_OK;
         case SHGEMM_CFG_K_CHUNK: *v = h->k_chunk; return SHGEMM_STATUS_OK;
         case SHGEMM_CFG_HOST_BLOCK_COLS: *v = h->host_block_cols; return SHGEMM_STATUS_OK;
+        case SHGEMM_CFG_TM_STAGES: *v = h->tm_stages; return SHGEMM_STATUS_OK;
         default: return SHGEMM_STATUS_INVALID_VALUE;
     }
 }
@@ -941,15 +962,17 @@ static int run_tiled(shgemm_b200_handle_t h, int op_a, int op_b, size_t m, size_
     P.a_read_once = use_tm && pl.tiles_n == 1;
     P.b_blocked = block_b ? 1 : 0;
 
-    const KernelEntry e = use_tm ? tm_kernel_table(a_kmajor, h->k_chunk / 64) : kernel_table(tc, pl.bn, a_kmajor, b_kmajor);
-    const int threads = use_tm ? TmCfg<true>::NUM_THREADS : 512;
+    const int kc = pl.kc ? pl.kc : h->k_chunk / 64;
+    const int sv = pl.sv >= 0 ? pl.sv : h->tm_stages;
+    const KernelEntry e = use_tm ? tm_kernel_table(a_kmajor, kc, sv) : kernel_table(tc, pl.bn, a_kmajor, b_kmajor);
+    const int threads = use_tm ? TmCfg<true, 1, 0>::NUM_THREADS : 512;
     if (!e.fn) return SHGEMM_STATUS_NOT_SUPPORTED;
     const int grid = std::min(P.num_units, h->num_sms);
     if (h->debug_mode) {
         std::printf("[shape=(%zu,%zu,%zu),op_a=%s,op_b=%s,compute_type=%s] kernel_level = %d, tile = 128x%d, "
                     "k_slices = %d, chunk_k = %d, grid = %d%s\n",
                     m, n, k, op_a == kOpN ? "N" : "T", op_b == kOpN ? "N" : "T", tc == kTF32 ? "TF32" : "FP16",
-                    pl.level, pl.bn, pl.slices, use_tm ? h->k_chunk : bk, grid, use_tm ? ", operands in TMEM" : "");
+                    pl.level, pl.bn, pl.slices, use_tm ? 64 * kc : bk, grid, use_tm ? ", operands in TMEM" : "");
     }
     if (block_b) {
         const size_t total = kblocks * n * 8;
@@ -1232,6 +1255,90 @@ static int time_config(shgemm_b200_handle_t h, int op_a, int op_b, size_t m, siz
     return SHGEMM_STATUS_OK;
 }
 
+// The k-chunk accuracy gate samples up to two blocks of C: the top-left and the bottom-right
+// 128 x 128 (one block when they coincide).
+static int sampled_blocks(size_t m, size_t n, size_t* r0, size_t* c0, size_t* bm, size_t* bn) {
+    *bm = std::min<size_t>(m, 128);
+    *bn = std::min<size_t>(n, 128);
+    r0[0] = 0;
+    c0[0] = 0;
+    r0[1] = m - *bm;
+    c0[1] = n - *bn;
+    return (r0[1] == 0 && c0[1] == 0) ? 1 : 2;
+}
+
+// Relative Frobenius error against FP64 (ref64, one buffer per block) of the op_n result C
+// over the sampled blocks; SHGEMM_STATUS_INVALID_VALUE when C and FP64 disagree on finiteness.
+static int block_error(shgemm_b200_handle_t h, size_t m, size_t n, const float* c, size_t ldc, double* const* ref64,
+                       double* err) {
+    size_t r0[2], c0[2], bm, bn;
+    const int nb = sampled_blocks(m, n, r0, c0, &bm, &bn);
+    double d2 = 0, r2 = 0;
+    for (int i = 0; i < nb; ++i) {
+        double out[4];
+        const int st = shgemm_b200_eval_error(h, bm, bn, c + r0[i] + c0[i] * ldc, ldc, kOpN, ref64[i], 1.0, 0.0,
+                                              nullptr, out);
+        if (st != SHGEMM_STATUS_OK) return st;
+        if (out[3] != 0) return SHGEMM_STATUS_INVALID_VALUE;
+        d2 += out[0] * out[0];
+        r2 += out[1] * out[1];
+    }
+    *err = r2 > 0 ? std::sqrt(d2 / r2) : std::sqrt(d2);
+    return SHGEMM_STATUS_OK;
+}
+
+// The accuracy gate of the 128-k chunk: its sampled error against FP64 at most 1.25x the
+// 64-k chunk's (plus an FP32-ulp floor). The FP64 blocks come from the library's evaluation
+// kernels on the same operands.
+static int k_chunk_gate(shgemm_b200_handle_t h, int op_a, int op_b, size_t m, size_t n, size_t k, const float* a,
+                        size_t lda, const void* b, size_t ldb, float* c, size_t ldc, int tc,
+                        shgemm_b200_tuned_config cfg64, shgemm_b200_tuned_config cfg128, bool* pass,
+                        double* e64_out, double* e128_out) {
+    *pass = false;
+    size_t r0[2], c0[2], bm, bn;
+    const int nb = sampled_blocks(m, n, r0, c0, &bm, &bn);
+    double* ref[2] = {nullptr, nullptr};
+    int st = SHGEMM_STATUS_OK;
+    for (int i = 0; i < nb && st == SHGEMM_STATUS_OK; ++i) {
+        if (cudaMalloc(&ref[i], bm * bn * sizeof(double)) != cudaSuccess) {
+            cudaGetLastError();
+            st = SHGEMM_STATUS_ALLOC_FAILED;
+            break;
+        }
+        const float* ab = op_a == kOpN ? a + r0[i] : a + r0[i] * lda;
+        const __half* bh = static_cast<const __half*>(b);
+        const __half* bb = op_b == kOpN ? bh + c0[i] * ldb : bh + c0[i];
+        st = shgemm_b200_eval_dgemm(h, op_a, op_b, bm, bn, k, ab, lda, bb, ldb, ref[i]);
+    }
+    double e[2] = {0, 0};
+    for (int j = 0; j < 2 && st == SHGEMM_STATUS_OK; ++j) {
+        int lvl = 0;
+        st = run_tiled(h, op_a, op_b, m, n, k, 1.0f, a, lda, b, ldb, 0.0f, c, ldc, tc, kOpN, &lvl, h->workspace,
+                       h->workspace_bytes, j == 0 ? &cfg64 : &cfg128);
+        if (st == SHGEMM_STATUS_OK && cudaStreamSynchronize(h->stream) != cudaSuccess) st = SHGEMM_STATUS_CUDA_ERROR;
+        if (st == SHGEMM_STATUS_OK) {
+            int code = 0;
+            if (shgemm_b200_check_error(h, &code) != SHGEMM_STATUS_OK) st = SHGEMM_STATUS_TIMEOUT;
+        }
+        if (st == SHGEMM_STATUS_OK) {
+            const int be = block_error(h, m, n, c, ldc, ref, &e[j]);
+            if (be == SHGEMM_STATUS_INVALID_VALUE)
+                e[j] = 1e300;  // a finite/non-finite disagreement: the candidate fails
+            else
+                st = be;
+        }
+    }
+    for (double* r : ref) cudaFree(r);
+    if (st != SHGEMM_STATUS_OK) {
+        cudaGetLastError();
+        return st;
+    }
+    *e64_out = e[0];
+    *e128_out = e[1];
+    *pass = e[1] <= 1.25 * e[0] + 4.0 * 5.9604644775390625e-8;
+    return SHGEMM_STATUS_OK;
+}
+
 int shgemm_b200_autotune(shgemm_b200_handle_t h, int op_a, int op_b, size_t m, size_t n, size_t k, const float* a,
                          size_t lda, const void* b, size_t ldb, float* c, size_t ldc, int tc,
                          shgemm_b200_tuned_config* best_out) {
@@ -1254,16 +1361,30 @@ int shgemm_b200_autotune(shgemm_b200_handle_t h, int op_a, int op_b, size_t m, s
     const int fit = static_cast<int>(std::min<size_t>(h->workspace_bytes / per_slice, 1024));
     const int tile_ns[] = {64, 128, 256};
     const int slice_set[] = {1, 2, 3, 4, 6, 8, 12, 16};
+    auto cfg_of = [](int bn, int sl, int gm, int sv, int kchunk) {
+        shgemm_b200_tuned_config c{};
+        c.tile_n = bn;
+        c.slices = sl;
+        c.group_m = gm;
+        c.stages = sv;
+        c.k_chunk = kchunk;
+        return c;
+    };
+    auto same = [](const shgemm_b200_tuned_config& x, const shgemm_b200_tuned_config& y) {
+        return x.tile_n == y.tile_n && x.slices == y.slices && x.group_m == y.group_m && x.stages == y.stages &&
+               x.k_chunk == y.k_chunk;
+    };
     // one timed run of the heuristic plan sizes the repetitions
     shgemm_b200_tuned_config best{};
     {
         const Plan hp = make_plan_for(h->num_sms, SHGEMM_LEVEL_AUTO, 0, m, n, k, tc, h->workspace_bytes);
-        best = {hp.bn, hp.slices, static_cast<int>(h->group_m), 0.0f};
+        best = cfg_of(hp.bn, hp.slices, static_cast<int>(h->group_m), h->tm_stages, 64);
         const int st = time_config(h, op_a, op_b, m, n, k, a, lda, b, ldb, c, ldc, tc, best, 1, &best.time_us);
         if (st != SHGEMM_STATUS_OK) return st;
     }
     const int reps = best.time_us > 50000.0f ? 1 : 3;
     auto consider = [&](shgemm_b200_tuned_config cand) -> int {
+        if (same(cand, best) && best.time_us < 3.0e38f) return SHGEMM_STATUS_OK;
         const int st = time_config(h, op_a, op_b, m, n, k, a, lda, b, ldb, c, ldc, tc, cand, reps, &cand.time_us);
         if (st != SHGEMM_STATUS_OK) return st;
         if (cand.time_us < best.time_us) best = cand;
@@ -1281,24 +1402,47 @@ int shgemm_b200_autotune(shgemm_b200_handle_t h, int op_a, int op_b, size_t m, s
         const long long tiles = static_cast<long long>((m + 127) / 128) * static_cast<long long>((n + bn - 1) / bn);
         for (int sl : slice_set) {
             if (sl > 1 && (sl > fit || steps / sl < 4 || tiles >= 2LL * h->num_sms)) continue;
-            const shgemm_b200_tuned_config cand{bn, sl, static_cast<int>(h->group_m), 0.0f};
-            if (cand.tile_n == best.tile_n && cand.slices == best.slices && cand.group_m == best.group_m) continue;
-            const int st = consider(cand);
+            const int st = consider(cfg_of(bn, sl, static_cast<int>(h->group_m), best.stages, 64));
             if (st != SHGEMM_STATUS_OK) return st;
         }
     }
     for (int gm : {2, 4, 8, 16, 32}) {
-        if (gm == best.group_m) continue;
-        const int st = consider({best.tile_n, best.slices, gm, 0.0f});
+        const int st = consider(cfg_of(best.tile_n, best.slices, gm, best.stages, 64));
         if (st != SHGEMM_STATUS_OK) return st;
+    }
+    // The 128 x 256 binary16 tiles of the tensor-memory kernel: its operand ring, then the
+    // 128-k drain chunk, which is kept only if it is faster and passes the accuracy gate.
+    const bool tm = tc == kFP16 && best.tile_n == 256 && op_b == kOpN && h->tile_kernel == 0;
+    double gate_e64 = -1, gate_e128 = -1;
+    int gate = -1;  // -1 not run, 0 failed, 1 passed
+    if (tm) {
+        int st = consider(cfg_of(best.tile_n, best.slices, best.group_m, 1 - best.stages, 64));
+        if (st != SHGEMM_STATUS_OK) return st;
+        shgemm_b200_tuned_config c128 = cfg_of(best.tile_n, best.slices, best.group_m, best.stages, 128);
+        st = time_config(h, op_a, op_b, m, n, k, a, lda, b, ldb, c, ldc, tc, c128, reps, &c128.time_us);
+        if (st != SHGEMM_STATUS_OK) return st;
+        if (c128.time_us < best.time_us) {
+            bool pass = false;
+            st = k_chunk_gate(h, op_a, op_b, m, n, k, a, lda, b, ldb, c, ldc, tc, best, c128, &pass, &gate_e64,
+                              &gate_e128);
+            if (st != SHGEMM_STATUS_OK) return st;
+            gate = pass ? 1 : 0;
+            if (pass) best = c128;
+        }
     }
     {
         std::lock_guard<std::mutex> lk(h->tune_mu);
         h->tuned[tune_key(tc, op_a, op_b, m, n, k)] = best;
     }
-    if (h->debug_mode)
-        std::printf("[autotune] (%zu,%zu,%zu) %s: tile = 128x%d, k_slices = %d, group_m = %d, %.1f us\n", m, n, k,
-                    tc == kTF32 ? "TF32" : "FP16", best.tile_n, best.slices, best.group_m, best.time_us);
+    if (h->debug_mode) {
+        std::printf("[autotune] (%zu,%zu,%zu) %s: tile = 128x%d, k_slices = %d, group_m = %d, stages = %d, "
+                    "k_chunk = %d, %.1f us\n",
+                    m, n, k, tc == kTF32 ? "TF32" : "FP16", best.tile_n, best.slices, best.group_m, best.stages,
+                    best.k_chunk, best.time_us);
+        if (gate >= 0)
+            std::printf("[autotune] k_chunk 128 accuracy gate %s: sampled error %.3e vs %.3e at 64\n",
+                        gate ? "passed" : "failed", gate_e128, gate_e64);
+    }
     if (best_out) *best_out = best;
     return SHGEMM_STATUS_OK;
 }
@@ -1313,19 +1457,26 @@ int shgemm_b200_autotune_lookup(shgemm_b200_handle_t h, int op_a, int op_b, size
     return SHGEMM_STATUS_OK;
 }
 
+// Text format, one entry per line:
+//   kind tc op_a op_b log2m log2n log2k tile_n slices group_m stages k_chunk time_us
+// kind 0: a plain shape bucket; kind 1: a grouped n bucket (op_b holds the B format, 1 =
+// FP32; log2m and log2k are 0). Lines of the earlier 10-field form (no kind, stages and
+// k_chunk) load as plain entries with the default ring and a 64-k chunk.
 int shgemm_b200_autotune_save(shgemm_b200_handle_t h, const char* path) {
     if (!h || !path) return SHGEMM_STATUS_INVALID_VALUE;
     FILE* f = std::fopen(path, "w");
     if (!f) return SHGEMM_STATUS_INVALID_VALUE;
     std::lock_guard<std::mutex> lk(h->tune_mu);
-    std::fprintf(f, "# shgemm_b200 autotune v1: tc op_a op_b log2m log2n log2k tile_n slices group_m time_us\n");
+    std::fprintf(f, "# shgemm_b200 autotune v2: kind tc op_a op_b log2m log2n log2k tile_n slices group_m stages "
+                    "k_chunk time_us\n");
     for (const auto& kv : h->tuned) {
         const uint64_t key = kv.first;
-        std::fprintf(f, "%d %d %d %d %d %d %d %d %d %.3f\n", static_cast<int>((key >> 27) & 1),
-                     static_cast<int>((key >> 26) & 1), static_cast<int>((key >> 25) & 1),
-                     static_cast<int>((key >> 16) & 0xFF), static_cast<int>((key >> 8) & 0xFF),
-                     static_cast<int>(key & 0xFF), kv.second.tile_n, kv.second.slices, kv.second.group_m,
-                     kv.second.time_us);
+        const shgemm_b200_tuned_config& t = kv.second;
+        std::fprintf(f, "%d %d %d %d %d %d %d %d %d %d %d %d %.3f\n", (key & kTuneGrouped) ? 1 : 0,
+                     static_cast<int>((key >> 27) & 1), static_cast<int>((key >> 26) & 1),
+                     static_cast<int>((key >> 25) & 1), static_cast<int>((key >> 16) & 0xFF),
+                     static_cast<int>((key >> 8) & 0xFF), static_cast<int>(key & 0xFF), t.tile_n, t.slices, t.group_m,
+                     t.stages, t.k_chunk, t.time_us);
     }
     const bool ok = std::fclose(f) == 0;
     return ok ? SHGEMM_STATUS_OK : SHGEMM_STATUS_INVALID_VALUE;
@@ -1340,19 +1491,45 @@ int shgemm_b200_autotune_load(shgemm_b200_handle_t h, const char* path) {
     std::map<uint64_t, shgemm_b200_tuned_config> add;
     while (std::fgets(line, sizeof(line), f)) {
         if (line[0] == '#' || line[0] == '\n') continue;
-        int tc, oa, ob, lm, ln, lk, bn, sl, gm;
+        int kind = 0, tc, oa, ob, lm, ln, lk, bn, sl, gm, sv = 0, kch = 64;
         float us;
-        if (std::sscanf(line, "%d %d %d %d %d %d %d %d %d %f", &tc, &oa, &ob, &lm, &ln, &lk, &bn, &sl, &gm, &us) != 10 ||
-            (tc != kFP16 && tc != kTF32) || (oa != 0 && oa != 1) || (ob != 0 && ob != 1) || lm < 0 || lm > 40 ||
-            ln < 0 || ln > 40 || lk < 0 || lk > 40 || !tile_n_valid(tc, bn) || sl < 1 || sl > 1024 || gm < 1 ||
-            gm > 1024) {
+        const int got = std::sscanf(line, "%d %d %d %d %d %d %d %d %d %d %d %d %f", &kind, &tc, &oa, &ob, &lm, &ln,
+                                    &lk, &bn, &sl, &gm, &sv, &kch, &us);
+        if (got != 13) {  // the earlier form: tc op_a op_b log2m log2n log2k tile_n slices group_m time_us
+            kind = 0;
+            sv = 0;
+            kch = 64;
+            if (std::sscanf(line, "%d %d %d %d %d %d %d %d %d %f", &tc, &oa, &ob, &lm, &ln, &lk, &bn, &sl, &gm, &us) !=
+                10) {
+                status = SHGEMM_STATUS_INVALID_VALUE;
+                break;
+            }
+        }
+        const bool bad_common = (kind != 0 && kind != 1) || (tc != kFP16 && tc != kTF32) || (oa != 0 && oa != 1) ||
+                                (ob != 0 && ob != 1) || lm < 0 || lm > 40 || ln < 0 || ln > 40 || lk < 0 || lk > 40;
+        const bool bad_plain = kind == 0 && (!tile_n_valid(tc, bn) || sl < 1 || sl > 1024 || gm < 1 || gm > 1024 ||
+                                             (sv != 0 && sv != 1) || (kch != 64 && kch != 128));
+        const bool bad_grouped = kind == 1 && !(bn == 32 || bn == 64 || bn == 128 || bn == 256);
+        if (bad_common || bad_plain || bad_grouped) {
             status = SHGEMM_STATUS_INVALID_VALUE;
             break;
         }
-        const uint64_t key = (static_cast<uint64_t>(tc) << 27) | (static_cast<uint64_t>(oa) << 26) |
-                             (static_cast<uint64_t>(ob) << 25) | (static_cast<uint64_t>(lm) << 16) |
-                             (static_cast<uint64_t>(ln) << 8) | static_cast<uint64_t>(lk);
-        add[key] = {bn, sl, gm, us};
+        shgemm_b200_tuned_config t{};
+        t.tile_n = bn;
+        t.slices = kind ? 1 : sl;
+        t.group_m = kind ? 1 : gm;
+        t.time_us = us;
+        t.stages = kind ? 0 : sv;
+        t.k_chunk = kind ? 64 : kch;
+        uint64_t key;
+        if (kind == 1) {
+            key = tune_key_grouped(tc, oa, ob, ln);
+        } else {
+            key = (static_cast<uint64_t>(tc) << 27) | (static_cast<uint64_t>(oa) << 26) |
+                  (static_cast<uint64_t>(ob) << 25) | (static_cast<uint64_t>(lm) << 16) |
+                  (static_cast<uint64_t>(ln) << 8) | static_cast<uint64_t>(lk);
+        }
+        add[key] = t;
     }
     std::fclose(f);
     if (status != SHGEMM_STATUS_OK) return status;
@@ -1606,12 +1783,44 @@ int shgemm_b200_eval_error(shgemm_b200_handle_t h, size_t m, size_t n, const flo
 // Grouped launches: many problems, one persistent kernel.
 namespace {
 
+int grouped_max_bn(int tc, bool b_wide) {
+    return tc == kFP16 ? kGroupedMaxBnF16 : (b_wide ? kGroupedMaxBnTf32Wide : kGroupedMaxBnTf32);
+}
+
+// The default rule: the smallest power of two (>= 32) covering n, up to the kernel's tile.
 int grouped_tile_n(int tc, bool b_wide, size_t n) {
-    const int cap = tc == kFP16 ? kGroupedMaxBnF16 : (b_wide ? kGroupedMaxBnTf32Wide : kGroupedMaxBnTf32);
+    const int cap = grouped_max_bn(tc, b_wide);
     int bn = 32;
     while (bn < cap && static_cast<size_t>(bn) < n) bn *= 2;
     return bn;
 }
+
+bool grouped_bn_valid(int tc, bool b_wide, int bn) {
+    return (bn == 32 || bn == 64 || bn == 128 || bn == 256) && bn <= grouped_max_bn(tc, b_wide);
+}
+
+// Tile N per n bucket for one staging call: the autotuner's entries (when the handle uses
+// them), else the default rule; looked up once per bucket.
+struct GroupedTileChoice {
+    int bn_of[64] = {};
+    shgemm_b200_handle_t h = nullptr;
+    int tc = 0, op_a = 0;
+    bool b_wide = false;
+    int get(size_t n) {
+        const int L = ilog2(n);
+        if (L < 0 || L >= 64) return grouped_tile_n(tc, b_wide, n);
+        if (!bn_of[L]) {
+            int bn = 0;
+            if (h->autotune_mode != 0) {
+                std::lock_guard<std::mutex> lk(h->tune_mu);
+                auto it = h->tuned.find(tune_key_grouped(tc, op_a, b_wide ? 1 : 0, L));
+                if (it != h->tuned.end() && grouped_bn_valid(tc, b_wide, it->second.tile_n)) bn = it->second.tile_n;
+            }
+            bn_of[L] = bn ? bn : -1;
+        }
+        return bn_of[L] > 0 ? bn_of[L] : grouped_tile_n(tc, b_wide, n);
+    }
+};
 
 // Writes the problem table and the unit list of a batch into table t's pinned host staging.
 int grouped_stage(shgemm_b200_handle_t h, GroupedTable& t, bool b_wide, int op_a, int op_b, int tc, int op_c,
@@ -1636,6 +1845,11 @@ int grouped_stage(shgemm_b200_handle_t h, GroupedTable& t, bool b_wide, int op_a
     const int bk = tc == kFP16 ? 64 : 32;
     b_wide = b_wide && tc == kTF32;  // B given as FP32 (exact binary16 values)
     const size_t b_elem = b_wide ? 4 : 2;
+    GroupedTileChoice tiles;
+    tiles.h = h;
+    tiles.tc = tc;
+    tiles.op_a = op_a;
+    tiles.b_wide = b_wide;
     struct Cost {
         long long cost;
         int2 unit;
@@ -1651,7 +1865,7 @@ int grouped_stage(shgemm_b200_handle_t h, GroupedTable& t, bool b_wide, int op_a
         if (!q.c || q.ldc < c_rows) return SHGEMM_STATUS_INVALID_VALUE;
         if (q.m >= (1u << 31) || q.n >= (1u << 31) || q.k >= (1u << 31) || (q.m + 127) / 128 > 0xFFFF)
             return SHGEMM_STATUS_NOT_SUPPORTED;
-        const int bn = grouped_tile_n(tc, b_wide, q.n);
+        const int bn = tiles.get(q.n);
         const long long tiles_n = static_cast<long long>((q.n + bn - 1) / bn);
         if (tiles_n > 0x7FFF) return SHGEMM_STATUS_NOT_SUPPORTED;
         if (q.k > 0) {
@@ -1774,6 +1988,123 @@ int shgemm_b200_shgemm_grouped(shgemm_b200_handle_t h, int op_a, int op_b, int c
 }  // extern "C"
 
 // ---------------------------------------------------------------------------
+// Autotuning of grouped launches: tile N per n bucket.
+extern "C" {
+
+int shgemm_b200_autotune_grouped(shgemm_b200_handle_t h, int op_a, int op_b, int tc, int op_c,
+                                 const shgemm_b200_problem* probs, int count, int* tuned_out) {
+    if (tuned_out) *tuned_out = 0;
+    if (!h || count < 1 || !probs) return SHGEMM_STATUS_INVALID_VALUE;
+    DeviceGuard g(h->device);
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(h->stream, &cap) != cudaSuccess || cap != cudaStreamCaptureStatusNone) {
+        cudaGetLastError();
+        return SHGEMM_STATUS_NOT_SUPPORTED;
+    }
+    const bool b_wide = tc == kTF32 && h->grouped_b_fp32 != 0;
+    const int cap_bn = grouped_max_bn(tc, b_wide);
+    std::vector<int> buckets;
+    for (int i = 0; i < count; ++i)
+        if (probs[i].m > 0 && probs[i].n > 0) buckets.push_back(ilog2(probs[i].n));
+    std::sort(buckets.begin(), buckets.end());
+    buckets.erase(std::unique(buckets.begin(), buckets.end()), buckets.end());
+    if (buckets.empty()) return SHGEMM_STATUS_OK;
+
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) {
+        cudaGetLastError();
+        if (e0) cudaEventDestroy(e0);
+        return SHGEMM_STATUS_CUDA_ERROR;
+    }
+    // the batch's median time with the current table (one untimed launch first)
+    auto time_batch = [&](float* us) -> int {
+        std::vector<float> t;
+        for (int r = -1; r < 3; ++r) {
+            cudaEventRecord(e0, h->stream);
+            const int st = grouped_run(h, h->grouped, b_wide, op_a, op_b, tc, op_c, probs, count);
+            cudaEventRecord(e1, h->stream);
+            if (st != SHGEMM_STATUS_OK) return st;
+            if (cudaEventSynchronize(e1) != cudaSuccess) return SHGEMM_STATUS_CUDA_ERROR;
+            float ms = 0;
+            cudaEventElapsedTime(&ms, e0, e1);
+            if (r >= 0) t.push_back(ms * 1000.0f);
+        }
+        int code = 0;
+        if (shgemm_b200_check_error(h, &code) != SHGEMM_STATUS_OK) return SHGEMM_STATUS_TIMEOUT;
+        std::sort(t.begin(), t.end());
+        *us = t[t.size() / 2];
+        return SHGEMM_STATUS_OK;
+    };
+    auto set_entry = [&](int L, int bn, float us) {
+        std::lock_guard<std::mutex> lk(h->tune_mu);
+        shgemm_b200_tuned_config c{};
+        c.tile_n = bn;
+        c.slices = 1;
+        c.group_m = 1;
+        c.time_us = us;
+        c.k_chunk = 64;
+        h->tuned[tune_key_grouped(tc, op_a, b_wide ? 1 : 0, L)] = c;
+    };
+    const int saved_mode = h->autotune_mode;
+    if (h->autotune_mode == 0) h->autotune_mode = 1;  // the timing runs must see the trial entries
+    // start from the current choice of every bucket (an entry, or the default rule)
+    std::vector<int> choice(buckets.size());
+    for (size_t b = 0; b < buckets.size(); ++b) {
+        const int L = buckets[b];
+        int bn = 0;
+        {
+            std::lock_guard<std::mutex> lk(h->tune_mu);
+            auto it = h->tuned.find(tune_key_grouped(tc, op_a, b_wide ? 1 : 0, L));
+            if (it != h->tuned.end() && grouped_bn_valid(tc, b_wide, it->second.tile_n)) bn = it->second.tile_n;
+        }
+        choice[b] = bn ? bn : grouped_tile_n(tc, b_wide, size_t(1) << L);
+        set_entry(L, choice[b], 0.0f);
+    }
+    float best_us = 0;
+    int st = time_batch(&best_us);
+    for (size_t b = 0; b < buckets.size() && st == SHGEMM_STATUS_OK; ++b) {
+        const int L = buckets[b];
+        for (int bn = 32; bn <= cap_bn && st == SHGEMM_STATUS_OK; bn *= 2) {
+            if (bn == choice[b]) continue;
+            set_entry(L, bn, 0.0f);
+            float us = 0;
+            st = time_batch(&us);
+            if (st == SHGEMM_STATUS_OK && us < best_us) {
+                best_us = us;
+                choice[b] = bn;
+            }
+        }
+        set_entry(L, choice[b], best_us);
+    }
+    h->autotune_mode = saved_mode;
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (st != SHGEMM_STATUS_OK) {
+        cudaGetLastError();
+        return st;
+    }
+    if (h->debug_mode) {
+        for (size_t b = 0; b < buckets.size(); ++b)
+            std::printf("[autotune grouped] %s n in [%zu, %zu): tile N = %d\n", tc == kTF32 ? "TF32" : "FP16",
+                        size_t(1) << buckets[b], size_t(2) << buckets[b], choice[b]);
+        std::printf("[autotune grouped] batch of %d problems: %.1f us\n", count, best_us);
+    }
+    if (tuned_out) *tuned_out = static_cast<int>(buckets.size());
+    return SHGEMM_STATUS_OK;
+}
+
+int shgemm_b200_autotune_grouped_lookup(shgemm_b200_handle_t h, int op_a, int tc, int b_fp32, size_t n, int* tile_n) {
+    if (!h || !tile_n || n == 0) return SHGEMM_STATUS_INVALID_VALUE;
+    std::lock_guard<std::mutex> lk(h->tune_mu);
+    auto it = h->tuned.find(tune_key_grouped(tc, op_a, b_fp32 ? 1 : 0, ilog2(n)));
+    if (it == h->tuned.end()) return SHGEMM_STATUS_INVALID_VALUE;
+    *tile_n = it->second.tile_n;
+    return SHGEMM_STATUS_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
 // Allocation-free split-K entry point.
 //
 // For callers that cannot call cudaMalloc (for example code running inside an
@@ -1834,15 +2165,16 @@ int noalloc_setup(int dev, NoAllocDevice*& out) {
                             return SHGEMM_STATUS_NOT_SUPPORTED;
                         }
                     }
-        for (int ak = 0; ak < 2; ++ak) {
-            for (int kc = 1; kc <= 2; ++kc) {
-                KernelEntry e = tm_kernel_table(ak != 0, kc);
-                if (cudaFuncSetAttribute(e.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, e.smem) != cudaSuccess) {
-                    cudaGetLastError();
-                    return SHGEMM_STATUS_NOT_SUPPORTED;
+        for (int ak = 0; ak < 2; ++ak)
+            for (int kc = 1; kc <= 2; ++kc)
+                for (int sv = 0; sv < 2; ++sv) {
+                    KernelEntry e = tm_kernel_table(ak != 0, kc, sv);
+                    if (cudaFuncSetAttribute(e.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, e.smem) !=
+                        cudaSuccess) {
+                        cudaGetLastError();
+                        return SHGEMM_STATUS_NOT_SUPPORTED;
+                    }
                 }
-            }
-        }
         d.num_sms = sms;
         const char* dbg = std::getenv("MTK_SHGEMM_DEBUG");
         d.debug_mode = (dbg && dbg[0] == '1') ? 1u : 0u;
