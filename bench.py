@@ -54,6 +54,11 @@ WORKLOADS = {
     "square16k_tn": dict(m=16384, n=16384, k=16384, op_a=1, op_b=0, tc=0, alpha=1.0, beta=0.5, dist="wide",
                          desc="large square SHGEMM 16384^3 TN, fp16 compute, A N(0,1)*2^U(-15,15), B N(0,1), "
                               "beta=0.5"),
+    # the large square SHGEMM with lda = m + 1 (4-byte aligned columns): TMA cannot address A, so
+    # it is staged into the workspace (sized here to hold all of A: one k-slab)
+    "square16k_oddld": dict(m=16384, n=16384, k=16384, op_a=0, op_b=0, tc=0, alpha=1.0, beta=0.5, dist="wide",
+                            lda_pad=1, desc="large square SHGEMM 16384^3 NN with lda = 16385, fp16 compute, "
+                                            "A N(0,1)*2^U(-15,15), B N(0,1), beta=0.5"),
     # a smaller square case of the same kernel, for profiler captures (inputs still exceed L2)
     "square8k": dict(m=8192, n=8192, k=8192, op_a=0, op_b=0, tc=0, alpha=1.0, beta=0.5, dist="wide",
                      desc="square SHGEMM 8192^3 NN, fp16 compute, A N(0,1)*2^U(-15,15), B N(0,1), beta=0.5"),
@@ -78,11 +83,18 @@ WORKLOADS = {
     "grouped": dict(m=0, n=0, k=0, op_a=0, op_b=0, tc=0, alpha=1.0, beta=0.0, dist="grouped", count=512, bound="hbm",
                     desc="grouped batch of 512 uneven right sketches Y_i = A_i Omega_i, m_i log-U[64,8192], "
                          "k_i log-U[256,16384], n_i in {32,64,128,256}, A_i rank n_i/2 (sigma_j = j^-1.5) + N(0,1e-4), "
-                         "Omega_i Rademacher/sqrt(n_i), fp16 compute, one CUDA-graph-captured launch"),
+                         "Omega_i Rademacher/sqrt(n_i) (block-sign +-1 operand, the scale as alpha), fp16 compute, "
+                         "one CUDA-graph-captured launch"),
     # the reference's power test: square 2^10 .. 2^14 NN, TF32 and fp16, ~10 s loops under NVML
     "energy": dict(m=0, n=0, k=0, op_a=0, op_b=0, tc=0, alpha=1.0, beta=0.0, dist="energy",
                    desc="energy per call: square SHGEMM m = n = k = 2^10 .. 2^14 NN, inputs uniform (0, 1], "
                         "tf32 and fp16 compute, a ~10 s loop per shape with NVML power sampled every 50 ms"),
+    # the same batch with Omega_i generated inside the grouped kernel (no Omega in memory)
+    "grouped_fused": dict(m=0, n=0, k=0, op_a=0, op_b=0, tc=0, alpha=1.0, beta=0.0, dist="grouped", count=512,
+                          bound="hbm", fused=True,
+                          desc="grouped batch of 512 uneven right sketches (shapes as the fp16 batch), Omega_i "
+                               "block-sign Rademacher generated by the grouped kernel's B producer (no Omega reads), "
+                               "scale 1/sqrt(n_i) as alpha, fp16 compute, one CUDA-graph-captured launch"),
     # the same batch in TF32 compute, Omega_i handed over widened to FP32 (as the sketch server keeps it)
     "grouped_tf32": dict(m=0, n=0, k=0, op_a=0, op_b=0, tc=1, alpha=1.0, beta=0.0, dist="grouped", count=512,
                          bound="hbm", b_fp32=True,
@@ -270,9 +282,9 @@ def make_inputs(wl, dev, seed=0):
     g = torch.Generator(device=dev)
     g.manual_seed(seed)
     m, n, k = wl["m"], wl["n"], wl["k"]
-    a_rows = m if wl["op_a"] == 0 else k
+    a_rows = (m if wl["op_a"] == 0 else k) + wl.get("lda_pad", 0)  # a padded lda: not TMA-addressable
     b_rows = k if wl["op_b"] == 0 else n
-    na = m * k
+    na = a_rows * (k if wl["op_a"] == 0 else m)
     nb = k * n
     if wl["dist"] == "wide":
         A = torch.randn(na, generator=g, device=dev)
@@ -363,11 +375,15 @@ def square_case(args, wl, ctx, traffic_key, tf32_error=False, e2e=True):
     if (wl["tc"] == 1 or tf32_error) and wl["op_b"] == 0:
         # room for the widened FP32 copy of B (the TF32 route that loads B unconverted)
         h.set_workspace_size(max(64 << 20, n * ((k + 3) // 4 * 4) * 4 + (1 << 20)))
+    if wl.get("lda_pad"):
+        # room for the staged copy of A (aligned leading dimension) in one k-slab
+        cols = k if wl["op_a"] == 0 else m
+        h.set_workspace_size((64 << 20) + ((lda - wl["lda_pad"] + 3) // 4 * 4) * cols * 4)
     if wl["tc"] == 0 and wl["op_b"] == 0 and ldb * 2 >= (1 << 20):
         # room for B re-laid out as contiguous k-blocks (columns >= 1 MiB apart) plus the split-K partials
         h.set_workspace_size((64 << 20) + n * ((k + 63) // 64 * 64) * 2)
     tuned = None
-    if not args.no_autotune and op_c == 0:
+    if not args.no_autotune and op_c == 0 and not wl.get("lda_pad"):  # tuning takes TMA-addressable operands
         tuned = h.autotune(wl["op_a"], wl["op_b"], m, n, k, A, lda, B, ldb, C, ldc, wl["tc"])
         if C0 is not None:
             C.copy_(C0)
@@ -501,9 +517,14 @@ def square_case(args, wl, ctx, traffic_key, tf32_error=False, e2e=True):
 
 # ---------------------------------------------------------------- grouped batch
 def make_grouped_batch(count, dev, seed=0):
-    """The uneven sketch batch on the device; returns problem tuples and sizes."""
+    """The uneven sketch batch on the device; returns problem tuples, sizes, the tensors to
+    keep, and each problem's Omega seed. Omega_i is the block-sign Rademacher operand of its
+    seed (entries +1 / -1, generated on the device) and the 1/sqrt(n_i) scale is alpha, so the
+    same batch can also run with Omega_i generated inside the grouped kernel."""
     import numpy as np
     import torch
+
+    from shgemm_b200 import server as srv
 
     rng = np.random.default_rng(seed)
     g = torch.Generator(device=dev)
@@ -511,8 +532,8 @@ def make_grouped_batch(count, dev, seed=0):
     ms = np.exp(rng.uniform(np.log(64), np.log(8192), count)).astype(int)
     ks = np.exp(rng.uniform(np.log(256), np.log(16384), count)).astype(int)
     ns = rng.choice([32, 64, 128, 256], count)
-    probs, shapes, keep = [], [], []
-    for m, k, n in zip(ms, ks, ns):
+    probs, shapes, keep, seeds = [], [], [], []
+    for i, (m, k, n) in enumerate(zip(ms, ks, ns)):
         m, k, n = int(m), int(k), int(n)
         lda = (m + 3) // 4 * 4
         ldb = (k + 7) // 8 * 8
@@ -524,16 +545,18 @@ def make_grouped_batch(count, dev, seed=0):
         Afull = torch.empty(k, lda, device=dev)  # column-major m x k with leading dimension lda
         Afull[:, :m] = ((U * sig) @ V.T).T
         Afull[:, :m].add_(torch.randn(k, m, device=dev, generator=g), alpha=1e-2)
-        Om = torch.empty(n, ldb, device=dev, dtype=torch.float16)  # column-major k x n, ld = ldb
-        Om[:, :k] = ((torch.randint(0, 2, (n, k), device=dev, generator=g) * 2 - 1).float() / np.sqrt(n)).half()
+        Om = torch.zeros(n, ldb, device=dev, dtype=torch.float16)  # column-major k x n, ld = ldb
+        sd = seed * 1000003 + i
+        srv.generate_omega(Om, ldb, k, n, srv.RADEMACHER_BLOCKS, sd, 1.0)
         Y = torch.zeros(n, m, device=dev)
         A = Afull.reshape(-1)
         B = Om.reshape(-1)
         C = Y.reshape(-1)
         keep.append((A, B, C))
-        probs.append((m, n, k, A, lda, B, ldb, C, m, 1.0, 0.0))
+        probs.append((m, n, k, A, lda, B, ldb, C, m, float(n) ** -0.5, 0.0))
         shapes.append((m, n, k))
-    return probs, shapes, keep
+        seeds.append(sd)
+    return probs, shapes, keep, seeds
 
 
 def grouped_case(args, wl, ctx, steps=None):
@@ -543,19 +566,24 @@ def grouped_case(args, wl, ctx, steps=None):
 
     import shgemm_b200 as sg
     from shgemm_b200 import evaluation as ev
+    from shgemm_b200 import server as srv
 
     steps = steps or args.steps
     dev = ctx.dev
     h = sg.Handle(ctx.local)
     stream = torch.cuda.Stream(dev)
     h.set_stream(stream)
-    probs, shapes, keep = make_grouped_batch(wl["count"], dev, seed=ctx.rank)
+    probs, shapes, keep, seeds = make_grouped_batch(wl["count"], dev, seed=ctx.rank)
     torch.cuda.synchronize(dev)
     flops = sum(2.0 * m * n * k for (m, n, k) in shapes)
-    b_bytes = 4.0 if wl.get("b_fp32") else 2.0
+    b_bytes = 0.0 if wl.get("fused") else (4.0 if wl.get("b_fp32") else 2.0)
     bytes_min = sum(4.0 * m * k + b_bytes * k * n + 4.0 * m * n for (m, n, k) in shapes)
     gprobs, keep_w = probs, []
-    if wl.get("b_fp32"):
+    if wl.get("fused"):
+        # Omega_i generated by the grouped kernel's B producer from its seed: not read at all
+        gprobs = [(m, n, k, A, lda, None, 0, C, ldc, al, be, srv.RADEMACHER_BLOCKS, sd)
+                  for (m, n, k, A, lda, B, ldb, C, ldc, al, be), sd in zip(probs, seeds)]
+    elif wl.get("b_fp32"):
         # Omega_i widened to FP32 once (exact: binary16 values), K-major with a 16-byte ld
         gprobs = []
         for (m, n, k, A, lda, B, ldb, C, ldc, al, be) in probs:
@@ -628,11 +656,11 @@ def grouped_case(args, wl, ctx, steps=None):
             for i in range(0, len(probs), max(1, len(probs) // 16)):
                 m, n, k, A, lda, B, ldb, C, ldc, al, be = probs[i]
                 c64 = ev.fp64_product(h, 0, 0, m, n, k, A, lda, B, ldb)
-                e_sh = ev.error(h, m, n, C, ldc, c64)["rel_fro"]
+                e_sh = ev.error(h, m, n, C, ldc, c64, al)["rel_fro"]
                 Bf = B.view(n, ldb)[:, :k].float()
                 Af = A.view(k, lda)[:, :m].T
-                S = (Af @ Bf.T).T.contiguous().reshape(-1)  # n x m row-major == m x n column-major
-                errs.append((e_sh, ev.error(h, m, n, S, m, c64)["rel_fro"]))
+                S = (Af @ Bf.T).mul_(al).T.contiguous().reshape(-1)  # n x m row-major == m x n column-major
+                errs.append((e_sh, ev.error(h, m, n, S, m, c64, al)["rel_fro"]))
         torch.cuda.synchronize(dev)
     del graph
     h.close()
@@ -1225,6 +1253,10 @@ def main():
             gw = WORKLOADS["grouped"]
             g = grouped_case(args, gw, ctx)
             nested["grouped"] = g
+            gf = grouped_case(args, WORKLOADS["grouped_fused"], ctx)
+            nested["grouped_fused_omega"] = {key: gf[key] for key in (
+                "value", "unit", "ms_per_step", "workload", "algorithmic_bytes", "per_call_baseline",
+                "speedup_vs_per_call", "roofline", "error", "autotuned_tile_n")}
             sw = WORKLOADS["square16k"]
             sq = square_case(args, sw, ctx, "square16k", tf32_error=True)
             nested["square16k"] = nested_square(sw, sq)

@@ -219,6 +219,13 @@ typedef struct shgemm_b200_problem {
     float* c;
     size_t ldc;
     float alpha, beta;
+    /* 0: B is given (b, ldb). SHGEMM_OMEGA_RADEMACHER_BLOCKS (binary16 compute only): B is the
+     * k x n block-sign operand of omega_seed with entries +1 / -1, generated by the kernel
+     * as it goes instead of loaded (b and ldb unused): no Omega in memory and no Omega
+     * traffic. The values are those shgemm_b200_generate_omega writes for the same seed with
+     * scale 1; scale the sketch through alpha. */
+    int b_generated;
+    unsigned long long omega_seed;
 } shgemm_b200_problem;
 
 /* Enqueues (on the handle's stream) the copy of the batch's tables from the
@@ -338,8 +345,11 @@ int shgemm_b200_noalloc_check_error(void* cuda_stream, int* device_code);
  * (whose sketches are host loops of shgemm calls).
  * ------------------------------------------------------------------------ */
 
-/* Distribution of a generated sketch operand Omega. */
-enum { SHGEMM_OMEGA_GAUSSIAN = 0, SHGEMM_OMEGA_RADEMACHER = 1 };
+/* Distribution of a generated sketch operand Omega. RADEMACHER_BLOCKS: random signs from one
+ * 64-bit hash per 64 consecutive entries of a column (entry (r, c) is negative when bit
+ * r mod 64 of splitmix64(seed * 0x9E3779B97F4A7C15 + c * ceil(k / 64) + r / 64 + 1) is set),
+ * the stream grouped launches can generate in the kernel instead of loading Omega. */
+enum { SHGEMM_OMEGA_GAUSSIAN = 0, SHGEMM_OMEGA_RADEMACHER = 1, SHGEMM_OMEGA_RADEMACHER_BLOCKS = 2 };
 
 /* Writes Omega (k x cols, column-major, leading dimension ld elements) on `cuda_stream`:
  * entry (r, c) = scale * g(seed, c * k + r) rounded to binary16, g standard normal

@@ -42,7 +42,8 @@ class Problem(ctypes.Structure):
 
     _fields_ = [("m", ctypes.c_size_t), ("n", ctypes.c_size_t), ("k", ctypes.c_size_t), ("a", ctypes.c_void_p),
                 ("lda", ctypes.c_size_t), ("b", ctypes.c_void_p), ("ldb", ctypes.c_size_t), ("c", ctypes.c_void_p),
-                ("ldc", ctypes.c_size_t), ("alpha", ctypes.c_float), ("beta", ctypes.c_float)]
+                ("ldc", ctypes.c_size_t), ("alpha", ctypes.c_float), ("beta", ctypes.c_float),
+                ("b_generated", ctypes.c_int), ("omega_seed", ctypes.c_ulonglong)]
 
 
 class TunedConfig(ctypes.Structure):
@@ -429,7 +430,10 @@ def _problem_array(problems):
         m, n, k, a, lda, b, ldb, c, ldc = q[:9]
         alpha = q[9] if len(q) > 9 else 1.0
         beta = q[10] if len(q) > 10 else 0.0
-        arr[i] = Problem(m, n, k, _addr(a), lda, _addr(b), ldb, _addr(c), ldc, alpha, beta)
+        gen = q[11] if len(q) > 11 else 0  # RADEMACHER_BLOCKS: B generated in the kernel from q[12]
+        seed = q[12] if len(q) > 12 else 0
+        arr[i] = Problem(m, n, k, _addr(a), lda, _addr(b), ldb, _addr(c), ldc, alpha, beta, gen,
+                         seed & 0xFFFFFFFFFFFFFFFF)
     return arr
 
 

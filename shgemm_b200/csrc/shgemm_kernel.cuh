@@ -166,7 +166,9 @@ struct alignas(64) GroupedProblem {
     int bn;     // tile N of this problem (<= the kernel's BN; 16-multiple)
     int steps;  // k-steps
     float alpha, beta;
-    int pad[3];
+    int b_gen;          // 1: B is the block-sign Rademacher operand of gen_seed (entries +-1), generated
+    int pad0;           //    by the B producer instead of loaded (binary16 compute); tmap_b unused
+    uint64_t gen_seed;
 };
 static_assert(sizeof(GroupedProblem) % 64 == 0, "GroupedProblem alignment");
 
@@ -190,12 +192,14 @@ struct UnitDesc {
     float* c;
     uint64_t ldc;
     float* partial;  // split-K: this slice's partial buffer [n][m]; null: write C
-    int m, n;
+    int m, n, k;
     int tm, tn;
     int s0, s1;  // k-step range
     int bn;      // tile N
     float alpha, beta;
     bool maps_in_global;  // descriptors written by a copy before the launch
+    bool b_gen;           // B generated by the producer (block-sign Rademacher, gen_seed)
+    uint64_t gen_seed;
 };
 
 // Device-resident alpha and beta of a launch, read once per epilogue warp; `on` false when
@@ -226,6 +230,9 @@ __device__ __forceinline__ void get_unit(const TileGemmParams& p, int u, UnitDes
     d.partial = p.num_slices > 1 ? p.workspace + static_cast<size_t>(slice) * p.n * p.m : nullptr;
     d.m = p.m;
     d.n = p.n;
+    d.k = p.k;
+    d.b_gen = false;
+    d.gen_seed = 0;
     d.tm = tm;
     d.tn = tn;
     d.s0 = s0;
@@ -247,6 +254,9 @@ __device__ __forceinline__ void get_unit(const GroupedParams& p, int u, UnitDesc
     d.partial = nullptr;
     d.m = q.m;
     d.n = q.n;
+    d.k = q.k;
+    d.b_gen = q.b_gen != 0;
+    d.gen_seed = q.gen_seed;
     d.tm = e.y & 0xFFFF;
     d.tn = e.y >> 16;
     d.s0 = 0;
@@ -266,6 +276,21 @@ __device__ __forceinline__ void prefetch_params_maps(const TileGemmParams& p) {
     ptx::tma_prefetch_desc(&p.tmap_b);
 }
 __device__ __forceinline__ void prefetch_params_maps(const GroupedParams&) {}
+
+// ---------------------------------------------------------------------------
+// Counter hash for generated sketch operands: splitmix64's finaliser (Steele, Lea and Flood,
+// "Fast splittable pseudorandom number generators", OOPSLA 2014).
+__device__ __forceinline__ uint64_t mix64(uint64_t z) {
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+
+// 64 sign bits of a block-sign Rademacher operand: entries r = 64 b .. 64 b + 63 of column c of
+// a k x n operand, block index c * ceil(k / 64) + b; bit j set means entry 64 b + j is negative.
+__device__ __forceinline__ uint64_t rademacher_block_bits(uint64_t seed, uint64_t block) {
+    return mix64(seed * 0x9E3779B97F4A7C15ull + block + 1);
+}
 
 // ---------------------------------------------------------------------------
 // Epilogue helpers.
@@ -593,9 +618,58 @@ __device__ __forceinline__ bool split_step_tf32(uint8_t* a_st, uint8_t* b_st, in
     return true;
 }
 
-template <int TC, int BN, bool A_KMAJOR, bool B_KMAJOR, bool B_WIDE, class Params>
+// Four binary16 values +1 / -1 (0x3C00 / 0xBC00) for the sign bits of a nibble, lowest bit first.
+__device__ __forceinline__ uint2 rademacher_nibble(uint32_t nib) {
+    uint32_t h[4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) h[i] = ((nib >> i) & 1u) ? 0xBC00u : 0x3C00u;
+    return make_uint2(h[0] | (h[1] << 16), h[2] | (h[3] << 16));
+}
+
+// One k-step (64 k) of a generated B stage: rows j < bn (columns tn bn + j of the k x n
+// block-sign operand), each 64 binary16 values K-major in the 128-byte-swizzled layout the
+// TMA would have written (16-byte chunk q of row j at chunk q ^ (j & 7)). Entries past n or
+// past k are zero, as the TMA's out-of-range fill. Lane l writes rows l, l + 32, ...
+__device__ __forceinline__ void gen_b_stage(uint8_t* stage, const UnitDesc& ud, int st, int lane, const uint2* lut) {
+    const int c0 = ud.tn * ud.bn;
+    const int kvalid = ud.k - st * 64;  // >= 1 on every step of the range
+    const uint64_t kblocks = static_cast<uint64_t>((ud.k + 63) / 64);
+    const uint64_t vmask = kvalid >= 64 ? ~0ull : ((1ull << kvalid) - 1ull);
+    for (int j = lane; j < ud.bn; j += 32) {
+        const int c = c0 + j;
+        uint8_t* row = stage + j * 128;
+        if (c >= ud.n) {
+#pragma unroll
+            for (int q = 0; q < 8; ++q) *reinterpret_cast<uint4*>(row + ((q ^ (j & 7)) << 4)) = make_uint4(0, 0, 0, 0);
+            continue;
+        }
+        const uint64_t bits = rademacher_block_bits(ud.gen_seed, static_cast<uint64_t>(c) * kblocks + st);
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+            const uint32_t b8 = static_cast<uint32_t>(bits >> (8 * q)) & 0xFFu;
+            const uint32_t v8 = static_cast<uint32_t>(vmask >> (8 * q)) & 0xFFu;
+            uint4 w;
+            if (v8 == 0xFFu) {
+                const uint2 lo = lut[b8 & 15u], hi = lut[b8 >> 4];
+                w = make_uint4(lo.x, lo.y, hi.x, hi.y);
+            } else {  // the last k-step's ragged edge
+                uint32_t h[8];
+#pragma unroll
+                for (int e = 0; e < 8; ++e)
+                    h[e] = ((v8 >> e) & 1u) ? (((b8 >> e) & 1u) ? 0xBC00u : 0x3C00u) : 0u;
+                w = make_uint4(h[0] | (h[1] << 16), h[2] | (h[3] << 16), h[4] | (h[5] << 16), h[6] | (h[7] << 16));
+            }
+            *reinterpret_cast<uint4*>(row + ((q ^ (j & 7)) << 4)) = w;
+        }
+    }
+}
+
+// GEN_B (grouped binary16 launches with a K-major B): problems may ask for their B to be
+// generated by the producer warp (block-sign Rademacher) instead of loaded.
+template <int TC, int BN, bool A_KMAJOR, bool B_KMAJOR, bool B_WIDE, bool GEN_B, class Params>
 __device__ __forceinline__ void tile_kernel_body(const Params& p) {
     using Cfg = TileCfg<TC, BN, A_KMAJOR, B_KMAJOR, B_WIDE>;
+    static_assert(!GEN_B || (TC == kFP16 && B_KMAJOR), "generated B: binary16 compute, K-major B");
     constexpr int SA = Cfg::SA;
     constexpr int SB = Cfg::SB;
     constexpr bool kTf32 = Cfg::kTf32;
@@ -619,10 +693,14 @@ __device__ __forceinline__ void tile_kernel_body(const Params& p) {
     uint64_t* drain_bar = d_empty + 2;
     uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(drain_bar + 1);
     volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
+    // the block-sign generator's nibble table (16 x 4 binary16 values), past the barriers
+    uint2* gen_lut = reinterpret_cast<uint2*>(reinterpret_cast<uint8_t*>(bars) + 512);
+    static_assert((4 * SA + 2 * SB + 5) * 8 + 8 <= 512 && 512 + 16 * 8 <= Cfg::BAR_BYTES, "barrier region");
 
     const int warp = threadIdx.x >> 5;
     const int lane = threadIdx.x & 31;
 
+    if (GEN_B && threadIdx.x < 16) gen_lut[threadIdx.x] = rademacher_nibble(threadIdx.x);
     if (threadIdx.x == 0) {
         for (int s = 0; s < SA; ++s) {
             ptx::mbar_init(&a_full[s], 1);
@@ -664,7 +742,9 @@ __device__ __forceinline__ void tile_kernel_body(const Params& p) {
     ptx::setmaxnreg_dec<Cfg::SPLIT_REGS>();
     if (warp == 0) {
         // ------------------------------------------------------------ TMA producer
-        if (lane == 0) {
+        // Lane 0 issues every TMA load. With GEN_B, the whole warp runs the loop and writes
+        // the B stages of problems whose B is generated (block-sign Rademacher) itself.
+        if (GEN_B || lane == 0) {
             int as = 0, bs = 0;
             uint32_t aph = 0, bph = 0;
             uint32_t a_issued = 0, a_par = 0, b_issued = 0, b_par = 0;  // per stage: load in flight, its parity
@@ -672,49 +752,63 @@ __device__ __forceinline__ void tile_kernel_body(const Params& p) {
                 UnitDesc ud;
                 get_unit<Cfg>(p, u, ud);
                 const int tm = ud.tm, tn = ud.tn, s0 = ud.s0, s1 = ud.s1;
-                if (ud.maps_in_global) {
+                if (lane == 0 && ud.maps_in_global) {
                     ptx::fence_tensormap_acquire(ud.tmap_a);
-                    ptx::fence_tensormap_acquire(ud.tmap_b);
+                    if (!ud.b_gen) ptx::fence_tensormap_acquire(ud.tmap_b);
                 }
                 for (int st = s0; st < s1; ++st) {
                     const int kc = st * Cfg::BK;
-                    if (!ptx::mbar_wait(&a_empty[as], aph ^ 1u, abort_flag, limit)) {
-                        fail(kErrProducerTimeout);
-                        goto producer_done;
-                    }
-                    {
-                        uint8_t* a_dst = a_base + as * Cfg::A_STAGE;
-                        ptx::mbar_arrive_expect_tx(&a_full[as], Cfg::A_RAW);
-                        if constexpr (A_KMAJOR) {
+                    int ok = 1;
+                    if (lane == 0) {
+                        ok = ptx::mbar_wait(&a_empty[as], aph ^ 1u, abort_flag, limit) ? 1 : 0;
+                        if (ok) {
+                            uint8_t* a_dst = a_base + as * Cfg::A_STAGE;
+                            ptx::mbar_arrive_expect_tx(&a_full[as], Cfg::A_RAW);
+                            if constexpr (A_KMAJOR) {
 #pragma unroll
-                            for (int sub = 0; sub < Cfg::BK / 32; ++sub)
-                                ptx::tma_load_2d(a_dst + sub * (Cfg::BM * 128), ud.tmap_a, &a_full[as],
-                                                 kc + 32 * sub, tm * Cfg::BM);
-                        } else if constexpr (!kTf32) {
+                                for (int sub = 0; sub < Cfg::BK / 32; ++sub)
+                                    ptx::tma_load_2d(a_dst + sub * (Cfg::BM * 128), ud.tmap_a, &a_full[as],
+                                                     kc + 32 * sub, tm * Cfg::BM);
+                            } else if constexpr (!kTf32) {
 #pragma unroll
-                            for (int h = 0; h < 2; ++h)
-                                ptx::tma_load_2d(a_dst + h * Cfg::MN_HALF_BYTES, ud.tmap_a, &a_full[as],
-                                                 tm * Cfg::BM + 64 * h, kc);
-                        } else if constexpr (B_WIDE) {
+                                for (int h = 0; h < 2; ++h)
+                                    ptx::tma_load_2d(a_dst + h * Cfg::MN_HALF_BYTES, ud.tmap_a, &a_full[as],
+                                                     tm * Cfg::BM + 64 * h, kc);
+                            } else if constexpr (B_WIDE) {
 #pragma unroll
-                            for (int b = 0; b < 4; ++b)
-                                ptx::tma_load_2d(a_dst + b * Cfg::MN_BOX_BYTES, ud.tmap_a, &a_full[as],
-                                                 tm * Cfg::BM + 32 * b, kc);
-                        } else {
-                            ptx::tma_load_2d(a_dst, ud.tmap_a, &a_full[as], tm * Cfg::BM, kc);
+                                for (int b = 0; b < 4; ++b)
+                                    ptx::tma_load_2d(a_dst + b * Cfg::MN_BOX_BYTES, ud.tmap_a, &a_full[as],
+                                                     tm * Cfg::BM + 32 * b, kc);
+                            } else {
+                                ptx::tma_load_2d(a_dst, ud.tmap_a, &a_full[as], tm * Cfg::BM, kc);
+                            }
+                            a_issued |= 1u << as;
+                            a_par = (a_par & ~(1u << as)) | (aph << as);
                         }
-                        a_issued |= 1u << as;
-                        a_par = (a_par & ~(1u << as)) | (aph << as);
+                    }
+                    if constexpr (GEN_B) ok = __shfl_sync(0xffffffffu, ok, 0);
+                    if (!ok) {
+                        if (lane == 0) fail(kErrProducerTimeout);
+                        goto producer_done;
                     }
                     if (++as == SA) {
                         as = 0;
                         aph ^= 1u;
                     }
-                    if (!ptx::mbar_wait(&b_empty[bs], bph ^ 1u, abort_flag, limit)) {
-                        fail(kErrProducerTimeout);
+                    if (lane == 0) ok = ptx::mbar_wait(&b_empty[bs], bph ^ 1u, abort_flag, limit) ? 1 : 0;
+                    if constexpr (GEN_B) ok = __shfl_sync(0xffffffffu, ok, 0);
+                    if (!ok) {
+                        if (lane == 0) fail(kErrProducerTimeout);
                         goto producer_done;
                     }
-                    {
+                    if (GEN_B && ud.b_gen) {
+                        // the block-sign operand written by the warp in the TMA's layout, then
+                        // published to the tensor core (async proxy) like the split warps' tiles
+                        gen_b_stage(b_base + bs * Cfg::B_STAGE, ud, st, lane, gen_lut);
+                        ptx::fence_proxy_async_smem();
+                        __syncwarp();
+                        if (lane == 0) ptx::mbar_arrive(&b_full[bs]);
+                    } else if (lane == 0) {
                         uint8_t* b_dst = b_base + bs * Cfg::B_STAGE;
                         ptx::mbar_arrive_expect_tx(&b_full[bs], ud.bn * Cfg::BK * (B_WIDE ? 4 : 2));
                         if constexpr (B_KMAJOR) {
@@ -738,17 +832,19 @@ __device__ __forceinline__ void tile_kernel_body(const Params& p) {
             }
         producer_done:
             // Never leave with bulk copies in flight into this CTA's shared memory.
-            for (int s = 0; s < SA + SB; ++s) {
-                const bool is_a = s < SA;
-                const int st = is_a ? s : s - SA;
-                if (!((is_a ? a_issued : b_issued) & (1u << st))) continue;
-                uint64_t* bar = is_a ? &a_full[st] : &b_full[st];
-                const uint32_t par = ((is_a ? a_par : b_par) >> st) & 1u;
-                const uint64_t t0 = ptx::globaltimer_ns();
-                while (!ptx::mbar_try_wait(bar, par)) {
-                    if (ptx::globaltimer_ns() - t0 > limit) {
-                        fail(kErrDrainTimeout);
-                        break;
+            if (lane == 0) {
+                for (int s = 0; s < SA + SB; ++s) {
+                    const bool is_a = s < SA;
+                    const int st = is_a ? s : s - SA;
+                    if (!((is_a ? a_issued : b_issued) & (1u << st))) continue;
+                    uint64_t* bar = is_a ? &a_full[st] : &b_full[st];
+                    const uint32_t par = ((is_a ? a_par : b_par) >> st) & 1u;
+                    const uint64_t t0 = ptx::globaltimer_ns();
+                    while (!ptx::mbar_try_wait(bar, par)) {
+                        if (ptx::globaltimer_ns() - t0 > limit) {
+                            fail(kErrDrainTimeout);
+                            break;
+                        }
                     }
                 }
             }
@@ -1000,13 +1096,14 @@ __device__ __forceinline__ void tile_kernel_body(const Params& p) {
 // Single problem (optionally split-K): descriptors in the kernel's parameter space.
 template <int TC, int BN, bool A_KMAJOR, bool B_KMAJOR>
 __global__ void __launch_bounds__(512, 1) shgemm_tile_kernel(const __grid_constant__ TileGemmParams p) {
-    tile_kernel_body<TC, BN, A_KMAJOR, B_KMAJOR, false>(p);
+    tile_kernel_body<TC, BN, A_KMAJOR, B_KMAJOR, false, false>(p);
 }
 
 // Many problems in one launch: per-problem descriptors and a unit list in device memory.
+// Binary16 launches can generate a problem's B (block-sign Rademacher) in the producer.
 template <int TC, int BN, bool A_KMAJOR, bool B_KMAJOR, bool B_WIDE>
 __global__ void __launch_bounds__(512, 1) shgemm_grouped_kernel(const __grid_constant__ GroupedParams p) {
-    tile_kernel_body<TC, BN, A_KMAJOR, B_KMAJOR, B_WIDE>(p);
+    tile_kernel_body<TC, BN, A_KMAJOR, B_KMAJOR, B_WIDE, TC == kFP16 && B_KMAJOR>(p);
 }
 
 }  // namespace shgemm_b200

@@ -321,23 +321,30 @@ __global__ void splitk_reduce_kernel(const float* __restrict__ ws, int slices, i
 }
 
 // Sketch operand generator: entry (r, c) of a k x cols column-major Omega from a
-// counter hash of (seed, c * k + r) -- splitmix64's finaliser (Steele, Lea and Flood,
-// "Fast splittable pseudorandom number generators", 2014) -- then Box-Muller for a
-// standard normal or the top bit for a sign; scaled and rounded to binary16.
-__device__ __forceinline__ uint64_t mix64(uint64_t z) {
-    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
-    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
-    return z ^ (z >> 31);
-}
-
+// counter hash of (seed, c * k + r) -- splitmix64's finaliser (mix64) -- then Box-Muller
+// for a standard normal or the top bit for a sign; scaled and rounded to binary16. The
+// block-sign stream (SHGEMM_OMEGA_RADEMACHER_BLOCKS) hashes (seed, c * ceil(k / 64) + r / 64)
+// once per 64 entries of a column and takes bit r mod 64: the stream the grouped kernel
+// generates in its B producer (rademacher_block_bits).
 __global__ void omega_kernel(void* dst, uint64_t ld, uint64_t k, uint64_t cols, int dist, uint64_t seed, float scale,
                              int fp32) {
     const uint64_t total = k * cols;
+    const uint64_t kblocks = (k + 63) / 64;
     for (uint64_t idx = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; idx < total;
          idx += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
         const uint64_t c = idx / k, r = idx - c * k;
-        const uint64_t x = mix64(seed * 0x9E3779B97F4A7C15ull + idx + 1);
         float v;
+        if (dist == SHGEMM_OMEGA_RADEMACHER_BLOCKS) {
+            const uint64_t bits = rademacher_block_bits(seed, c * kblocks + r / 64);
+            v = ((bits >> (r % 64)) & 1) ? -scale : scale;
+            const __half hv = __float2half_rn(v);
+            if (fp32)
+                static_cast<float*>(dst)[r + c * ld] = __half2float(hv);
+            else
+                static_cast<__half*>(dst)[r + c * ld] = hv;
+            continue;
+        }
+        const uint64_t x = mix64(seed * 0x9E3779B97F4A7C15ull + idx + 1);
         if (dist == SHGEMM_OMEGA_RADEMACHER) {
             v = (x >> 63) ? -scale : scale;
         } else {
@@ -834,7 +841,8 @@ int shgemm_b200_get_launch_count(shgemm_b200_handle_t h, long long* count) {
 
 int shgemm_b200_generate_omega(void* cuda_stream, void* dst, size_t ld, size_t k, size_t cols, int dist,
                                unsigned long long seed, float scale, int fp32) {
-    if ((dist != SHGEMM_OMEGA_GAUSSIAN && dist != SHGEMM_OMEGA_RADEMACHER) || (fp32 != 0 && fp32 != 1) || ld < k)
+    if ((dist != SHGEMM_OMEGA_GAUSSIAN && dist != SHGEMM_OMEGA_RADEMACHER && dist != SHGEMM_OMEGA_RADEMACHER_BLOCKS) ||
+        (fp32 != 0 && fp32 != 1) || ld < k)
         return SHGEMM_STATUS_INVALID_VALUE;
     if (k == 0 || cols == 0) return SHGEMM_STATUS_OK;
     if (!dst) return SHGEMM_STATUS_INVALID_VALUE;
@@ -1868,17 +1876,24 @@ int grouped_stage(shgemm_b200_handle_t h, GroupedTable& t, bool b_wide, int op_a
         const int bn = tiles.get(q.n);
         const long long tiles_n = static_cast<long long>((q.n + bn - 1) / bn);
         if (tiles_n > 0x7FFF) return SHGEMM_STATUS_NOT_SUPPORTED;
+        if (q.b_generated != 0 && q.b_generated != SHGEMM_OMEGA_RADEMACHER_BLOCKS) return SHGEMM_STATUS_INVALID_VALUE;
+        const bool gen = q.b_generated != 0;
+        if (gen && tc != kFP16) return SHGEMM_STATUS_NOT_SUPPORTED;  // generated B: binary16 compute only
         if (q.k > 0) {
-            if (!q.a || !q.b || q.lda < std::max<size_t>(1, a_rows) || q.ldb < std::max<size_t>(1, b_rows))
+            if (!q.a || (!gen && !q.b) || q.lda < std::max<size_t>(1, a_rows) ||
+                (!gen && q.ldb < std::max<size_t>(1, b_rows)))
                 return SHGEMM_STATUS_INVALID_VALUE;
-            if ((reinterpret_cast<uintptr_t>(q.a) & 15) || (reinterpret_cast<uintptr_t>(q.b) & 15) ||
-                (q.lda * 4) % 16 || (q.ldb * b_elem) % 16)
+            if ((reinterpret_cast<uintptr_t>(q.a) & 15) || (q.lda * 4) % 16 ||
+                (!gen && ((reinterpret_cast<uintptr_t>(q.b) & 15) || (q.ldb * b_elem) % 16)))
                 return SHGEMM_STATUS_NOT_SUPPORTED;  // grouped launches take TMA-addressable operands only
             bool ok = op_a == kOpT ? make_tmap(&g.tmap_a, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, q.a, q.k, q.m, q.lda * 4, 32,
                                                128, CU_TENSOR_MAP_SWIZZLE_128B)
                                    : make_tmap(&g.tmap_a, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, q.a, q.m, q.k, q.lda * 4,
                                                a_mmajor_box(tc, b_wide), bk, CU_TENSOR_MAP_SWIZZLE_NONE);
-            if (tc == kFP16)
+            if (gen) {
+                g.b_gen = 1;  // the producer writes B's stages itself: no tensor map
+                g.gen_seed = q.omega_seed;
+            } else if (tc == kFP16)
                 ok = ok && make_tmap(&g.tmap_b, CU_TENSOR_MAP_DATA_TYPE_FLOAT16, q.b, q.k, q.n, q.ldb * 2, 64, bn,
                                      CU_TENSOR_MAP_SWIZZLE_128B);
             else if (b_wide)  // [bn][32] FP32 rows of 128 bytes: the TF32 tile layout itself

@@ -12,7 +12,7 @@ import ctypes
 
 from . import ShgemmError, _addr, _check, _stream_addr, lib
 
-GAUSSIAN, RADEMACHER = 0, 1                                   # SHGEMM_OMEGA_*
+GAUSSIAN, RADEMACHER, RADEMACHER_BLOCKS = 0, 1, 2             # SHGEMM_OMEGA_*
 QUEUED, ADMITTED, RUNNING, DONE, FAILED, UNKNOWN = range(6)   # SHGEMM_REQ_*
 _SEED_STEP = 1099511628211                                    # draw j uses seed * _SEED_STEP + j
 

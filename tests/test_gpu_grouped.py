@@ -104,6 +104,63 @@ def test_grouped_tf32_widened_b_matches_oracle(h, op_a):
         K.assert_parity(K.parity_report(gpu_c, orc, ref, sgc, m, n, inp["ldc"], 0))
 
 
+@pytest.mark.parametrize("op_a", [0, 1])
+def test_generated_b_matches_materialised_b(h, op_a):
+    """Problems whose B is the block-sign Rademacher operand generated by the kernel's B
+    producer give C bit-identical to the same batch with that operand materialised by
+    shgemm_b200_generate_omega (scale 1) and loaded by TMA -- ragged n and k, k = 0, tiles
+    past n, mixed with ordinary problems -- and stay within the parity bar of the oracle."""
+    import torch
+
+    import shgemm_b200 as sg
+    from shgemm_b200 import server as srv
+
+    rng = np.random.default_rng(500 + op_a)
+    shapes = [(300, 64, 512), (129, 256, 1000), (640, 32, 320), (64, 100, 2049), (77, 17, 63), (200, 48, 0),
+              (1000, 250, 4096)]
+    inputs, dev, probs_gen, probs_mat, oms = [], [], [], [], []
+    for i, (m, n, k) in enumerate(shapes):
+        lda = ((m if op_a == 0 else k) + 4 + 3) // 4 * 4
+        ldb = (k + 8 + 7) // 8 * 8
+        inp = K.make_inputs_with_ld(rng, m, n, k, op_a, 0, 0, lda, ldb, m + 3)
+        A = torch.from_numpy(inp["A"]).cuda()
+        C1 = torch.from_numpy(inp["C"].copy()).cuda()
+        C2 = C1.clone()
+        seed = 1000 + i
+        Om = torch.zeros(n * ldb + 8, device="cuda", dtype=torch.float16)
+        if k > 0:
+            srv.generate_omega(Om, ldb, k, n, srv.RADEMACHER_BLOCKS, seed, 1.0)
+        alpha = float(n) ** -0.5
+        if i == 1:  # one ordinary problem in the mix: B given, loaded by TMA in both batches
+            Bg = torch.from_numpy(inp["B"].view(np.int16)).cuda().view(torch.float16)
+            probs_gen.append((m, n, k, A, lda, Bg, ldb, C1, m + 3, alpha, 0.5))
+            probs_mat.append((m, n, k, A, lda, Bg, ldb, C2, m + 3, alpha, 0.5))
+        else:
+            probs_gen.append((m, n, k, A, lda, None, 0, C1, m + 3, alpha, 0.5, srv.RADEMACHER_BLOCKS, seed))
+            probs_mat.append((m, n, k, A, lda, Om, ldb, C2, m + 3, alpha, 0.5))
+        inputs.append(inp)
+        dev.append((A, C1, C2))
+        oms.append((Om, ldb))
+    torch.cuda.synchronize()
+    sg.shgemm_grouped(h, probs_gen, sg.fp16, op_a=op_a)
+    sg.shgemm_grouped(h, probs_mat, sg.fp16, op_a=op_a)
+    torch.cuda.synchronize()
+    assert h.check_error() == 0
+    for i, ((m, n, k), inp, (A, C1, C2), (Om, ldb)) in enumerate(zip(shapes, inputs, dev, oms)):
+        assert torch.equal(C1.view(torch.int32), C2.view(torch.int32)), (i, m, n, k)
+        if i == 1 or k == 0:
+            continue
+        om_np = Om[:n * ldb].view(torch.int16).cpu().numpy().view(np.float16)
+        vals = np.unique(om_np.reshape(n, ldb)[:, :k].astype(np.float32))
+        assert set(vals.tolist()) <= {-1.0, 1.0}
+        ref_inp = dict(inp, B=om_np, ldb=ldb)
+        alpha = float(n) ** -0.5
+        orc = K.run_oracle(oracle.FP16, op_a, 0, m, n, k, alpha, ref_inp, 0.5, 0, chunk=0)
+        ref = K.fp64(op_a, 0, m, n, k, alpha, ref_inp, 0.5, 0)
+        sgc = K.sgemm(op_a, 0, m, n, k, alpha, ref_inp, 0.5, 0)
+        K.assert_parity(K.parity_report(C1.cpu().numpy(), orc, ref, sgc, m, n, m + 3, 0))
+
+
 def test_grouped_result_same_alone_and_in_the_mix(h):
     """A problem's result does not depend on the batch it runs in (bit for bit)."""
     import torch
@@ -240,3 +297,34 @@ def test_grouped_rejects_unsupported(h):
     with pytest.raises(sg.ShgemmError) as ei:  # lda not 16-byte aligned
         sg.shgemm_grouped(h, [(61, 64, 64, A, 61, B, 64, C, 64)], sg.fp16)
     assert ei.value.status == 2
+
+
+def _mix64(z):
+    """splitmix64's finaliser on numpy uint64 (wrapping arithmetic)."""
+    z = np.asarray(z, dtype=np.uint64)
+    with np.errstate(over="ignore"):
+        z = (z ^ (z >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)
+        z = (z ^ (z >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
+    return z ^ (z >> np.uint64(31))
+
+
+def test_block_sign_stream_is_the_documented_one(cuda_device):
+    """shgemm_b200_generate_omega(RADEMACHER_BLOCKS): entry (r, c) negative exactly when bit
+    r mod 64 of splitmix64(seed * 0x9E3779B97F4A7C15 + c * ceil(k / 64) + r / 64 + 1) is set."""
+    import torch
+
+    from shgemm_b200 import server as srv
+
+    k, n, seed, ld = 200, 5, 77, 208
+    Om = torch.zeros(n * ld, device="cuda", dtype=torch.float16)
+    srv.generate_omega(Om, ld, k, n, srv.RADEMACHER_BLOCKS, seed, 0.5)
+    got = Om.view(n, ld)[:, :k].float().cpu().numpy()
+    kb = (k + 63) // 64
+    with np.errstate(over="ignore"):
+        base = np.uint64(seed) * np.uint64(0x9E3779B97F4A7C15)
+    for c in range(n):
+        for r in range(k):
+            with np.errstate(over="ignore"):
+                x = _mix64(base + np.uint64(c * kb + r // 64 + 1))
+            neg = (int(x) >> (r % 64)) & 1
+            assert got[c, r] == (-0.5 if neg else 0.5), (c, r)
