@@ -372,6 +372,7 @@ def square_case(args, wl, ctx, traffic_key, tf32_error=False, e2e=True):
     if args.group_m:
         h.set_config(sg.CFG_GROUP_M, args.group_m)
     h.set_config(sg.CFG_TM_STAGES, args.stages)
+    h.set_config(sg.CFG_PAIR_TILES, args.pair)
     if (wl["tc"] == 1 or tf32_error) and wl["op_b"] == 0:
         # room for the widened FP32 copy of B (the TF32 route that loads B unconverted)
         h.set_workspace_size(max(64 << 20, n * ((k + 3) // 4 * 4) * 4 + (1 << 20)))
@@ -1233,6 +1234,8 @@ def main():
                     help="plain workloads: tile rasterisation group along m (with --no-autotune)")
     ap.add_argument("--stages", type=int, default=0, choices=[0, 1],
                     help="tensor-memory kernel operand ring (SHGEMM_CFG_TM_STAGES, with --no-autotune)")
+    ap.add_argument("--pair", type=int, default=0, choices=[0, 1],
+                    help="tensor-memory kernel in CTA pairs (SHGEMM_CFG_PAIR_TILES, with --no-autotune)")
     ap.add_argument("--rate", type=float, default=None, help="served: arrivals per second")
     ap.add_argument("--duration", type=float, default=None, help="served: seconds of arrivals")
     args = ap.parse_args()

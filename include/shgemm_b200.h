@@ -63,8 +63,11 @@ enum {
                                       the other kernels always drain every 64 */,
     SHGEMM_CFG_HOST_BLOCK_COLS = 9, /* columns of C per block of shgemm_b200_shgemm_host:
                                       0 (default) = a multiple of 256 giving about 16 blocks */
-    SHGEMM_CFG_TM_STAGES = 10      /* operand ring of the tensor-memory kernel when no tuned entry
+    SHGEMM_CFG_TM_STAGES = 10,     /* operand ring of the tensor-memory kernel when no tuned entry
                                       applies: 0 (default) = 4 FP32 A + 3 binary16 B stages, 1 = 3 + 4 */
+    SHGEMM_CFG_PAIR_TILES = 11     /* when no tuned entry applies: 1 = run the tensor-memory kernel in
+                                      CTA pairs (256 x 256 tiles over two SMs, tcgen05 cta_group::2,
+                                      half the B traffic per SM), 0 (default) = one CTA per tile */
 };
 
 /* ------------------------------------------------------------------------
@@ -85,6 +88,7 @@ typedef struct {
     float time_us;
     int stages;   /* tensor-memory kernel ring: 0 = 4 FP32 A + 3 binary16 B stages, 1 = 3 + 4 */
     int k_chunk;  /* tensor-memory kernel: k between FP32 drains, 64 or 128 */
+    int cta_group; /* tensor-memory kernel: 1 = one CTA per 128 x 256 tile, 2 = CTA pairs (256 x 256) */
 } shgemm_b200_tuned_config;
 
 /* Times every candidate configuration on the given operands (C is overwritten with

@@ -27,7 +27,7 @@ P0, P1 = 0, 1              # detail::kernel_level (include/shgemm/shgemm.hpp:30-
 
 CFG_SPLIT_K, CFG_WAIT_LIMIT_MS, CFG_GROUP_M, CFG_GROUPED_B_FP32, CFG_AUTOTUNE, CFG_TILE_KERNEL, CFG_K_CHUNK = (
     2, 3, 4, 5, 6, 7, 8)
-CFG_HOST_BLOCK_COLS, CFG_TM_STAGES = 9, 10
+CFG_HOST_BLOCK_COLS, CFG_TM_STAGES, CFG_PAIR_TILES = 9, 10, 11
 
 STATUS = {0: "OK", 1: "INVALID_VALUE", 2: "NOT_SUPPORTED", 3: "ALLOC_FAILED", 4: "LAUNCH_FAILED",
           5: "TIMEOUT", 6: "CUDA_ERROR", 7: "SCRATCH_TOO_SMALL"}
@@ -50,11 +50,12 @@ class TunedConfig(ctypes.Structure):
     """shgemm_b200_tuned_config: the autotuner's choice for a shape bucket (include/shgemm_b200.h)."""
 
     _fields_ = [("tile_n", ctypes.c_int), ("slices", ctypes.c_int), ("group_m", ctypes.c_int),
-                ("time_us", ctypes.c_float), ("stages", ctypes.c_int), ("k_chunk", ctypes.c_int)]
+                ("time_us", ctypes.c_float), ("stages", ctypes.c_int), ("k_chunk", ctypes.c_int),
+                ("cta_group", ctypes.c_int)]
 
     def as_dict(self) -> dict:
         return {"tile_n": self.tile_n, "slices": self.slices, "group_m": self.group_m, "time_us": self.time_us,
-                "stages": self.stages, "k_chunk": self.k_chunk}
+                "stages": self.stages, "k_chunk": self.k_chunk, "cta_group": self.cta_group}
 
 
 class ShgemmError(RuntimeError):

@@ -19,6 +19,7 @@
 #include "shgemm_b200.h"
 #include "shgemm_kernel.cuh"
 #include "shgemm_kernel_tm.cuh"
+#include "shgemm_kernel_tm2.cuh"
 
 using namespace shgemm_b200;
 
@@ -59,6 +60,7 @@ struct shgemm_b200_handle {
     int tile_kernel = 0;    // SHGEMM_CFG_TILE_KERNEL
     int k_chunk = 64;       // SHGEMM_CFG_K_CHUNK
     int tm_stages = 0;      // SHGEMM_CFG_TM_STAGES
+    int pair_tiles = 0;     // SHGEMM_CFG_PAIR_TILES
     std::mutex tune_mu;
     std::map<uint64_t, shgemm_b200_tuned_config> tuned;
     // host-buffer entry: device staging (A and three column-block slots of B and C), one
@@ -172,6 +174,12 @@ KernelEntry tm_entry() {
     return {reinterpret_cast<void*>(&shgemm_tm_kernel<AK, KC, SV>), TmCfg<AK, KC, SV>::SMEM_BYTES};
 }
 // kc: k-steps of 64 per FP32 drain (1 or 2); sv: operand ring variant (0 or 1)
+// The CTA-pair form (256 x 256 tiles over two SMs).
+KernelEntry tm2_kernel_table(bool ak) {
+    if (ak) return {reinterpret_cast<void*>(&shgemm_tm2_kernel<true>), Tm2Cfg<true>::SMEM_BYTES};
+    return {reinterpret_cast<void*>(&shgemm_tm2_kernel<false>), Tm2Cfg<false>::SMEM_BYTES};
+}
+
 KernelEntry tm_kernel_table(bool ak, int kc, int sv) {
     if (sv == 1) {
         if (kc == 2) return ak ? tm_entry<true, 2, 1>() : tm_entry<false, 2, 1>();
@@ -496,6 +504,7 @@ struct Plan {
     int steps_per_slice;
     int kc;  // tensor-memory kernel: k-steps of 64 per FP32 drain (0: the handle's SHGEMM_CFG_K_CHUNK)
     int sv;  // tensor-memory kernel: operand ring variant (-1: the handle's SHGEMM_CFG_TM_STAGES)
+    int pair;  // tensor-memory kernel in CTA pairs: 1 yes, 0 no (-1: the handle's SHGEMM_CFG_PAIR_TILES)
 };
 
 double wave_efficiency(long long units, int sms) {
@@ -549,6 +558,7 @@ Plan plan_from_tuned(const shgemm_b200_tuned_config& t, size_t m, size_t n, size
     p.slices = (p.total_steps + p.steps_per_slice - 1) / p.steps_per_slice;
     p.kc = t.k_chunk == 128 ? 2 : 0;  // a 64-k entry leaves the handle's SHGEMM_CFG_K_CHUNK in force
     p.sv = t.stages == 1 ? 1 : 0;
+    p.pair = t.cta_group == 2 ? 1 : (t.cta_group == 1 ? 0 : -1);
     return p;
 }
 
@@ -556,6 +566,7 @@ Plan make_plan_for(int num_sms, int fixed_level, long long split_k, size_t m, si
                    size_t ws_bytes) {
     Plan p{};
     p.sv = -1;
+    p.pair = -1;
     const int bk = (tc == kFP16) ? 64 : 32;
     p.total_steps = static_cast<int>((k + bk - 1) / bk);
     p.tiles_m = static_cast<int>((m + 127) / 128);
@@ -685,6 +696,10 @@ int shgemm_b200_create(shgemm_b200_handle_t* out, int device) {
                 KernelEntry e = tm_kernel_table(ak != 0, kc, sv);
                 cudaFuncSetAttribute(e.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, e.smem);
             }
+    for (int ak = 0; ak < 2; ++ak) {
+        KernelEntry e = tm2_kernel_table(ak != 0);
+        cudaFuncSetAttribute(e.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, e.smem);
+    }
     for (int tc = 0; tc < 2; ++tc)
         for (int ak = 0; ak < 2; ++ak)
             for (int bw = 0; bw < 2; ++bw) {
@@ -778,6 +793,10 @@ int shgemm_b200_set_config(shgemm_b200_handle_t h, int key, long long v) {
             if (v != 0 && v != 1) return SHGEMM_STATUS_INVALID_VALUE;
             h->tm_stages = static_cast<int>(v);
             return SHGEMM_STATUS_OK;
+        case SHGEMM_CFG_PAIR_TILES:
+            if (v != 0 && v != 1) return SHGEMM_STATUS_INVALID_VALUE;
+            h->pair_tiles = static_cast<int>(v);
+            return SHGEMM_STATUS_OK;
         default:
             return SHGEMM_STATUS_INVALID_VALUE;
     }
@@ -795,6 +814,7 @@ int shgemm_b200_get_config(shgemm_b200_handle_t h, int key, long long* v) {
         case SHGEMM_CFG_K_CHUNK: *v = h->k_chunk; return SHGEMM_STATUS_OK;
         case SHGEMM_CFG_HOST_BLOCK_COLS: *v = h->host_block_cols; return SHGEMM_STATUS_OK;
         case SHGEMM_CFG_TM_STAGES: *v = h->tm_stages; return SHGEMM_STATUS_OK;
+        case SHGEMM_CFG_PAIR_TILES: *v = h->pair_tiles; return SHGEMM_STATUS_OK;
         default: return SHGEMM_STATUS_INVALID_VALUE;
     }
 }
@@ -906,8 +926,14 @@ static int run_tiled(shgemm_b200_handle_t h, int op_a, int op_b, size_t m, size_
     if (force) group_m = force->group_m;
     float* part_ws = block_b ? splitk_ws + bblk_bytes / sizeof(float) : splitk_ws;
     __half* b_blk = reinterpret_cast<__half*>(splitk_ws);
-    // binary16 compute with 128 x 256 tiles and a K-major B: the tensor-memory operand kernel
+    // binary16 compute with 128 x 256 tiles and a K-major B: the tensor-memory operand kernel,
+    // in CTA pairs (256 x 256 tiles, SHGEMM_CFG_PAIR_TILES) when B is not re-laid out and the
+    // drain chunk and ring are the defaults
     const bool use_tm = tc == kFP16 && pl.bn == 256 && b_kmajor && h->tile_kernel == 0;
+    const int kc = pl.kc ? pl.kc : h->k_chunk / 64;
+    const int sv = pl.sv >= 0 ? pl.sv : h->tm_stages;
+    const int pair = pl.pair >= 0 ? pl.pair : h->pair_tiles;
+    const bool use_tm2 = use_tm && pair == 1 && !block_b && kc == 1 && sv == 0 && h->num_sms >= 2;
 
     TileGemmParams P;
     std::memset(&P, 0, sizeof(P));
@@ -918,7 +944,7 @@ static int run_tiled(shgemm_b200_handle_t h, int op_a, int op_b, size_t m, size_
     // The tensor-memory kernel loads a K-major tile as one 3-D box of whole 256-byte row
     // segments when k allows it (it streams at ~6.1 TB/s against ~4.4 TB/s for two
     // 128-byte-wide boxes over rows a full leading dimension apart).
-    if (a_kmajor && use_tm && k % 32 == 0 && make_tmap_a_paired(&P.tmap_a, a, k, m, lda * 4)) {
+    if (a_kmajor && use_tm && !use_tm2 && k % 32 == 0 && make_tmap_a_paired(&P.tmap_a, a, k, m, lda * 4)) {
         ok = true;
         P.a_rows_paired = 1;
     } else if (a_kmajor)
@@ -932,8 +958,8 @@ static int run_tiled(shgemm_b200_handle_t h, int op_a, int op_b, size_t m, size_
         if (block_b)  // k-blocks {64 k, n columns, kblocks}: one 64 x 256 tile step is 32 KB contiguous
             ok = make_tmap_3d(&P.tmap_b, CU_TENSOR_MAP_DATA_TYPE_FLOAT16, b_blk, 64, n, kblocks, 128, n * 128, 64,
                               pl.bn, 1, CU_TENSOR_MAP_SWIZZLE_128B);
-        else if (b_kmajor)
-            ok = make_tmap(&P.tmap_b, CU_TENSOR_MAP_DATA_TYPE_FLOAT16, b, k, n, ldb * 2, 64, pl.bn,
+        else if (b_kmajor)  // CTA pairs: each CTA loads 64 of every 128 columns
+            ok = make_tmap(&P.tmap_b, CU_TENSOR_MAP_DATA_TYPE_FLOAT16, b, k, n, ldb * 2, 64, use_tm2 ? 64 : pl.bn,
                            CU_TENSOR_MAP_SWIZZLE_128B);
         else
             ok = make_tmap(&P.tmap_b, CU_TENSOR_MAP_DATA_TYPE_FLOAT16, b, n, k, ldb * 2, 64, 64,
@@ -967,20 +993,26 @@ static int run_tiled(shgemm_b200_handle_t h, int op_a, int op_b, size_t m, size_
     P.steps_per_slice = pl.steps_per_slice;
     P.num_units = pl.tiles_m * pl.tiles_n * pl.slices;
     P.group_m = group_m;
-    P.a_read_once = use_tm && pl.tiles_n == 1;
+    P.a_read_once = use_tm && !use_tm2 && pl.tiles_n == 1;
     P.b_blocked = block_b ? 1 : 0;
+    if (use_tm2) {  // pair tiles of 256 rows
+        P.tiles_m = static_cast<int>((m + 255) / 256);
+        P.num_units = P.tiles_m * pl.tiles_n * pl.slices;
+    }
 
-    const int kc = pl.kc ? pl.kc : h->k_chunk / 64;
-    const int sv = pl.sv >= 0 ? pl.sv : h->tm_stages;
-    const KernelEntry e = use_tm ? tm_kernel_table(a_kmajor, kc, sv) : kernel_table(tc, pl.bn, a_kmajor, b_kmajor);
+    const KernelEntry e = use_tm2 ? tm2_kernel_table(a_kmajor)
+                          : use_tm ? tm_kernel_table(a_kmajor, kc, sv)
+                                   : kernel_table(tc, pl.bn, a_kmajor, b_kmajor);
     const int threads = use_tm ? TmCfg<true, 1, 0>::NUM_THREADS : 512;
     if (!e.fn) return SHGEMM_STATUS_NOT_SUPPORTED;
-    const int grid = std::min(P.num_units, h->num_sms);
+    // pairs: whole clusters of 2, one pair per two SMs
+    const int grid = use_tm2 ? 2 * std::min(P.num_units, h->num_sms / 2) : std::min(P.num_units, h->num_sms);
     if (h->debug_mode) {
         std::printf("[shape=(%zu,%zu,%zu),op_a=%s,op_b=%s,compute_type=%s] kernel_level = %d, tile = 128x%d, "
                     "k_slices = %d, chunk_k = %d, grid = %d%s\n",
                     m, n, k, op_a == kOpN ? "N" : "T", op_b == kOpN ? "N" : "T", tc == kTF32 ? "TF32" : "FP16",
-                    pl.level, pl.bn, pl.slices, use_tm ? 64 * kc : bk, grid, use_tm ? ", operands in TMEM" : "");
+                    pl.level, pl.bn, pl.slices, use_tm ? 64 * kc : bk, grid,
+                    use_tm2 ? ", operands in TMEM, CTA pairs" : use_tm ? ", operands in TMEM" : "");
     }
     if (block_b) {
         const size_t total = kblocks * n * 8;
@@ -1369,24 +1401,25 @@ int shgemm_b200_autotune(shgemm_b200_handle_t h, int op_a, int op_b, size_t m, s
     const int fit = static_cast<int>(std::min<size_t>(h->workspace_bytes / per_slice, 1024));
     const int tile_ns[] = {64, 128, 256};
     const int slice_set[] = {1, 2, 3, 4, 6, 8, 12, 16};
-    auto cfg_of = [](int bn, int sl, int gm, int sv, int kchunk) {
+    auto cfg_of = [](int bn, int sl, int gm, int sv, int kchunk, int cg = 1) {
         shgemm_b200_tuned_config c{};
         c.tile_n = bn;
         c.slices = sl;
         c.group_m = gm;
         c.stages = sv;
         c.k_chunk = kchunk;
+        c.cta_group = cg;
         return c;
     };
     auto same = [](const shgemm_b200_tuned_config& x, const shgemm_b200_tuned_config& y) {
         return x.tile_n == y.tile_n && x.slices == y.slices && x.group_m == y.group_m && x.stages == y.stages &&
-               x.k_chunk == y.k_chunk;
+               x.k_chunk == y.k_chunk && x.cta_group == y.cta_group;
     };
     // one timed run of the heuristic plan sizes the repetitions
     shgemm_b200_tuned_config best{};
     {
         const Plan hp = make_plan_for(h->num_sms, SHGEMM_LEVEL_AUTO, 0, m, n, k, tc, h->workspace_bytes);
-        best = cfg_of(hp.bn, hp.slices, static_cast<int>(h->group_m), h->tm_stages, 64);
+        best = cfg_of(hp.bn, hp.slices, static_cast<int>(h->group_m), h->tm_stages, 64, h->pair_tiles ? 2 : 1);
         const int st = time_config(h, op_a, op_b, m, n, k, a, lda, b, ldb, c, ldc, tc, best, 1, &best.time_us);
         if (st != SHGEMM_STATUS_OK) return st;
     }
@@ -1426,10 +1459,14 @@ int shgemm_b200_autotune(shgemm_b200_handle_t h, int op_a, int op_b, size_t m, s
     if (tm) {
         int st = consider(cfg_of(best.tile_n, best.slices, best.group_m, 1 - best.stages, 64));
         if (st != SHGEMM_STATUS_OK) return st;
-        shgemm_b200_tuned_config c128 = cfg_of(best.tile_n, best.slices, best.group_m, best.stages, 128);
-        st = time_config(h, op_a, op_b, m, n, k, a, lda, b, ldb, c, ldc, tc, c128, reps, &c128.time_us);
+        // CTA pairs (256 x 256 tiles over two SMs): the default ring and drain chunk only
+        st = consider(cfg_of(best.tile_n, best.slices, best.group_m, 0, 64, 2));
         if (st != SHGEMM_STATUS_OK) return st;
-        if (c128.time_us < best.time_us) {
+        shgemm_b200_tuned_config c128 = cfg_of(best.tile_n, best.slices, best.group_m, best.stages, 128);
+        if (best.cta_group != 2)
+            st = time_config(h, op_a, op_b, m, n, k, a, lda, b, ldb, c, ldc, tc, c128, reps, &c128.time_us);
+        if (st != SHGEMM_STATUS_OK) return st;
+        if (best.cta_group != 2 && c128.time_us < best.time_us) {
             bool pass = false;
             st = k_chunk_gate(h, op_a, op_b, m, n, k, a, lda, b, ldb, c, ldc, tc, best, c128, &pass, &gate_e64,
                               &gate_e128);
@@ -1444,9 +1481,9 @@ int shgemm_b200_autotune(shgemm_b200_handle_t h, int op_a, int op_b, size_t m, s
     }
     if (h->debug_mode) {
         std::printf("[autotune] (%zu,%zu,%zu) %s: tile = 128x%d, k_slices = %d, group_m = %d, stages = %d, "
-                    "k_chunk = %d, %.1f us\n",
+                    "k_chunk = %d, cta_group = %d, %.1f us\n",
                     m, n, k, tc == kTF32 ? "TF32" : "FP16", best.tile_n, best.slices, best.group_m, best.stages,
-                    best.k_chunk, best.time_us);
+                    best.k_chunk, best.cta_group, best.time_us);
         if (gate >= 0)
             std::printf("[autotune] k_chunk 128 accuracy gate %s: sampled error %.3e vs %.3e at 64\n",
                         gate ? "passed" : "failed", gate_e128, gate_e64);
@@ -1466,7 +1503,7 @@ int shgemm_b200_autotune_lookup(shgemm_b200_handle_t h, int op_a, int op_b, size
 }
 
 // Text format, one entry per line:
-//   kind tc op_a op_b log2m log2n log2k tile_n slices group_m stages k_chunk time_us
+//   kind tc op_a op_b log2m log2n log2k tile_n slices group_m stages k_chunk cta_group time_us
 // kind 0: a plain shape bucket; kind 1: a grouped n bucket (op_b holds the B format, 1 =
 // FP32; log2m and log2k are 0). Lines of the earlier 10-field form (no kind, stages and
 // k_chunk) load as plain entries with the default ring and a 64-k chunk.
@@ -1476,15 +1513,15 @@ int shgemm_b200_autotune_save(shgemm_b200_handle_t h, const char* path) {
     if (!f) return SHGEMM_STATUS_INVALID_VALUE;
     std::lock_guard<std::mutex> lk(h->tune_mu);
     std::fprintf(f, "# shgemm_b200 autotune v2: kind tc op_a op_b log2m log2n log2k tile_n slices group_m stages "
-                    "k_chunk time_us\n");
+                    "k_chunk cta_group time_us\n");
     for (const auto& kv : h->tuned) {
         const uint64_t key = kv.first;
         const shgemm_b200_tuned_config& t = kv.second;
-        std::fprintf(f, "%d %d %d %d %d %d %d %d %d %d %d %d %.3f\n", (key & kTuneGrouped) ? 1 : 0,
+        std::fprintf(f, "%d %d %d %d %d %d %d %d %d %d %d %d %d %.3f\n", (key & kTuneGrouped) ? 1 : 0,
                      static_cast<int>((key >> 27) & 1), static_cast<int>((key >> 26) & 1),
                      static_cast<int>((key >> 25) & 1), static_cast<int>((key >> 16) & 0xFF),
                      static_cast<int>((key >> 8) & 0xFF), static_cast<int>(key & 0xFF), t.tile_n, t.slices, t.group_m,
-                     t.stages, t.k_chunk, t.time_us);
+                     t.stages, t.k_chunk, t.cta_group, t.time_us);
     }
     const bool ok = std::fclose(f) == 0;
     return ok ? SHGEMM_STATUS_OK : SHGEMM_STATUS_INVALID_VALUE;
@@ -1499,14 +1536,15 @@ int shgemm_b200_autotune_load(shgemm_b200_handle_t h, const char* path) {
     std::map<uint64_t, shgemm_b200_tuned_config> add;
     while (std::fgets(line, sizeof(line), f)) {
         if (line[0] == '#' || line[0] == '\n') continue;
-        int kind = 0, tc, oa, ob, lm, ln, lk, bn, sl, gm, sv = 0, kch = 64;
+        int kind = 0, tc, oa, ob, lm, ln, lk, bn, sl, gm, sv = 0, kch = 64, cg = 1;
         float us;
-        const int got = std::sscanf(line, "%d %d %d %d %d %d %d %d %d %d %d %d %f", &kind, &tc, &oa, &ob, &lm, &ln,
-                                    &lk, &bn, &sl, &gm, &sv, &kch, &us);
-        if (got != 13) {  // the earlier form: tc op_a op_b log2m log2n log2k tile_n slices group_m time_us
+        const int got = std::sscanf(line, "%d %d %d %d %d %d %d %d %d %d %d %d %d %f", &kind, &tc, &oa, &ob, &lm, &ln,
+                                    &lk, &bn, &sl, &gm, &sv, &kch, &cg, &us);
+        if (got != 14) {  // the earlier form: tc op_a op_b log2m log2n log2k tile_n slices group_m time_us
             kind = 0;
             sv = 0;
             kch = 64;
+            cg = 1;
             if (std::sscanf(line, "%d %d %d %d %d %d %d %d %d %f", &tc, &oa, &ob, &lm, &ln, &lk, &bn, &sl, &gm, &us) !=
                 10) {
                 status = SHGEMM_STATUS_INVALID_VALUE;
@@ -1516,7 +1554,7 @@ int shgemm_b200_autotune_load(shgemm_b200_handle_t h, const char* path) {
         const bool bad_common = (kind != 0 && kind != 1) || (tc != kFP16 && tc != kTF32) || (oa != 0 && oa != 1) ||
                                 (ob != 0 && ob != 1) || lm < 0 || lm > 40 || ln < 0 || ln > 40 || lk < 0 || lk > 40;
         const bool bad_plain = kind == 0 && (!tile_n_valid(tc, bn) || sl < 1 || sl > 1024 || gm < 1 || gm > 1024 ||
-                                             (sv != 0 && sv != 1) || (kch != 64 && kch != 128));
+                                             (sv != 0 && sv != 1) || (kch != 64 && kch != 128) || (cg != 1 && cg != 2));
         const bool bad_grouped = kind == 1 && !(bn == 32 || bn == 64 || bn == 128 || bn == 256);
         if (bad_common || bad_plain || bad_grouped) {
             status = SHGEMM_STATUS_INVALID_VALUE;
@@ -1529,6 +1567,7 @@ int shgemm_b200_autotune_load(shgemm_b200_handle_t h, const char* path) {
         t.time_us = us;
         t.stages = kind ? 0 : sv;
         t.k_chunk = kind ? 64 : kch;
+        t.cta_group = kind ? 1 : cg;
         uint64_t key;
         if (kind == 1) {
             key = tune_key_grouped(tc, oa, ob, ln);
@@ -2058,6 +2097,7 @@ int shgemm_b200_autotune_grouped(shgemm_b200_handle_t h, int op_a, int op_b, int
         c.group_m = 1;
         c.time_us = us;
         c.k_chunk = 64;
+        c.cta_group = 1;
         h->tuned[tune_key_grouped(tc, op_a, b_wide ? 1 : 0, L)] = c;
     };
     const int saved_mode = h->autotune_mode;
@@ -2190,6 +2230,13 @@ int noalloc_setup(int dev, NoAllocDevice*& out) {
                         return SHGEMM_STATUS_NOT_SUPPORTED;
                     }
                 }
+        for (int ak = 0; ak < 2; ++ak) {
+            KernelEntry e = tm2_kernel_table(ak != 0);
+            if (cudaFuncSetAttribute(e.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, e.smem) != cudaSuccess) {
+                cudaGetLastError();
+                return SHGEMM_STATUS_NOT_SUPPORTED;
+            }
+        }
         d.num_sms = sms;
         const char* dbg = std::getenv("MTK_SHGEMM_DEBUG");
         d.debug_mode = (dbg && dbg[0] == '1') ? 1u : 0u;
