@@ -262,6 +262,8 @@ def nvml_energy(mon, calls, flops_per_call):
     except Exception:
         return None
     j = r["joules"] / calls
+    if not j > 0:  # the counter did not advance over a region this short
+        return None
     return {"avg_board_power_w": r["avg_w"], "joules_per_call": j, "effective_gflop_per_joule": flops_per_call / j / 1e9,
             "source": r["source"] + " over the timed region (whole board)", "samples": r["samples"]}
 
@@ -331,6 +333,7 @@ def gpu_error(h, wl, A, lda, B, ldb, C_out, ldc, C0, c64=None):
         C0m = C0.view(-1, ldc).T[:m, :n] if op_c == 0 else C0.view(-1, ldc)[:m, :n]
         S.add_(C0m, alpha=wl["beta"])
     Sbuf = S.T.contiguous().reshape(-1) if op_c == 0 else S.contiguous().reshape(-1)
+    torch.cuda.synchronize()  # Sbuf comes from torch's stream, the error kernel runs on the handle's
     es = ev.error(h, m, n, Sbuf, m if op_c == 0 else n, c64, wl["alpha"], wl["beta"],
                   C0 if wl["beta"] != 0 else None, op_c)
     # binary16 compute: an FP32 entry of magnitude >= 65520 rounds to inf in the hi part (as in
@@ -939,6 +942,7 @@ def served_case(args, wl, ctx):
                 Af = torch.as_strided(pools[n], (m, k), (1, lda), (a - pools[n].data_ptr()) // 4)
                 Bf = torch.as_strided(om, (k, n), (1, ldb), j * n * ldb).float()
                 S = (Af @ Bf).T.contiguous().reshape(-1)
+                torch.cuda.synchronize(dev)  # S comes from torch's stream, the error kernel runs on the handle's
                 errs.append((e_s, ev.error(h, m, n, S, m, c64)["rel_fro"]))
             chk.release(t)
         chk.close()

@@ -61,6 +61,7 @@ struct shgemm_b200_handle {
     int k_chunk = 64;       // SHGEMM_CFG_K_CHUNK
     int tm_stages = 0;      // SHGEMM_CFG_TM_STAGES
     int pair_tiles = 0;     // SHGEMM_CFG_PAIR_TILES
+    int max_pairs = 74;     // clusters of 2 of the pair kernel resident at once
     std::mutex tune_mu;
     std::map<uint64_t, shgemm_b200_tuned_config> tuned;
     // host-buffer entry: device staging (A and three column-block slots of B and C), one
@@ -178,6 +179,22 @@ KernelEntry tm_entry() {
 KernelEntry tm2_kernel_table(bool ak) {
     if (ak) return {reinterpret_cast<void*>(&shgemm_tm2_kernel<true>), Tm2Cfg<true>::SMEM_BYTES};
     return {reinterpret_cast<void*>(&shgemm_tm2_kernel<false>), Tm2Cfg<false>::SMEM_BYTES};
+}
+
+// Clusters of 2 of the pair kernel that can be resident at once: a GPC with an odd number of
+// free SMs leaves one out, so the persistent grid is sized by the occupancy query, not by SMs / 2
+// (a cluster beyond it would start only when another one finished, doubling the tail).
+int query_max_pairs(const KernelEntry& e, int num_sms) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(2 * (num_sms / 2));
+    cfg.blockDim = dim3(Tm2Cfg<true>::NUM_THREADS);
+    cfg.dynamicSmemBytes = e.smem;
+    int n = 0;
+    if (cudaOccupancyMaxActiveClusters(&n, e.fn, &cfg) != cudaSuccess || n <= 0) {
+        cudaGetLastError();
+        return num_sms / 2;
+    }
+    return std::min(n, num_sms / 2);
 }
 
 KernelEntry tm_kernel_table(bool ak, int kc, int sv) {
@@ -700,6 +717,7 @@ int shgemm_b200_create(shgemm_b200_handle_t* out, int device) {
         KernelEntry e = tm2_kernel_table(ak != 0);
         cudaFuncSetAttribute(e.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, e.smem);
     }
+    h->max_pairs = query_max_pairs(tm2_kernel_table(true), sms);
     for (int tc = 0; tc < 2; ++tc)
         for (int ak = 0; ak < 2; ++ak)
             for (int bw = 0; bw < 2; ++bw) {
@@ -1006,7 +1024,8 @@ static int run_tiled(shgemm_b200_handle_t h, int op_a, int op_b, size_t m, size_
     const int threads = use_tm ? TmCfg<true, 1, 0>::NUM_THREADS : 512;
     if (!e.fn) return SHGEMM_STATUS_NOT_SUPPORTED;
     // pairs: whole clusters of 2, one pair per two SMs
-    const int grid = use_tm2 ? 2 * std::min(P.num_units, h->num_sms / 2) : std::min(P.num_units, h->num_sms);
+    const int grid = use_tm2 ? 2 * std::min(P.num_units, std::min(h->max_pairs, h->num_sms / 2))
+                             : std::min(P.num_units, h->num_sms);
     if (h->debug_mode) {
         std::printf("[shape=(%zu,%zu,%zu),op_a=%s,op_b=%s,compute_type=%s] kernel_level = %d, tile = 128x%d, "
                     "k_slices = %d, chunk_k = %d, grid = %d%s\n",

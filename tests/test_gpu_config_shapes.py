@@ -2,7 +2,11 @@
 
 * Large square SHGEMM / HSGEMM, m = n = k = 16384, op_n and op_t, binary16 and TF32
   compute, alpha = 1, beta = 0.5 with C uniform[-1, 1]; FP32 operand N(0,1) 2^U(-15,15)
-  (the wide exponent range that exercises the lo term), binary16 operand N(0,1). The whole
+  (the wide exponent range that exercises the lo term), binary16 operand N(0,1). With
+  binary16 compute almost every row of that FP32 operand holds an entry >= 65520, whose hi
+  part overflows (the reference's behaviour, checked through the non-finite mask), so the
+  binary16 cases also run the reference's widest exponent-test range, +-2^U(-15,14)
+  (test/exponent_test.cu:202-250, random signs), where every entry stays finite. The whole
   product runs on the GPU; a 256 x 256 block of C (rows and columns off the tile grid) is
   recomputed by the oracle from the same rows of op(A) and columns of op(B) over the full
   k = 16384 -- each entry of C depends on nothing else.
@@ -40,8 +44,10 @@ def square_inputs(cuda_device):
     F.mul_(torch.exp2(torch.empty(N * N, device="cuda").uniform_(-15, 15, generator=g)))
     H = torch.randn(N * N, generator=g, device="cuda").to(torch.float16)
     Cin = torch.empty(N * N, device="cuda").uniform_(-1, 1, generator=g)
-    yield F, H, Cin
-    del F, H, Cin
+    X = torch.exp2(torch.empty(N * N, device="cuda").uniform_(-15, 14, generator=g))
+    X.mul_(torch.randn(N * N, generator=g, device="cuda").sign_())
+    yield {"wide": F, "exp14": X}, H, Cin
+    del F, H, Cin, X
     torch.cuda.empty_cache()
 
 
@@ -87,15 +93,17 @@ def _print(tag, r):
           f"e_ideal {r['e_ideal']:.3e}  e_sgemm {r['e_sgemm']:.3e}  gpu/tcmodel {hm:.3f}  gpu/sgemm {hs:.3f}")
 
 
-@pytest.mark.parametrize("tc", [oracle.FP16, oracle.TF32])
+@pytest.mark.parametrize("tc,dist", [(oracle.FP16, "wide"), (oracle.TF32, "wide"), (oracle.FP16, "exp14")],
+                         ids=["fp16", "tf32", "fp16-exp14"])
 @pytest.mark.parametrize("op", [0, 1])
 @pytest.mark.parametrize("hs", [False, True], ids=["shgemm", "hsgemm"])
-def test_square_16384_block(square_inputs, hbig, tc, op, hs):
+def test_square_16384_block(square_inputs, hbig, tc, dist, op, hs):
     import torch
 
     import shgemm_b200 as sg
 
-    F, H, Cin = square_inputs
+    Fs, H, Cin = square_inputs
+    F = Fs[dist]
     C = Cin.clone()
     alpha, beta = 1.0, 0.5
     if hs:  # A binary16 (m x k), B FP32 (k x n)
@@ -133,10 +141,10 @@ def test_square_16384_block(square_inputs, hbig, tc, op, hs):
         oracle.sgemm(0, 0, BLK, BLK, N, alpha, a_sub, BLK, b_sub, N, beta, sgc_buf, BLK, 0)
     sgc = oracle.logical_c(sgc_buf, BLK, BLK, BLK)
     r = _report(gpu_blk, tcm, ideal, ref, sgc)
-    _print(f"{'hsgemm' if hs else 'shgemm'} {'NT'[op]}{'NT'[op]} {['fp16', 'tf32'][tc]} 16384^3 block", r)
+    _print(f"{'hsgemm' if hs else 'shgemm'} {'NT'[op]}{'NT'[op]} {['fp16', 'tf32'][tc]} {dist} 16384^3 block", r)
     assert r["finite_mask_equal"], r
-    if tc == oracle.TF32:
-        assert r["finite_fraction"] == 1.0  # no overflow in TF32: the check covers every entry
+    if tc == oracle.TF32 or dist == "exp14":
+        assert r["finite_fraction"] == 1.0  # no overflow: the check covers every entry
     assert r["e_gpu"] <= 2.0 * r["e_oracle"] + K.ULP_FLOOR, r
     assert r["e_gpu"] <= 2.0 * r["e_sgemm"] + K.ULP_FLOOR, r
 
