@@ -350,9 +350,11 @@ int shgemm_b200_noalloc_check_error(void* cuda_stream, int* device_code);
  * ------------------------------------------------------------------------ */
 
 /* Distribution of a generated sketch operand Omega. RADEMACHER_BLOCKS: random signs from one
- * 64-bit hash per 64 consecutive entries of a column (entry (r, c) is negative when bit
- * r mod 64 of splitmix64(seed * 0x9E3779B97F4A7C15 + c * ceil(k / 64) + r / 64 + 1) is set),
- * the stream grouped launches can generate in the kernel instead of loading Omega. */
+ * 64-bit hash per 64 consecutive entries of a column: entry (r, c) is negative when bit
+ * b(r mod 64) of splitmix64(seed * 0x9E3779B97F4A7C15 + c * ceil(k / 64) + r / 64 + 1) is set,
+ * b(i) = 32 (i / 32) + (i / 2 mod 16) + 16 (i mod 2) -- adjacent entries take bits 16 apart,
+ * so a 32-bit word of two binary16 values is one shift and one mask. This is the stream
+ * grouped launches can generate in the kernel instead of loading Omega. */
 enum { SHGEMM_OMEGA_GAUSSIAN = 0, SHGEMM_OMEGA_RADEMACHER = 1, SHGEMM_OMEGA_RADEMACHER_BLOCKS = 2 };
 
 /* Writes Omega (k x cols, column-major, leading dimension ld elements) on `cuda_stream`:

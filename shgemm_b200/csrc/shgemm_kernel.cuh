@@ -127,7 +127,7 @@ struct TileCfg {
     static constexpr int HALF_N = BN / 2;                        // columns per epilogue warp
     // Per-thread registers after setmaxnreg: warpgroups 0-1 (producer, MMA, split) and
     // 2-3 (epilogue, which holds HALF_N running sums); 256 x (SPLIT_REGS + EPI_REGS) = 65536.
-    static constexpr int SPLIT_REGS = BN == 256 ? 72 : 112;
+    static constexpr int SPLIT_REGS = BN == 256 ? 80 : 112;
     static constexpr int EPI_REGS = 256 - SPLIT_REGS;
     static constexpr int BAR_BYTES = 1024;
     static constexpr int SMEM_BYTES = SA * A_STAGE + SB * B_STAGE + BAR_BYTES + 1024;
@@ -286,10 +286,18 @@ __device__ __forceinline__ uint64_t mix64(uint64_t z) {
     return z ^ (z >> 31);
 }
 
-// 64 sign bits of a block-sign Rademacher operand: entries r = 64 b .. 64 b + 63 of column c of
-// a k x n operand, block index c * ceil(k / 64) + b; bit j set means entry 64 b + j is negative.
+// 64 sign bits of a block-sign Rademacher operand: entries 64 b .. 64 b + 63 of column c of a
+// k x n operand, block index c * ceil(k / 64) + b; entry 64 b + r is negative when bit
+// block_sign_bit(r) is set.
 __device__ __forceinline__ uint64_t rademacher_block_bits(uint64_t seed, uint64_t block) {
     return mix64(seed * 0x9E3779B97F4A7C15ull + block + 1);
+}
+
+// The bit of a block's hash that gives the sign of entry r (0..63) of the block: entries 2p
+// and 2p + 1 take bits (p mod 16) and (p mod 16) + 16 of 32-bit half p / 16, so the two
+// binary16 values of a 32-bit word come from bits 16 apart (one shift and one mask a word).
+__host__ __device__ __forceinline__ int block_sign_bit(int r) {
+    return 32 * (r >> 5) + ((r >> 1) & 15) + 16 * (r & 1);
 }
 
 // ---------------------------------------------------------------------------
@@ -618,54 +626,54 @@ __device__ __forceinline__ bool split_step_tf32(uint8_t* a_st, uint8_t* b_st, in
     return true;
 }
 
-// Four binary16 values +1 / -1 (0x3C00 / 0xBC00) for the sign bits of a nibble, lowest bit first.
-__device__ __forceinline__ uint2 rademacher_nibble(uint32_t nib) {
-    uint32_t h[4];
-#pragma unroll
-    for (int i = 0; i < 4; ++i) h[i] = ((nib >> i) & 1u) ? 0xBC00u : 0x3C00u;
-    return make_uint2(h[0] | (h[1] << 16), h[2] | (h[3] << 16));
+// Two binary16 values +1 / -1 (0x3C00 / 0xBC00) as one 32-bit word: the sign of the low
+// half is bit i of h, the sign of the high half bit i + 16 (i < 16). One shift and one masked
+// OR per word: this pairing of bits 16 apart is why the block-sign stream orders its bits as
+// block_sign_bit says.
+__device__ __forceinline__ uint32_t sign_pair_word(uint32_t h, int i) {
+    return ((h << (15 - i)) & 0x80008000u) | 0x3C003C00u;
 }
 
-// One k-step (64 k) of a generated B stage: rows j < bn (columns tn bn + j of the k x n
-// block-sign operand), each 64 binary16 values K-major in the 128-byte-swizzled layout the
-// TMA would have written (16-byte chunk q of row j at chunk q ^ (j & 7)). Entries past n or
-// past k are zero, as the TMA's out-of-range fill. Lane l writes rows l, l + 32, ...
-__device__ __forceinline__ void gen_b_stage(uint8_t* stage, const UnitDesc& ud, int st, int lane, const uint2* lut) {
+// One k-step (64 k) of a generated B stage, rows j = t0, t0 + nthreads, ... < bn (columns
+// tn bn + j of the k x n block-sign operand): each row 64 binary16 values K-major in the
+// 128-byte-swizzled layout the TMA would have written (16-byte chunk q of row j at chunk
+// q ^ (j & 7)). Entries past n or past k are zero, as the TMA's out-of-range fill. Entry r of
+// the row is word r / 2 of the chunk sequence; word p = 4 q + e takes bits (p mod 16) and
+// (p mod 16) + 16 of 32-bit half p / 16 of the block's hash (block_sign_bit).
+__device__ __forceinline__ void gen_b_rows(uint8_t* stage, const UnitDesc& ud, int st, int t0, int nthreads) {
     const int c0 = ud.tn * ud.bn;
     const int kvalid = ud.k - st * 64;  // >= 1 on every step of the range
     const uint64_t kblocks = static_cast<uint64_t>((ud.k + 63) / 64);
-    const uint64_t vmask = kvalid >= 64 ? ~0ull : ((1ull << kvalid) - 1ull);
-    for (int j = lane; j < ud.bn; j += 32) {
+    for (int j = t0; j < ud.bn; j += nthreads) {
         const int c = c0 + j;
         uint8_t* row = stage + j * 128;
-        if (c >= ud.n) {
-#pragma unroll
-            for (int q = 0; q < 8; ++q) *reinterpret_cast<uint4*>(row + ((q ^ (j & 7)) << 4)) = make_uint4(0, 0, 0, 0);
-            continue;
+        const int sw = j & 7;
+        uint32_t h0 = 0, h1 = 0, on = 0;
+        if (c < ud.n) {
+            const uint64_t bits = rademacher_block_bits(ud.gen_seed, static_cast<uint64_t>(c) * kblocks + st);
+            h0 = static_cast<uint32_t>(bits);
+            h1 = static_cast<uint32_t>(bits >> 32);
+            on = ~0u;
         }
-        const uint64_t bits = rademacher_block_bits(ud.gen_seed, static_cast<uint64_t>(c) * kblocks + st);
 #pragma unroll
         for (int q = 0; q < 8; ++q) {
-            const uint32_t b8 = static_cast<uint32_t>(bits >> (8 * q)) & 0xFFu;
-            const uint32_t v8 = static_cast<uint32_t>(vmask >> (8 * q)) & 0xFFu;
-            uint4 w;
-            if (v8 == 0xFFu) {
-                const uint2 lo = lut[b8 & 15u], hi = lut[b8 >> 4];
-                w = make_uint4(lo.x, lo.y, hi.x, hi.y);
-            } else {  // the last k-step's ragged edge
-                uint32_t h[8];
-#pragma unroll
-                for (int e = 0; e < 8; ++e)
-                    h[e] = ((v8 >> e) & 1u) ? (((b8 >> e) & 1u) ? 0xBC00u : 0x3C00u) : 0u;
-                w = make_uint4(h[0] | (h[1] << 16), h[2] | (h[3] << 16), h[4] | (h[5] << 16), h[6] | (h[7] << 16));
-            }
-            *reinterpret_cast<uint4*>(row + ((q ^ (j & 7)) << 4)) = w;
+            const uint32_t h = q < 4 ? h0 : h1;
+            const int i = 4 * (q & 3);
+            *reinterpret_cast<uint4*>(row + ((q ^ sw) << 4)) =
+                make_uint4(sign_pair_word(h, i) & on, sign_pair_word(h, i + 1) & on, sign_pair_word(h, i + 2) & on,
+                           sign_pair_word(h, i + 3) & on);
         }
+        // the last k-step's ragged edge: entries r >= kvalid are zero
+        for (int r = kvalid; r < 64; ++r)
+            *reinterpret_cast<uint16_t*>(row + (((r >> 3) ^ sw) << 4) + (r & 7) * 2) = 0;
     }
 }
 
 // GEN_B (grouped binary16 launches with a K-major B): problems may ask for their B to be
-// generated by the producer warp (block-sign Rademacher) instead of loaded.
+// generated (block-sign Rademacher) instead of loaded. The split warps write those B stages,
+// spread over their 192 threads, after their share of the A split; the TMA producer skips
+// them. A B stage then completes on the split warps' arrivals (one per warp) or on the
+// producer's TMA (expect_tx plus the same number of arrivals).
 template <int TC, int BN, bool A_KMAJOR, bool B_KMAJOR, bool B_WIDE, bool GEN_B, class Params>
 __device__ __forceinline__ void tile_kernel_body(const Params& p) {
     using Cfg = TileCfg<TC, BN, A_KMAJOR, B_KMAJOR, B_WIDE>;
@@ -693,14 +701,12 @@ __device__ __forceinline__ void tile_kernel_body(const Params& p) {
     uint64_t* drain_bar = d_empty + 2;
     uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(drain_bar + 1);
     volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
-    // the block-sign generator's nibble table (16 x 4 binary16 values), past the barriers
-    uint2* gen_lut = reinterpret_cast<uint2*>(reinterpret_cast<uint8_t*>(bars) + 512);
-    static_assert((4 * SA + 2 * SB + 5) * 8 + 8 <= 512 && 512 + 16 * 8 <= Cfg::BAR_BYTES, "barrier region");
+    static_assert((4 * SA + 2 * SB + 5) * 8 + 8 <= Cfg::BAR_BYTES, "barrier region");
+    constexpr uint32_t kBFullCount = GEN_B ? NSPLIT : 1;
 
     const int warp = threadIdx.x >> 5;
     const int lane = threadIdx.x & 31;
 
-    if (GEN_B && threadIdx.x < 16) gen_lut[threadIdx.x] = rademacher_nibble(threadIdx.x);
     if (threadIdx.x == 0) {
         for (int s = 0; s < SA; ++s) {
             ptx::mbar_init(&a_full[s], 1);
@@ -709,7 +715,7 @@ __device__ __forceinline__ void tile_kernel_body(const Params& p) {
             ptx::mbar_init(&a_empty[s], 1);
         }
         for (int s = 0; s < SB; ++s) {
-            ptx::mbar_init(&b_full[s], 1);
+            ptx::mbar_init(&b_full[s], kBFullCount);
             ptx::mbar_init(&b_empty[s], 1);
         }
         for (int b = 0; b < 2; ++b) {
@@ -742,9 +748,7 @@ __device__ __forceinline__ void tile_kernel_body(const Params& p) {
     ptx::setmaxnreg_dec<Cfg::SPLIT_REGS>();
     if (warp == 0) {
         // ------------------------------------------------------------ TMA producer
-        // Lane 0 issues every TMA load. With GEN_B, the whole warp runs the loop and writes
-        // the B stages of problems whose B is generated (block-sign Rademacher) itself.
-        if (GEN_B || lane == 0) {
+        if (lane == 0) {
             int as = 0, bs = 0;
             uint32_t aph = 0, bph = 0;
             uint32_t a_issued = 0, a_par = 0, b_issued = 0, b_par = 0;  // per stage: load in flight, its parity
@@ -752,16 +756,18 @@ __device__ __forceinline__ void tile_kernel_body(const Params& p) {
                 UnitDesc ud;
                 get_unit<Cfg>(p, u, ud);
                 const int tm = ud.tm, tn = ud.tn, s0 = ud.s0, s1 = ud.s1;
-                if (lane == 0 && ud.maps_in_global) {
+                if (ud.maps_in_global) {
                     ptx::fence_tensormap_acquire(ud.tmap_a);
                     if (!ud.b_gen) ptx::fence_tensormap_acquire(ud.tmap_b);
                 }
                 for (int st = s0; st < s1; ++st) {
                     const int kc = st * Cfg::BK;
-                    int ok = 1;
-                    if (lane == 0) {
-                        ok = ptx::mbar_wait(&a_empty[as], aph ^ 1u, abort_flag, limit) ? 1 : 0;
-                        if (ok) {
+                    {
+                        if (!ptx::mbar_wait(&a_empty[as], aph ^ 1u, abort_flag, limit)) {
+                            fail(kErrProducerTimeout);
+                            goto producer_done;
+                        }
+                        {
                             uint8_t* a_dst = a_base + as * Cfg::A_STAGE;
                             ptx::mbar_arrive_expect_tx(&a_full[as], Cfg::A_RAW);
                             if constexpr (A_KMAJOR) {
@@ -786,31 +792,22 @@ __device__ __forceinline__ void tile_kernel_body(const Params& p) {
                             a_par = (a_par & ~(1u << as)) | (aph << as);
                         }
                     }
-                    if constexpr (GEN_B) ok = __shfl_sync(0xffffffffu, ok, 0);
-                    if (!ok) {
-                        if (lane == 0) fail(kErrProducerTimeout);
-                        goto producer_done;
-                    }
                     if (++as == SA) {
                         as = 0;
                         aph ^= 1u;
                     }
-                    if (lane == 0) ok = ptx::mbar_wait(&b_empty[bs], bph ^ 1u, abort_flag, limit) ? 1 : 0;
-                    if constexpr (GEN_B) ok = __shfl_sync(0xffffffffu, ok, 0);
-                    if (!ok) {
-                        if (lane == 0) fail(kErrProducerTimeout);
+                    if (!ptx::mbar_wait(&b_empty[bs], bph ^ 1u, abort_flag, limit)) {
+                        fail(kErrProducerTimeout);
                         goto producer_done;
                     }
                     if (GEN_B && ud.b_gen) {
-                        // the block-sign operand written by the warp in the TMA's layout, then
-                        // published to the tensor core (async proxy) like the split warps' tiles
-                        gen_b_stage(b_base + bs * Cfg::B_STAGE, ud, st, lane, gen_lut);
-                        ptx::fence_proxy_async_smem();
-                        __syncwarp();
-                        if (lane == 0) ptx::mbar_arrive(&b_full[bs]);
-                    } else if (lane == 0) {
+                        // the split warps write this stage; the slot's earlier load has been
+                        // consumed, so none of it is in flight
+                        b_issued &= ~(1u << bs);
+                    } else {
                         uint8_t* b_dst = b_base + bs * Cfg::B_STAGE;
                         ptx::mbar_arrive_expect_tx(&b_full[bs], ud.bn * Cfg::BK * (B_WIDE ? 4 : 2));
+                        if constexpr (GEN_B) ptx::mbar_arrive_n(&b_full[bs], kBFullCount - 1);
                         if constexpr (B_KMAJOR) {
                             ptx::tma_load_2d(b_dst, ud.tmap_b, &b_full[bs], kc, tn * ud.bn);
                         } else if constexpr (!kTf32) {
@@ -993,7 +990,23 @@ __device__ __forceinline__ void tile_kernel_body(const Params& p) {
                     as = 0;
                     aph ^= 1u;
                 }
-                if constexpr (kTf32 && !B_WIDE) {
+                if constexpr (GEN_B) {
+                    if (ud.b_gen) {
+                        // this stage's generated B, rows spread over all split threads (the
+                        // unit's fields read again here keep them out of the split's registers)
+                        if (!ptx::mbar_wait(&b_empty[bs], bph ^ 1u, abort_flag, limit)) {
+                            fail(kErrSplitTimeout);
+                            goto split_done;
+                        }
+                        UnitDesc ug;
+                        get_unit<Cfg>(p, u, ug);
+                        gen_b_rows(b_base + bs * Cfg::B_STAGE, ug, st, sidx, Cfg::SPLIT_THREADS);
+                        ptx::fence_proxy_async_smem();
+                        __syncwarp();
+                        if (lane == 0) ptx::mbar_arrive(&b_full[bs]);
+                    }
+                }
+                if constexpr ((kTf32 && !B_WIDE) || GEN_B) {
                     if (++bs == SB) {
                         bs = 0;
                         bph ^= 1u;

@@ -349,8 +349,8 @@ __global__ void splitk_reduce_kernel(const float* __restrict__ ws, int slices, i
 // counter hash of (seed, c * k + r) -- splitmix64's finaliser (mix64) -- then Box-Muller
 // for a standard normal or the top bit for a sign; scaled and rounded to binary16. The
 // block-sign stream (SHGEMM_OMEGA_RADEMACHER_BLOCKS) hashes (seed, c * ceil(k / 64) + r / 64)
-// once per 64 entries of a column and takes bit r mod 64: the stream the grouped kernel
-// generates in its B producer (rademacher_block_bits).
+// once per 64 entries of a column and takes bit block_sign_bit(r mod 64): the stream the
+// grouped kernel generates as it goes (rademacher_block_bits, gen_b_rows).
 __global__ void omega_kernel(void* dst, uint64_t ld, uint64_t k, uint64_t cols, int dist, uint64_t seed, float scale,
                              int fp32) {
     const uint64_t total = k * cols;
@@ -361,7 +361,7 @@ __global__ void omega_kernel(void* dst, uint64_t ld, uint64_t k, uint64_t cols, 
         float v;
         if (dist == SHGEMM_OMEGA_RADEMACHER_BLOCKS) {
             const uint64_t bits = rademacher_block_bits(seed, c * kblocks + r / 64);
-            v = ((bits >> (r % 64)) & 1) ? -scale : scale;
+            v = ((bits >> block_sign_bit(static_cast<int>(r % 64))) & 1) ? -scale : scale;
             const __half hv = __float2half_rn(v);
             if (fp32)
                 static_cast<float*>(dst)[r + c * ld] = __half2float(hv);

@@ -308,9 +308,21 @@ def _mix64(z):
     return z ^ (z >> np.uint64(31))
 
 
+def _block_sign_bit(r):
+    """Bit of a block's hash that signs entry r (0..63) of the block: entries 2p and 2p + 1
+    take bits (p mod 16) and (p mod 16) + 16 of 32-bit half p / 16."""
+    p = r >> 1
+    return 32 * (p >> 4) + (p & 15) + 16 * (r & 1)
+
+
+def test_block_sign_bit_order_is_a_permutation():
+    assert sorted(_block_sign_bit(r) for r in range(64)) == list(range(64))
+
+
 def test_block_sign_stream_is_the_documented_one(cuda_device):
     """shgemm_b200_generate_omega(RADEMACHER_BLOCKS): entry (r, c) negative exactly when bit
-    r mod 64 of splitmix64(seed * 0x9E3779B97F4A7C15 + c * ceil(k / 64) + r / 64 + 1) is set."""
+    b(r mod 64) of splitmix64(seed * 0x9E3779B97F4A7C15 + c * ceil(k / 64) + r / 64 + 1) is set,
+    b(r) = 32 (r / 32) + (r / 2 mod 16) + 16 (r mod 2)."""
     import torch
 
     from shgemm_b200 import server as srv
@@ -326,5 +338,5 @@ def test_block_sign_stream_is_the_documented_one(cuda_device):
         for r in range(k):
             with np.errstate(over="ignore"):
                 x = _mix64(base + np.uint64(c * kb + r // 64 + 1))
-            neg = (int(x) >> (r % 64)) & 1
+            neg = (int(x) >> _block_sign_bit(r % 64)) & 1
             assert got[c, r] == (-0.5 if neg else 0.5), (c, r)
