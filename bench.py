@@ -508,6 +508,8 @@ def square_case(args, wl, ctx, traffic_key, tf32_error=False, e2e=True):
                     "frac": achieved / peak, "traffic": None, "peak_kind": label,
                     "work_per_launch": f"4mnk = {flops_issued:.4e} issued tensor flops (two MMAs per k: hi and lo)"}
     roofline["traffic"] = traffic_for(traffic_key + ("_tf32" if wl["tc"] else ""))
+    if roofline["traffic"] is not None:
+        roofline["traffic_source"] = traffic_for(traffic_key + ("_tf32" if wl["tc"] else "") + "_source")
     clocks = clk.summary()
     h.close()
     del A, B, C, C0

@@ -10,13 +10,17 @@
 // therefore loads 16 KB of B per k-step instead of 32 KB, for the same MMA work.
 //
 // Roles in each CTA (640 threads): 8 split warps and 8 epilogue warps as in shgemm_tm_kernel,
-// warp 16 the TMA producer (and tensor-memory allocator), warps 17-18 the two MMA issuers of
-// the even CTA (idle in the odd one). Barriers the even CTA's issuers wait on -- operand
+// warp 16 the TMA producer (and tensor-memory allocator), warps 17-19 the three MMA issuers of
+// the even CTA (idle in the odd one), one per accumulator buffer: half-step g (N-half g mod 2
+// of k-step g / 2) goes to issuer g mod 3 and buffer g mod 3, so an issuer has three
+// half-steps of tensor work (~1500 cycles) to do its barrier waits and commits in while the
+// other two keep the tensor pipe fed. Barriers the even CTA's issuers wait on -- operand
 // stages written (t_full), B stages landed (b_full), accumulator buffers drained (d_empty) --
 // live in the even CTA and count both CTAs' arrivals; the odd CTA's split and epilogue warps
-// arrive there through the cluster window, and both CTAs' B loads complete on the even CTA's
-// b_full. The issuers' commits arrive on the barriers of both CTAs (one commit each, no
-// multicast). Every wait is bounded, as in the other kernels.
+// arrive there through the cluster window (relaxed arrivals: they publish completed
+// tensor-memory accesses only), and both CTAs' B loads complete on the even CTA's b_full.
+// The issuers' commits arrive on the barriers of both CTAs (one commit each, no multicast).
+// Every wait is bounded, as in the other kernels.
 #pragma once
 
 #include "shgemm_kernel_tm.cuh"
@@ -68,7 +72,7 @@ __device__ __forceinline__ void tm2_kernel_body(const TileGemmParams& p) {
     uint64_t* d_full = t_empty + ST;      // accumulator buffer ready to drain
     uint64_t* d_empty = d_full + Cfg::ND; // even CTA: both CTAs drained the buffer
     uint64_t* drain_bar = d_empty + Cfg::ND;  // per issuer: its last MMAs completed
-    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(drain_bar + 2);
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(drain_bar + Cfg::ND);
     volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
 
     const int warp = threadIdx.x >> 5;
@@ -93,8 +97,7 @@ __device__ __forceinline__ void tm2_kernel_body(const TileGemmParams& p) {
             ptx::mbar_init(&d_full[b], 1);
             ptx::mbar_init(&d_empty[b], 16);  // epilogue warps of both CTAs
         }
-        ptx::mbar_init(&drain_bar[0], 1);
-        ptx::mbar_init(&drain_bar[1], 1);
+        for (int b = 0; b < Cfg::ND; ++b) ptx::mbar_init(&drain_bar[b], 1);
         *abort_flag = 0;
         ptx::fence_mbarrier_init();
     }
@@ -183,7 +186,7 @@ __device__ __forceinline__ void tm2_kernel_body(const TileGemmParams& p) {
                 ptx::tc_fence_before();
                 __syncwarp();
                 if (lane == 0) {
-                    ptx::mbar_arrive_cluster(lead(&t_full[ts]));
+                    ptx::mbar_arrive_cluster_relaxed(lead(&t_full[ts]));
                     ptx::mbar_arrive(&a_free[as]);
                 }
                 if (++as == SA) {
@@ -249,7 +252,7 @@ __device__ __forceinline__ void tm2_kernel_body(const TileGemmParams& p) {
                     }
                     ptx::tc_fence_before();
                     __syncwarp();
-                    if (lane == 0) ptx::mbar_arrive_cluster(lead(&d_empty[buf]));
+                    if (lane == 0) ptx::mbar_arrive_cluster_relaxed(lead(&d_empty[buf]));
                 }
                 ++gc;
             }
@@ -349,49 +352,54 @@ __device__ __forceinline__ void tm2_kernel_body(const TileGemmParams& p) {
                     }
                 }
             }
-        } else if ((warp == Cfg::CTRL_WARP0 + 1 || warp == Cfg::CTRL_WARP0 + 2) && lane == 0) {
-            const int h = warp - (Cfg::CTRL_WARP0 + 1);
+        } else if (warp > Cfg::CTRL_WARP0 && lane == 0) {
+            const int j = warp - (Cfg::CTRL_WARP0 + 1);  // issuer j: half-steps g = j mod 3, buffer j
             if (leader) {
                 // -------------------------------------------------------- MMA issuers (even CTA)
                 constexpr uint32_t idesc = ptx::make_idesc(false, false, false, Cfg::PAIR_M, Cfg::HALF_N);
                 int ts = 0, bs = 0;
                 uint32_t tph = 0, bph = 0, gc = 0;
+                const uint32_t d = tmem_base + j * Cfg::HALF_N;
                 for (int u = pair; u < num_units; u += num_pairs) {
                     UnitDesc ud;
                     get_unit<Cfg>(p, u, ud);
                     const int nsteps = ud.s1 - ud.s0;
                     for (int i = 0; i < nsteps; ++i) {
-                        const uint32_t buf = (2 * gc + h) % Cfg::ND;
-                        const bool ok = ptx::mbar_wait_cluster(&t_full[ts], tph, abort_flag, limit) &&
-                                        ptx::mbar_wait_cluster(&b_full[bs], bph, abort_flag, limit) &&
-                                        ptx::mbar_wait_cluster(&d_empty[buf], (((2 * gc + h) / Cfg::ND) & 1u) ^ 1u,
-                                                               abort_flag, limit);
-                        if (!ok) {
-                            fail(kErrMmaTimeout);
-                            goto mma_done;
-                        }
-                        ptx::tc_fence_after();
-                        {
-                            const uint32_t d = tmem_base + buf * Cfg::HALF_N;
-                            const uint32_t a_hi = tmem_base + Cfg::TMEM_OPERAND0 + ts * 64;
-                            // this CTA's 64 rows of N-half h in the stage; the peer's at the same offset
-                            auto bd = [&](int kk) -> uint64_t {
-                                return ptx::make_smem_desc(ptx::smem_u32(b_base + bs * Cfg::B_STAGE) +
-                                                               h * (Cfg::B_COLS * 128) + kk * 32,
-                                                           16, 1024, ptx::kLayoutSW128);
-                            };
 #pragma unroll
-                            for (int kk = 0; kk < 4; ++kk) ptx::umma_f16_ts_pair(d, a_hi + 32 + kk * 8, bd(kk), idesc, kk > 0);
-                            ptx::umma_f16_ts_scale11_pair(d, a_hi, bd(0), idesc);
+                        for (int h = 0; h < 2; ++h) {
+                            const uint32_t g = 2 * gc + h;
+                            if (g % Cfg::ND != static_cast<uint32_t>(j)) continue;
+                            const bool ok = ptx::mbar_wait_cluster(&t_full[ts], tph, abort_flag, limit) &&
+                                            ptx::mbar_wait_cluster(&b_full[bs], bph, abort_flag, limit) &&
+                                            ptx::mbar_wait_cluster(&d_empty[j], ((g / Cfg::ND) & 1u) ^ 1u, abort_flag,
+                                                                   limit);
+                            if (!ok) {
+                                fail(kErrMmaTimeout);
+                                goto mma_done;
+                            }
+                            ptx::tc_fence_after();
+                            {
+                                const uint32_t a_hi = tmem_base + Cfg::TMEM_OPERAND0 + ts * 64;
+                                // this CTA's 64 rows of N-half h in the stage; the peer's at the same offset
+                                auto bd = [&](int kk) -> uint64_t {
+                                    return ptx::make_smem_desc(ptx::smem_u32(b_base + bs * Cfg::B_STAGE) +
+                                                                   h * (Cfg::B_COLS * 128) + kk * 32,
+                                                               16, 1024, ptx::kLayoutSW128);
+                                };
 #pragma unroll
-                            for (int kk = 1; kk < 4; ++kk) ptx::umma_f16_ts_pair(d, a_hi + kk * 8, bd(kk), idesc, 1u);
+                                for (int kk = 0; kk < 4; ++kk)
+                                    ptx::umma_f16_ts_pair(d, a_hi + 32 + kk * 8, bd(kk), idesc, kk > 0);
+                                ptx::umma_f16_ts_scale11_pair(d, a_hi, bd(0), idesc);
+#pragma unroll
+                                for (int kk = 1; kk < 4; ++kk) ptx::umma_f16_ts_pair(d, a_hi + kk * 8, bd(kk), idesc, 1u);
+                            }
+                            ptx::umma_commit_pair(self(&d_full[j]));
+                            ptx::umma_commit_pair(peer(&d_full[j]));
+                            ptx::umma_commit_pair(self(&t_empty[ts]));
+                            ptx::umma_commit_pair(peer(&t_empty[ts]));
+                            ptx::umma_commit_pair(self(&b_empty[bs]));
+                            ptx::umma_commit_pair(peer(&b_empty[bs]));
                         }
-                        ptx::umma_commit_pair(self(&d_full[buf]));
-                        ptx::umma_commit_pair(peer(&d_full[buf]));
-                        ptx::umma_commit_pair(self(&t_empty[ts]));
-                        ptx::umma_commit_pair(peer(&t_empty[ts]));
-                        ptx::umma_commit_pair(self(&b_empty[bs]));
-                        ptx::umma_commit_pair(peer(&b_empty[bs]));
                         if (++ts == ST) {
                             ts = 0;
                             tph ^= 1u;
@@ -405,12 +413,12 @@ __device__ __forceinline__ void tm2_kernel_body(const TileGemmParams& p) {
                 }
             mma_done:
                 // the pair's tensor memory is released only after every MMA of this issuer completed
-                ptx::umma_commit_pair(self(&drain_bar[h]));
-                ptx::umma_commit_pair(peer(&drain_bar[h]));
+                ptx::umma_commit_pair(self(&drain_bar[j]));
+                ptx::umma_commit_pair(peer(&drain_bar[j]));
             }
             // both CTAs: wait for the even CTA's issuers' final commits before the release
             const uint64_t t0 = ptx::globaltimer_ns();
-            while (!ptx::mbar_try_wait_cluster(&drain_bar[h], 0, 20000u)) {
+            while (!ptx::mbar_try_wait_cluster(&drain_bar[j], 0, 20000u)) {
                 if (ptx::globaltimer_ns() - t0 > limit) {
                     fail(kErrDrainTimeout);
                     break;
