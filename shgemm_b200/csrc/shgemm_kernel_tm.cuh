@@ -98,7 +98,7 @@ __device__ __forceinline__ void tm_kernel_body(const Params& p) {
     uint64_t* d_full = t_empty + ST;   // accumulator buffer ready to drain
     uint64_t* d_empty = d_full + Cfg::ND;  // accumulator buffer drained
     uint64_t* drain_bar = d_empty + Cfg::ND;  // one per MMA issuer
-    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(drain_bar + 2);
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(drain_bar + Cfg::ND);
     volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
 
     const int warp = threadIdx.x >> 5;
@@ -111,18 +111,17 @@ __device__ __forceinline__ void tm_kernel_body(const Params& p) {
         }
         for (int s = 0; s < SB; ++s) {
             ptx::mbar_init(&b_full[s], 1);
-            ptx::mbar_init(&b_empty[s], 2);  // both MMA issuers' commits
+            ptx::mbar_init(&b_empty[s], 2);  // the commits of both N-halves' MMAs
         }
         for (int t = 0; t < ST; ++t) {
             ptx::mbar_init(&t_full[t], Cfg::SPLIT_WARPS);
-            ptx::mbar_init(&t_empty[t], 2);  // both MMA issuers' commits
+            ptx::mbar_init(&t_empty[t], 2);  // the commits of both N-halves' MMAs
         }
         for (int b = 0; b < Cfg::ND; ++b) {
             ptx::mbar_init(&d_full[b], 1);
             ptx::mbar_init(&d_empty[b], 8);
         }
-        ptx::mbar_init(&drain_bar[0], 1);
-        ptx::mbar_init(&drain_bar[1], 1);
+        for (int b = 0; b < Cfg::ND; ++b) ptx::mbar_init(&drain_bar[b], 1);
         *abort_flag = 0;
         ptx::fence_mbarrier_init();
     }
@@ -399,12 +398,14 @@ __device__ __forceinline__ void tm_kernel_body(const Params& p) {
                     }
                 }
             }
-        } else if ((warp == Cfg::CTRL_WARP0 + 1 || warp == Cfg::CTRL_WARP0 + 2) && lane == 0) {
+        } else if (warp > Cfg::CTRL_WARP0 && warp <= Cfg::CTRL_WARP0 + Cfg::ND && lane == 0) {
             // ------------------------------------------------------------ MMA issuers
-            // One thread per N-half, in different warps: tcgen05.mma issue stalls while the
-            // tensor pipe's queue is full, so a single issuer's waits and commits between
-            // the halves would leave the pipe idle; two keep it fed.
-            const int h = warp - (Cfg::CTRL_WARP0 + 1);
+            // One thread per accumulator buffer, in different warps: half-chunk g (N-half
+            // g mod 2 of k-chunk g / 2) goes to issuer g mod ND and buffer g mod ND.
+            // tcgen05.mma issue stalls while the tensor pipe's queue is full, so a single
+            // issuer's waits and commits would leave the pipe idle; with ND issuers each has
+            // ND half-chunks of tensor work to do them in while the others keep it fed.
+            const int j = warp - (Cfg::CTRL_WARP0 + 1);
             constexpr uint32_t idesc = ptx::make_idesc(false, false, false, Cfg::BM, Cfg::HALF_N);
             int ts = 0, bs = 0;
             uint32_t tph = 0, bph = 0, gc = 0;  // gc counts k-chunks
@@ -415,76 +416,82 @@ __device__ __forceinline__ void tm_kernel_body(const Params& p) {
                 const int nsteps = ud.s1 - ud.s0;
                 for (int i = 0; i < nsteps; i += KC) {
                     const int c = nsteps - i < KC ? nsteps - i : KC;  // k-steps in this chunk
-                    const uint32_t buf = (2 * gc + h) % Cfg::ND;
                     int tsj[KC], bsj[KC];
-                    bool ok = true;
-                    {
-                        int t = ts, b = bs;
-                        uint32_t tp = tph, bp = bph;
+                    uint32_t tpj[KC], bpj[KC];
 #pragma unroll
-                        for (int j = 0; j < KC; ++j) {
-                            tsj[j] = t;
-                            bsj[j] = b;
-                            if (j < c) {
-                                ok = ok && ptx::mbar_wait(&t_full[t], tp, abort_flag, limit) &&
-                                     ptx::mbar_wait(&b_full[b], bp, abort_flag, limit);
-                                if (++t == ST) {
-                                    t = 0;
-                                    tp ^= 1u;
+                    for (int jj = 0; jj < KC; ++jj) {
+                        tsj[jj] = ts;
+                        bsj[jj] = bs;
+                        tpj[jj] = tph;
+                        bpj[jj] = bph;
+                        if (jj < c) {
+                            if (++ts == ST) {
+                                ts = 0;
+                                tph ^= 1u;
+                            }
+                            if (++bs == SB) {
+                                bs = 0;
+                                bph ^= 1u;
+                            }
+                        }
+                    }
+#pragma unroll
+                    for (int h = 0; h < 2; ++h) {
+                        const uint32_t g = 2 * gc + h;
+                        if (g % Cfg::ND != static_cast<uint32_t>(j)) continue;
+                        bool ok = true;
+#pragma unroll
+                        for (int jj = 0; jj < KC; ++jj) {
+                            if (jj < c)
+                                ok = ok && ptx::mbar_wait(&t_full[tsj[jj]], tpj[jj], abort_flag, limit) &&
+                                     ptx::mbar_wait(&b_full[bsj[jj]], bpj[jj], abort_flag, limit);
+                        }
+                        ok = ok && ptx::mbar_wait(&d_empty[j], ((g / Cfg::ND) & 1u) ^ 1u, abort_flag, limit);
+                        if (!ok) {
+                            fail(kErrMmaTimeout);
+                            goto mma_done;
+                        }
+                        ptx::tc_fence_after();
+                        {
+                            const uint32_t d = tmem_base + j * Cfg::HALF_N;
+                            // rows 128 h .. 128 h + 127 of the [256 n][64 k] B stage of step jj of the chunk
+                            auto bd = [&](int jj, int kk) -> uint64_t {
+                                return ptx::make_smem_desc(ptx::smem_u32(b_base + bsj[jj] * Cfg::B_STAGE) +
+                                                               h * (Cfg::HALF_N * 128) + kk * 32,
+                                                           16, 1024, ptx::kLayoutSW128);
+                            };
+                            auto a_hi = [&](int jj) -> uint32_t {
+                                return tmem_base + Cfg::TMEM_OPERAND0 + tsj[jj] * 64;
+                            };
+                            // the chunk's lo products into a fresh accumulator ...
+#pragma unroll
+                            for (int jj = 0; jj < KC; ++jj) {
+                                if (jj < c) {
+#pragma unroll
+                                    for (int kk = 0; kk < 4; ++kk)
+                                        ptx::umma_f16_ts(d, a_hi(jj) + 32 + kk * 8, bd(jj, kk), idesc,
+                                                         (jj > 0 || kk > 0) ? 1u : 0u);
                                 }
-                                if (++b == SB) {
-                                    b = 0;
-                                    bp ^= 1u;
+                            }
+                            // ... scaled by 2^-11 under the first hi product, then the other hi products
+                            ptx::umma_f16_ts_scale11(d, a_hi(0), bd(0, 0), idesc);
+#pragma unroll
+                            for (int jj = 0; jj < KC; ++jj) {
+                                if (jj < c) {
+#pragma unroll
+                                    for (int kk = (jj == 0 ? 1 : 0); kk < 4; ++kk)
+                                        ptx::umma_f16_ts(d, a_hi(jj) + kk * 8, bd(jj, kk), idesc, 1u);
                                 }
                             }
                         }
-                        ts = t;
-                        tph = tp;
-                        bs = b;
-                        bph = bp;
-                    }
-                    ok = ok && ptx::mbar_wait(&d_empty[buf], (((2 * gc + h) / Cfg::ND) & 1u) ^ 1u, abort_flag, limit);
-                    if (!ok) {
-                        fail(kErrMmaTimeout);
-                        goto mma_done;
-                    }
-                    ptx::tc_fence_after();
-                    {
-                        const uint32_t d = tmem_base + buf * Cfg::HALF_N;
-                        // rows 128 h .. 128 h + 127 of the [256 n][64 k] B stage of step j of the chunk
-                        auto bd = [&](int j, int kk) -> uint64_t {
-                            return ptx::make_smem_desc(ptx::smem_u32(b_base + bsj[j] * Cfg::B_STAGE) +
-                                                           h * (Cfg::HALF_N * 128) + kk * 32,
-                                                       16, 1024, ptx::kLayoutSW128);
-                        };
-                        auto a_hi = [&](int j) -> uint32_t { return tmem_base + Cfg::TMEM_OPERAND0 + tsj[j] * 64; };
-                        // the chunk's lo products into a fresh accumulator ...
+                        issued_any = true;
+                        ptx::umma_commit(&d_full[j]);
 #pragma unroll
-                        for (int j = 0; j < KC; ++j) {
-                            if (j < c) {
-#pragma unroll
-                                for (int kk = 0; kk < 4; ++kk)
-                                    ptx::umma_f16_ts(d, a_hi(j) + 32 + kk * 8, bd(j, kk), idesc, (j > 0 || kk > 0) ? 1u : 0u);
+                        for (int jj = 0; jj < KC; ++jj) {
+                            if (jj < c) {
+                                ptx::umma_commit(&t_empty[tsj[jj]]);
+                                ptx::umma_commit(&b_empty[bsj[jj]]);
                             }
-                        }
-                        // ... scaled by 2^-11 under the first hi product, then the other hi products
-                        ptx::umma_f16_ts_scale11(d, a_hi(0), bd(0, 0), idesc);
-#pragma unroll
-                        for (int j = 0; j < KC; ++j) {
-                            if (j < c) {
-#pragma unroll
-                                for (int kk = (j == 0 ? 1 : 0); kk < 4; ++kk)
-                                    ptx::umma_f16_ts(d, a_hi(j) + kk * 8, bd(j, kk), idesc, 1u);
-                            }
-                        }
-                    }
-                    issued_any = true;
-                    ptx::umma_commit(&d_full[buf]);
-#pragma unroll
-                    for (int j = 0; j < KC; ++j) {
-                        if (j < c) {
-                            ptx::umma_commit(&t_empty[tsj[j]]);
-                            ptx::umma_commit(&b_empty[bsj[j]]);
                         }
                     }
                     ++gc;
@@ -493,9 +500,9 @@ __device__ __forceinline__ void tm_kernel_body(const Params& p) {
         mma_done:
             // Wait for every MMA this thread issued before tensor memory is released.
             if (issued_any) {
-                ptx::umma_commit(&drain_bar[h]);
+                ptx::umma_commit(&drain_bar[j]);
                 const uint64_t t0 = ptx::globaltimer_ns();
-                while (!ptx::mbar_try_wait(&drain_bar[h], 0)) {
+                while (!ptx::mbar_try_wait(&drain_bar[j], 0)) {
                     if (ptx::globaltimer_ns() - t0 > limit) {
                         fail(kErrDrainTimeout);
                         break;
