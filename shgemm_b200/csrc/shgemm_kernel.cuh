@@ -958,6 +958,24 @@ __device__ __forceinline__ void tile_kernel_body(const Params& p) {
             UnitDesc ud;
             get_unit<Cfg>(p, u, ud);
             for (int st = ud.s0; st < ud.s1; ++st) {
+                if constexpr (GEN_B) {
+                    if (ud.b_gen) {
+                        // this stage's generated B, rows spread over all split threads, written
+                        // while the stage's A is still in flight (its slot was freed by the MMAs
+                        // of SB stages back); the unit's fields are read again here, which keeps
+                        // them out of the A split's registers
+                        if (!ptx::mbar_wait(&b_empty[bs], bph ^ 1u, abort_flag, limit)) {
+                            fail(kErrSplitTimeout);
+                            goto split_done;
+                        }
+                        UnitDesc ug;
+                        get_unit<Cfg>(p, u, ug);
+                        gen_b_rows(b_base + bs * Cfg::B_STAGE, ug, st, sidx, Cfg::SPLIT_THREADS);
+                        ptx::fence_proxy_async_smem();
+                        __syncwarp();
+                        if (lane == 0) ptx::mbar_arrive(&b_full[bs]);
+                    }
+                }
                 if (!ptx::mbar_wait(&a_full[as], aph, abort_flag, limit) ||
                     (kTf32 && !B_WIDE && !ptx::mbar_wait(&b_full[bs], bph, abort_flag, limit))) {
                     fail(kErrSplitTimeout);
@@ -989,22 +1007,6 @@ __device__ __forceinline__ void tile_kernel_body(const Params& p) {
                 if (++as == SA) {
                     as = 0;
                     aph ^= 1u;
-                }
-                if constexpr (GEN_B) {
-                    if (ud.b_gen) {
-                        // this stage's generated B, rows spread over all split threads (the
-                        // unit's fields read again here keep them out of the split's registers)
-                        if (!ptx::mbar_wait(&b_empty[bs], bph ^ 1u, abort_flag, limit)) {
-                            fail(kErrSplitTimeout);
-                            goto split_done;
-                        }
-                        UnitDesc ug;
-                        get_unit<Cfg>(p, u, ug);
-                        gen_b_rows(b_base + bs * Cfg::B_STAGE, ug, st, sidx, Cfg::SPLIT_THREADS);
-                        ptx::fence_proxy_async_smem();
-                        __syncwarp();
-                        if (lane == 0) ptx::mbar_arrive(&b_full[bs]);
-                    }
                 }
                 if constexpr ((kTf32 && !B_WIDE) || GEN_B) {
                     if (++bs == SB) {
