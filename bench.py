@@ -579,7 +579,7 @@ def grouped_case(args, wl, ctx, steps=None):
     h = sg.Handle(ctx.local)
     stream = torch.cuda.Stream(dev)
     h.set_stream(stream)
-    probs, shapes, keep, seeds = make_grouped_batch(wl["count"], dev, seed=ctx.rank)
+    probs, shapes, keep, seeds = make_grouped_batch(args.count or wl["count"], dev, seed=ctx.rank)
     torch.cuda.synchronize(dev)
     flops = sum(2.0 * m * n * k for (m, n, k) in shapes)
     b_bytes = 0.0 if wl.get("fused") else (4.0 if wl.get("b_fp32") else 2.0)
@@ -1233,6 +1233,8 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer end-to-end measurement")
     ap.add_argument("--no-autotune", action="store_true", help="plain workloads: use the heuristic plan")
+    ap.add_argument("--count", type=int, default=0,
+                    help="grouped workloads: a batch of COUNT problems from the same distributions (a smaller profiling case)")
     ap.add_argument("--no-nested", action="store_true", help="headline: skip the grouped and square results")
     ap.add_argument("--k-chunk", type=int, default=64, choices=[64, 128],
                     help="k between FP32 drains in the tensor-memory kernel (SHGEMM_CFG_K_CHUNK)")
