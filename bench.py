@@ -676,8 +676,11 @@ def grouped_case(args, wl, ctx, steps=None):
     peaks, peak_kind = load_peaks()
     peak = peaks.get("hbm_gbs", 6650.0)
     achieved = bytes_min / (ms_step * 1e-3) / 1e9
+    # the Omega-generating launch reads no Omega: its ratio is not the measured one
+    ratio = None if wl.get("fused") else traffic_for("grouped" + ("_tf32" if wl["tc"] else "") + "_dram_ratio")
     return {
-        "value": value, "unit": "TFLOP/s", "ms_per_step": ms_step, "steps": steps, "workload": wl["desc"],
+        "value": value, "unit": "TFLOP/s", "ms_per_step": ms_step, "steps": steps,
+        "workload": wl["desc"].replace("batch of 512", f"batch of {len(shapes)}"),
         "problems": len(shapes), "total_flops_2mnk": flops, "algorithmic_bytes": bytes_min,
         "autotuned_tile_n": tiles,
         "per_call_baseline": {"value": per_call_tflops, "unit": "TFLOP/s", "ms_per_step": ms_pc,
@@ -687,7 +690,9 @@ def grouped_case(args, wl, ctx, steps=None):
         "issued_tflops": 2 * value,
         "gpu_launches": steps,  # one grouped kernel per graph replay
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "traffic": traffic_for("grouped" + ("_tf32" if wl["tc"] else "")),
+                     "traffic": (bytes_min * ratio) if ratio else None,
+                     "traffic_source": "measured DRAM/algorithmic ratio of the kernel (profiles/traffic.json) x "
+                                       "this batch's algorithmic bytes" if ratio else None,
                      "peak_kind": f"{peak_kind} HBM copy bandwidth",
                      "work_per_launch": f"sum over problems of A + Omega + Y = {bytes_min:.4e} bytes"},
         "clocks": clk.summary(),
