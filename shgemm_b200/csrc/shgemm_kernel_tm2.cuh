@@ -288,6 +288,7 @@ __device__ __forceinline__ void tm2_kernel_body(const TileGemmParams& p) {
             int as = 0, bs = 0;
             uint32_t aph = 0, bph = 0;
             uint32_t a_issued = 0, a_par = 0;
+            uint32_t b_armed = 0, b_par = 0;  // even CTA: B phases armed with expect_tx, their parity
             const uint32_t b_full_lead0 = lead(&b_full[0]);
             for (int u = pair; u < num_units; u += num_pairs) {
                 UnitDesc ud;
@@ -324,7 +325,11 @@ __device__ __forceinline__ void tm2_kernel_body(const TileGemmParams& p) {
                     {
                         // this CTA's 64 columns of each N-half; both CTAs' loads complete on the
                         // even CTA's b_full, which expects the bytes of all four boxes
-                        if (leader) ptx::mbar_arrive_expect_tx(&b_full[bs], 2 * Cfg::B_STAGE);
+                        if (leader) {
+                            ptx::mbar_arrive_expect_tx(&b_full[bs], 2 * Cfg::B_STAGE);
+                            b_armed |= 1u << bs;
+                            b_par = (b_par & ~(1u << bs)) | (bph << bs);
+                        }
                         uint8_t* b_dst = b_base + bs * Cfg::B_STAGE;
                         const uint32_t bar = b_full_lead0 + bs * 8;
 #pragma unroll
@@ -339,8 +344,23 @@ __device__ __forceinline__ void tm2_kernel_body(const TileGemmParams& p) {
                 }
             }
         producer_done:
-            // Never leave with this CTA's A copies in flight (its B copies complete on the even
-            // CTA's barrier; the pair's final cluster barrier orders them before the exit).
+            // Never leave with copies in flight: this CTA's A copies complete on its own
+            // barriers; both CTAs' B copies complete on the even CTA's, so the even CTA's
+            // producer waits for every B phase it armed, and the pair's final cluster barrier
+            // keeps the odd CTA resident until then.
+            if (leader) {
+                for (int s = 0; s < SB; ++s) {
+                    if (!(b_armed & (1u << s))) continue;
+                    const uint32_t par = (b_par >> s) & 1u;
+                    const uint64_t t0 = ptx::globaltimer_ns();
+                    while (!ptx::mbar_try_wait_cluster(&b_full[s], par, 20000u)) {
+                        if (ptx::globaltimer_ns() - t0 > limit) {
+                            fail(kErrDrainTimeout);
+                            break;
+                        }
+                    }
+                }
+            }
             for (int s = 0; s < SA; ++s) {
                 if (!(a_issued & (1u << s))) continue;
                 const uint32_t par = (a_par >> s) & 1u;
