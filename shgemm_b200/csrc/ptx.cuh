@@ -337,7 +337,7 @@ __device__ __forceinline__ bool mbar_wait_cluster(uint64_t* bar, uint32_t parity
 }
 
 // 2-D TMA load into this CTA's shared memory whose completion is counted on an mbarrier that
-// may live in the pair's other CTA (`bar_cluster` from mapa_shared). No multicast.
+// may live in the pair's other CTA (`bar_cluster` from mapa_shared); the copy lands in this CTA only.
 __device__ __forceinline__ void tma_load_2d_pair(void* dst, const void* tmap, uint32_t bar_cluster, int32_t x,
                                                  int32_t y) {
     asm volatile(

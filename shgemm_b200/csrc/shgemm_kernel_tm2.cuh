@@ -19,7 +19,7 @@
 // live in the even CTA and count both CTAs' arrivals; the odd CTA's split and epilogue warps
 // arrive there through the cluster window (relaxed arrivals: they publish completed
 // tensor-memory accesses only), and both CTAs' B loads complete on the even CTA's b_full.
-// The issuers' commits arrive on the barriers of both CTAs (one commit each, no multicast).
+// The issuers' commits arrive on the barriers of both CTAs (one commit per barrier, by address).
 // Every wait is bounded, as in the other kernels.
 #pragma once
 
