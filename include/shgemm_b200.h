@@ -358,12 +358,30 @@ int shgemm_b200_noalloc_check_error(void* cuda_stream, int* device_code);
 enum { SHGEMM_OMEGA_GAUSSIAN = 0, SHGEMM_OMEGA_RADEMACHER = 1, SHGEMM_OMEGA_RADEMACHER_BLOCKS = 2 };
 
 /* Writes Omega (k x cols, column-major, leading dimension ld elements) on `cuda_stream`:
- * entry (r, c) = scale * g(seed, c * k + r) rounded to binary16, g standard normal
- * (Box-Muller over a splitmix64 counter hash) or a random sign. fp32 = 0 stores
- * binary16; fp32 = 1 stores the same binary16 values widened to FP32 (the B operand
- * of a TF32 batch with SHGEMM_CFG_GROUPED_B_FP32). */
+ * entry (r, c) = scale * g rounded to binary16. GAUSSIAN: entries 2i and 2i + 1 of a column
+ * are the cosine and sine normals of one Box-Muller pair from the splitmix64 counter hash of
+ * (seed, c * k + 2i). RADEMACHER: a random sign from the hash of (seed, c * k + r).
+ * fp32 = 0 stores binary16; fp32 = 1 stores the same binary16 values widened to FP32 (the B
+ * operand of a TF32 batch with SHGEMM_CFG_GROUPED_B_FP32). */
 int shgemm_b200_generate_omega(void* cuda_stream, void* dst, size_t ld, size_t k, size_t cols, int dist,
                                unsigned long long seed, float scale, int fp32);
+
+/* One Omega of a batch, with the arguments of shgemm_b200_generate_omega. */
+struct shgemm_b200_omega_job {
+    void* dst;
+    size_t ld;
+    size_t k;
+    size_t cols;
+    unsigned long long seed;
+    float scale;
+    int dist;
+};
+
+/* Writes `count` Omegas, each exactly as shgemm_b200_generate_omega would, in one launch per 64
+ * jobs on `cuda_stream` (the sketch server generates all draws of a batch this way). fp32 applies
+ * to every job. */
+int shgemm_b200_generate_omega_batch(void* cuda_stream, const struct shgemm_b200_omega_job* jobs, int count,
+                                     int fp32);
 
 typedef struct shgemm_b200_server* shgemm_b200_server_t;
 

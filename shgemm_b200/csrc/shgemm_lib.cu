@@ -345,44 +345,63 @@ __global__ void splitk_reduce_kernel(const float* __restrict__ ws, int slices, i
     }
 }
 
-// Sketch operand generator: entry (r, c) of a k x cols column-major Omega from a
-// counter hash of (seed, c * k + r) -- splitmix64's finaliser (mix64) -- then Box-Muller
-// for a standard normal or the top bit for a sign; scaled and rounded to binary16. The
-// block-sign stream (SHGEMM_OMEGA_RADEMACHER_BLOCKS) hashes (seed, c * ceil(k / 64) + r / 64)
-// once per 64 entries of a column and takes bit block_sign_bit(r mod 64): the stream the
-// grouped kernel generates as it goes (rademacher_block_bits, gen_b_rows).
-__global__ void omega_kernel(void* dst, uint64_t ld, uint64_t k, uint64_t cols, int dist, uint64_t seed, float scale,
-                             int fp32) {
-    const uint64_t total = k * cols;
-    const uint64_t kblocks = (k + 63) / 64;
-    for (uint64_t idx = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; idx < total;
-         idx += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
-        const uint64_t c = idx / k, r = idx - c * k;
-        float v;
-        if (dist == SHGEMM_OMEGA_RADEMACHER_BLOCKS) {
-            const uint64_t bits = rademacher_block_bits(seed, c * kblocks + r / 64);
-            v = ((bits >> block_sign_bit(static_cast<int>(r % 64))) & 1) ? -scale : scale;
-            const __half hv = __float2half_rn(v);
-            if (fp32)
-                static_cast<float*>(dst)[r + c * ld] = __half2float(hv);
-            else
-                static_cast<__half*>(dst)[r + c * ld] = hv;
-            continue;
-        }
-        const uint64_t x = mix64(seed * 0x9E3779B97F4A7C15ull + idx + 1);
-        if (dist == SHGEMM_OMEGA_RADEMACHER) {
-            v = (x >> 63) ? -scale : scale;
-        } else {
+// Sketch operand generator. GAUSSIAN: entries 2i and 2i + 1 of column c of a k x cols
+// column-major Omega are z cos(2 pi u2) and z sin(2 pi u2), z = sqrt(-2 ln u1), u1 and u2 the
+// top and middle 24 bits of the counter hash of (seed, c k + 2i) -- splitmix64's finaliser
+// (mix64) -- one hash, one logarithm and one sincos per pair; scaled and rounded to binary16.
+// RADEMACHER: the top bit of the hash of (seed, c k + r) as the sign of entry r. The block-sign
+// stream (SHGEMM_OMEGA_RADEMACHER_BLOCKS) hashes (seed, c * ceil(k / 64) + r / 64) once per 64
+// entries of a column and takes bit block_sign_bit(r mod 64): the stream the grouped kernel
+// generates as it goes (rademacher_block_bits, gen_b_rows).
+__device__ __forceinline__ void omega_store(void* dst, uint64_t i, float v, int fp32) {
+    const __half hv = __float2half_rn(v);
+    if (fp32)
+        static_cast<float*>(dst)[i] = __half2float(hv);
+    else
+        static_cast<__half*>(dst)[i] = hv;
+}
+
+// Thread t of nt writes its share of one Omega.
+__device__ __forceinline__ void omega_fill(const shgemm_b200_omega_job& j, int fp32, uint64_t t, uint64_t nt) {
+    const uint64_t k = j.k, cols = j.cols, ld = j.ld;
+    const float scale = j.scale;
+    if (j.dist == SHGEMM_OMEGA_GAUSSIAN) {
+        const uint64_t kp = (k + 1) / 2, total = kp * cols;
+        for (uint64_t idx = t; idx < total; idx += nt) {
+            const uint64_t c = idx / kp, r = 2 * (idx - c * kp);
+            const uint64_t x = mix64(j.seed * 0x9E3779B97F4A7C15ull + c * k + r + 1);
             const float u1 = static_cast<float>((x >> 40) + 1) * 0x1p-24f;  // (0, 1]
             const float u2 = static_cast<float>((x >> 16) & 0xFFFFFFull) * 0x1p-24f;
-            v = scale * (sqrtf(-2.0f * logf(u1)) * cospif(2.0f * u2));
+            const float z = scale * sqrtf(-2.0f * logf(u1));
+            float sn, cs;
+            sincospif(2.0f * u2, &sn, &cs);
+            omega_store(j.dst, r + c * ld, z * cs, fp32);
+            if (r + 1 < k) omega_store(j.dst, r + 1 + c * ld, z * sn, fp32);
         }
-        const __half hv = __float2half_rn(v);
-        if (fp32)
-            static_cast<float*>(dst)[r + c * ld] = __half2float(hv);
-        else
-            static_cast<__half*>(dst)[r + c * ld] = hv;
+        return;
     }
+    const uint64_t total = k * cols, kblocks = (k + 63) / 64;
+    for (uint64_t idx = t; idx < total; idx += nt) {
+        const uint64_t c = idx / k, r = idx - c * k;
+        bool neg;
+        if (j.dist == SHGEMM_OMEGA_RADEMACHER_BLOCKS)
+            neg = (rademacher_block_bits(j.seed, c * kblocks + r / 64) >> block_sign_bit(static_cast<int>(r % 64))) & 1;
+        else
+            neg = mix64(j.seed * 0x9E3779B97F4A7C15ull + idx + 1) >> 63;
+        omega_store(j.dst, r + c * ld, neg ? -scale : scale, fp32);
+    }
+}
+
+constexpr int kOmegaJobsPerLaunch = 64;
+struct OmegaBatch {
+    shgemm_b200_omega_job job[kOmegaJobsPerLaunch];
+    int fp32;
+};
+
+// blockIdx.y = job; the x blocks of a job share its entries.
+__global__ void omega_kernel(const __grid_constant__ OmegaBatch b) {
+    omega_fill(b.job[blockIdx.y], b.fp32, blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x,
+               static_cast<uint64_t>(gridDim.x) * blockDim.x);
 }
 
 __global__ void selftest_wait_kernel(int* error_flag, uint64_t limit_ns) {
@@ -877,21 +896,47 @@ int shgemm_b200_get_launch_count(shgemm_b200_handle_t h, long long* count) {
     return SHGEMM_STATUS_OK;
 }
 
-int shgemm_b200_generate_omega(void* cuda_stream, void* dst, size_t ld, size_t k, size_t cols, int dist,
-                               unsigned long long seed, float scale, int fp32) {
-    if ((dist != SHGEMM_OMEGA_GAUSSIAN && dist != SHGEMM_OMEGA_RADEMACHER && dist != SHGEMM_OMEGA_RADEMACHER_BLOCKS) ||
-        (fp32 != 0 && fp32 != 1) || ld < k)
-        return SHGEMM_STATUS_INVALID_VALUE;
-    if (k == 0 || cols == 0) return SHGEMM_STATUS_OK;
-    if (!dst) return SHGEMM_STATUS_INVALID_VALUE;
+int shgemm_b200_generate_omega_batch(void* cuda_stream, const struct shgemm_b200_omega_job* jobs, int count,
+                                     int fp32) {
+    if (count < 0 || (count > 0 && !jobs) || (fp32 != 0 && fp32 != 1)) return SHGEMM_STATUS_INVALID_VALUE;
+    for (int i = 0; i < count; ++i) {
+        const shgemm_b200_omega_job& j = jobs[i];
+        if ((j.dist != SHGEMM_OMEGA_GAUSSIAN && j.dist != SHGEMM_OMEGA_RADEMACHER &&
+             j.dist != SHGEMM_OMEGA_RADEMACHER_BLOCKS) ||
+            j.ld < j.k || (j.k > 0 && j.cols > 0 && !j.dst))
+            return SHGEMM_STATUS_INVALID_VALUE;
+    }
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    const uint64_t total = static_cast<uint64_t>(k) * cols;
-    const unsigned blocks = static_cast<unsigned>(std::min<uint64_t>((total + 255) / 256, static_cast<uint64_t>(sms) * 8));
-    omega_kernel<<<blocks, 256, 0, static_cast<cudaStream_t>(cuda_stream)>>>(dst, ld, k, cols, dist, seed, scale, fp32);
-    if (cudaGetLastError() != cudaSuccess) return SHGEMM_STATUS_LAUNCH_FAILED;
+    for (int first = 0; first < count; first += kOmegaJobsPerLaunch) {
+        OmegaBatch b;
+        std::memset(&b, 0, sizeof(b));
+        b.fp32 = fp32;
+        int n = 0;
+        uint64_t most = 0, all = 0;
+        for (int i = first; i < count && i < first + kOmegaJobsPerLaunch; ++i) {
+            if (jobs[i].k == 0 || jobs[i].cols == 0) continue;
+            b.job[n++] = jobs[i];
+            const uint64_t items = jobs[i].dist == SHGEMM_OMEGA_GAUSSIAN ? (jobs[i].k + 1) / 2 * jobs[i].cols
+                                                                         : static_cast<uint64_t>(jobs[i].k) * jobs[i].cols;
+            most = std::max(most, items);
+            all += items;
+        }
+        if (n == 0) continue;
+        // blocks per job: the largest job's items, with the whole launch near 8 blocks per SM
+        const uint64_t cap = std::max<uint64_t>(1, (static_cast<uint64_t>(sms) * 8 * most + all - 1) / all);
+        const unsigned bx = static_cast<unsigned>(std::min<uint64_t>((most + 255) / 256, cap));
+        omega_kernel<<<dim3(bx, n), 256, 0, static_cast<cudaStream_t>(cuda_stream)>>>(b);
+        if (cudaGetLastError() != cudaSuccess) return SHGEMM_STATUS_LAUNCH_FAILED;
+    }
     return SHGEMM_STATUS_OK;
+}
+
+int shgemm_b200_generate_omega(void* cuda_stream, void* dst, size_t ld, size_t k, size_t cols, int dist,
+                               unsigned long long seed, float scale, int fp32) {
+    const shgemm_b200_omega_job j{dst, ld, k, cols, seed, scale, dist};
+    return shgemm_b200_generate_omega_batch(cuda_stream, &j, 1, fp32);
 }
 
 int shgemm_b200_selftest_wait_timeout(shgemm_b200_handle_t h, unsigned limit_us, int* observed) {

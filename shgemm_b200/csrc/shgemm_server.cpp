@@ -219,17 +219,17 @@ bool shgemm_b200_server::launch_locked(Slot& s) {
     }
     if (s.reqs.empty()) return false;
     bool ok = cudaEventRecord(s.start, s.stream) == cudaSuccess;
+    std::vector<shgemm_b200_omega_job> jobs;
     for (auto& qp : s.reqs) {
         Request& q = *qp;
         q.state = SHGEMM_REQ_RUNNING;
         const size_t cols = q.r.n * static_cast<size_t>(q.r.draws);
         // draw j of Omega from (seed, j): column block j of the k x (draws n) operand
-        for (int j = 0; j < q.r.draws && ok; ++j) {
+        for (int j = 0; j < q.r.draws; ++j) {
             uint8_t* dst = arena.ptr(q.om_off) + static_cast<size_t>(j) * q.r.n * q.ldb * omega_elem(*this);
-            ok = shgemm_b200_generate_omega(s.stream, dst, q.ldb, q.r.k, q.r.n, q.r.omega_dist,
-                                            q.r.omega_seed * 0x100000001B3ull + static_cast<unsigned long long>(j),
-                                            q.r.omega_scale, fp32) == SHGEMM_STATUS_OK;
-            ++n_launches;
+            jobs.push_back({dst, q.ldb, q.r.k, q.r.n,
+                            q.r.omega_seed * 0x100000001B3ull + static_cast<unsigned long long>(j), q.r.omega_scale,
+                            q.r.omega_dist});
         }
         shgemm_b200_problem p{};
         p.m = q.r.m;
@@ -245,6 +245,10 @@ bool shgemm_b200_server::launch_locked(Slot& s) {
         p.beta = 0.0f;
         probs.push_back(p);
     }
+    // every draw of the batch in one launch (per 64 draws)
+    ok = ok && shgemm_b200_generate_omega_batch(s.stream, jobs.data(), static_cast<int>(jobs.size()), fp32) ==
+                   SHGEMM_STATUS_OK;
+    n_launches += (jobs.size() + 63) / 64;
     ok = ok && cudaEventRecord(s.mid, s.stream) == cudaSuccess;
     ok = ok && shgemm_b200_shgemm_grouped(s.h, SHGEMM_OP_N, SHGEMM_OP_N, tc, SHGEMM_OP_N, probs.data(),
                                           static_cast<int>(probs.size())) == SHGEMM_STATUS_OK;

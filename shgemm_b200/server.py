@@ -28,6 +28,11 @@ class SketchRequest(ctypes.Structure):
                 ("omega_scale", ctypes.c_float), ("omega_seed", ctypes.c_ulonglong)]
 
 
+class OmegaJob(ctypes.Structure):
+    _fields_ = [("dst", ctypes.c_void_p), ("ld", ctypes.c_size_t), ("k", ctypes.c_size_t), ("cols", ctypes.c_size_t),
+                ("seed", ctypes.c_ulonglong), ("scale", ctypes.c_float), ("dist", ctypes.c_int)]
+
+
 class ServerStats(ctypes.Structure):
     _fields_ = [("submitted", ctypes.c_ulonglong), ("completed", ctypes.c_ulonglong), ("failed", ctypes.c_ulonglong),
                 ("batches", ctypes.c_ulonglong), ("p50_ms", ctypes.c_double), ("p99_ms", ctypes.c_double),
@@ -52,6 +57,7 @@ def _declare():
     ull = ctypes.c_ulonglong
     sig = {
         "shgemm_b200_generate_omega": [vp, vp, sz, sz, sz, i, ull, ctypes.c_float, i],
+        "shgemm_b200_generate_omega_batch": [vp, ctypes.POINTER(OmegaJob), i, i],
         "shgemm_b200_server_create": [ctypes.POINTER(vp), i, ctypes.POINTER(ServerConfig)],
         "shgemm_b200_server_destroy": [vp],
         "shgemm_b200_server_submit": [vp, ctypes.POINTER(SketchRequest), ctypes.POINTER(ull)],
@@ -81,6 +87,17 @@ def generate_omega(dst, ld: int, k: int, cols: int, dist: int = GAUSSIAN, seed: 
     """Writes a k x cols column-major Omega (binary16, or binary16 values widened to FP32) on `stream`."""
     _check(_declare().shgemm_b200_generate_omega(_stream_addr(stream), _addr(dst), ld, k, cols, dist,
                                                  seed & 0xFFFFFFFFFFFFFFFF, scale, int(fp32)), "generate_omega")
+
+
+def generate_omega_batch(jobs, fp32: bool = False, stream=None) -> None:
+    """Writes several Omegas in one launch per 64: ``jobs`` holds (dst, ld, k, cols, dist, seed,
+    scale) tuples, each written exactly as ``generate_omega`` would."""
+    arr = (OmegaJob * max(1, len(jobs)))()
+    for q, (dst, ld, k, cols, dist, seed, scale) in zip(arr, jobs):
+        q.dst, q.ld, q.k, q.cols = _addr(dst), ld, k, cols
+        q.seed, q.scale, q.dist = seed & 0xFFFFFFFFFFFFFFFF, scale, dist
+    _check(_declare().shgemm_b200_generate_omega_batch(_stream_addr(stream), arr, len(jobs), int(fp32)),
+           "generate_omega_batch")
 
 
 class SketchServer:

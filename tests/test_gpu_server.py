@@ -58,6 +58,67 @@ def test_generate_omega(cuda_device, dist):
         assert abs(np.mean(x > 0) - 0.5) < 0.01
 
 
+def _mix64(z):
+    """splitmix64's finaliser on numpy uint64 (wrapping arithmetic)."""
+    z = np.asarray(z, dtype=np.uint64)
+    with np.errstate(over="ignore"):
+        z = (z ^ (z >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)
+        z = (z ^ (z >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
+    return z ^ (z >> np.uint64(31))
+
+
+def test_gaussian_omega_is_box_muller_pairs_of_the_hash(cuda_device):
+    """Entries 2i, 2i + 1 of column c are z cos(2 pi u2), z sin(2 pi u2) with z = sqrt(-2 ln u1)
+    and u1, u2 from splitmix64(seed * 0x9E3779B97F4A7C15 + c k + 2i + 1): checked through the
+    pair's radius and angle, to the binary16 rounding of the stored values (odd k: the last
+    entry of a column is a cosine alone)."""
+    from shgemm_b200 import server as srv
+
+    k, n, seed, scale = 301, 7, 99, 1.0
+    _, om = _omega_host(k, n, seed, True, scale, srv.GAUSSIAN)
+    om = om.astype(np.float64)
+    with np.errstate(over="ignore"):
+        base = np.uint64(seed) * np.uint64(0x9E3779B97F4A7C15)
+    for c in range(n):
+        r = np.arange(0, k, 2, dtype=np.uint64)
+        with np.errstate(over="ignore"):
+            x = _mix64(base + np.uint64(c * k) + r + np.uint64(1))
+        u1 = ((x >> np.uint64(40)) + np.uint64(1)).astype(np.float64) * 2.0 ** -24
+        u2 = ((x >> np.uint64(16)) & np.uint64(0xFFFFFF)).astype(np.float64) * 2.0 ** -24
+        z = np.sqrt(-2.0 * np.log(u1))
+        z0 = om[c, 0::2]
+        np.testing.assert_allclose(z0, scale * z * np.cos(2 * np.pi * u2), rtol=2e-3, atol=2e-3)
+        z1 = om[c, 1::2]
+        np.testing.assert_allclose(z1, (scale * z * np.sin(2 * np.pi * u2))[:len(z1)], rtol=2e-3, atol=2e-3)
+
+
+@pytest.mark.parametrize("fp32", [False, True])
+def test_omega_batch_matches_single_calls(cuda_device, fp32):
+    """One batched launch writes every job exactly as its own generate_omega call would: mixed
+    distributions, seeds, scales, ragged and odd k, leading dimensions past k, an empty job."""
+    import torch
+
+    from shgemm_b200 import server as srv
+
+    specs = [(300, 17, srv.GAUSSIAN, 5, 0.25), (301, 3, srv.RADEMACHER, 6, 1.0), (64, 64, srv.RADEMACHER_BLOCKS, 7, 0.5),
+             (1, 9, srv.GAUSSIAN, 8, 2.0), (0, 4, srv.GAUSSIAN, 9, 1.0), (4097, 2, srv.GAUSSIAN, 10, 0.125)]
+    dt = torch.float32 if fp32 else torch.float16
+    bufs1, bufs2, jobs = [], [], []
+    for (k, cols, dist, seed, scale) in specs:
+        ld = k + 8
+        b1 = torch.zeros(max(1, cols * ld), device="cuda", dtype=dt)
+        b2 = torch.zeros_like(b1)
+        srv.generate_omega(b1, ld, k, cols, dist, seed, scale, fp32)
+        jobs.append((b2, ld, k, cols, dist, seed, scale))
+        bufs1.append(b1)
+        bufs2.append(b2)
+    srv.generate_omega_batch(jobs, fp32)
+    torch.cuda.synchronize()
+    for b1, b2 in zip(bufs1, bufs2):
+        assert torch.equal(b1.view(torch.int16 if not fp32 else torch.int32),
+                           b2.view(torch.int16 if not fp32 else torch.int32))
+
+
 @pytest.mark.parametrize("tc", [oracle.FP16, oracle.TF32])
 def test_server_result_matches_oracle(cuda_device, tc):
     import torch
