@@ -93,7 +93,7 @@ WORKLOADS = {
     "grouped_fused": dict(m=0, n=0, k=0, op_a=0, op_b=0, tc=0, alpha=1.0, beta=0.0, dist="grouped", count=512,
                           bound="hbm", fused=True,
                           desc="grouped batch of 512 uneven right sketches (shapes as the fp16 batch), Omega_i "
-                               "block-sign Rademacher generated by the grouped kernel's B producer (no Omega reads), "
+                               "block-sign Rademacher generated inside the grouped kernel (no Omega reads), "
                                "scale 1/sqrt(n_i) as alpha, fp16 compute, one CUDA-graph-captured launch"),
     # the same batch in TF32 compute, Omega_i handed over widened to FP32 (as the sketch server keeps it)
     "grouped_tf32": dict(m=0, n=0, k=0, op_a=0, op_b=0, tc=1, alpha=1.0, beta=0.0, dist="grouped", count=512,
@@ -586,7 +586,7 @@ def grouped_case(args, wl, ctx, steps=None):
     bytes_min = sum(4.0 * m * k + b_bytes * k * n + 4.0 * m * n for (m, n, k) in shapes)
     gprobs, keep_w = probs, []
     if wl.get("fused"):
-        # Omega_i generated by the grouped kernel's B producer from its seed: not read at all
+        # Omega_i generated inside the grouped kernel from its seed: not read at all
         gprobs = [(m, n, k, A, lda, None, 0, C, ldc, al, be, srv.RADEMACHER_BLOCKS, sd)
                   for (m, n, k, A, lda, B, ldb, C, ldc, al, be), sd in zip(probs, seeds)]
     elif wl.get("b_fp32"):

@@ -166,8 +166,8 @@ struct alignas(64) GroupedProblem {
     int bn;     // tile N of this problem (<= the kernel's BN; 16-multiple)
     int steps;  // k-steps
     float alpha, beta;
-    int b_gen;          // 1: B is the block-sign Rademacher operand of gen_seed (entries +-1), generated
-    int pad0;           //    by the B producer instead of loaded (binary16 compute); tmap_b unused
+    int b_gen;          // 1: B is the block-sign Rademacher operand of gen_seed (entries +-1), written
+    int pad0;           //    by the split warps instead of loaded (binary16 compute); tmap_b unused
     uint64_t gen_seed;
 };
 static_assert(sizeof(GroupedProblem) % 64 == 0, "GroupedProblem alignment");

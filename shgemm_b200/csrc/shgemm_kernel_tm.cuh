@@ -14,7 +14,7 @@
 //    MMAs (about 1024 cycles) instead of one;
 //  * 20 warps: 8 split warps (two per TMEM lane quadrant, one per 32-k half of the
 //    step), 8 epilogue warps (two per quadrant, one per 64-column quarter of each
-//    half), a TMA producer warp and two MMA warps (one per N-half).
+//    half), a TMA producer warp and three MMA warps (one per accumulator buffer).
 //
 // Tensor memory (512 columns): accumulator buffer b at columns [128 b, 128 b + 128), b < 3,
 // used by half h of k-step s when (2 s + h) % 3 == b; operand stage t at
