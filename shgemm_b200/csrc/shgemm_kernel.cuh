@@ -640,8 +640,14 @@ __device__ __forceinline__ uint32_t sign_pair_word(uint32_t h, int i) {
 // q ^ (j & 7)). Entries past n or past k are zero, as the TMA's out-of-range fill. Entry r of
 // the row is word r / 2 of the chunk sequence; word p = 4 q + e takes bits (p mod 16) and
 // (p mod 16) + 16 of 32-bit half p / 16 of the block's hash (block_sign_bit).
-__device__ __forceinline__ void gen_b_rows(uint8_t* stage, const UnitDesc& ud, int st, int t0, int nthreads) {
-    const int c0 = ud.tn * ud.bn;
+// What the generator needs of a unit: its first B column, tile N, n, k and seed.
+struct GenB {
+    uint64_t seed;
+    int c0, bn, n, k;
+};
+
+__device__ __forceinline__ void gen_b_rows(uint8_t* stage, const GenB& ud, int st, int t0, int nthreads) {
+    const int c0 = ud.c0;
     const int kvalid = ud.k - st * 64;  // >= 1 on every step of the range
     const uint64_t kblocks = static_cast<uint64_t>((ud.k + 63) / 64);
     for (int j = t0; j < ud.bn; j += nthreads) {
@@ -650,7 +656,7 @@ __device__ __forceinline__ void gen_b_rows(uint8_t* stage, const UnitDesc& ud, i
         const int sw = j & 7;
         uint32_t h0 = 0, h1 = 0, on = 0;
         if (c < ud.n) {
-            const uint64_t bits = rademacher_block_bits(ud.gen_seed, static_cast<uint64_t>(c) * kblocks + st);
+            const uint64_t bits = rademacher_block_bits(ud.seed, static_cast<uint64_t>(c) * kblocks + st);
             h0 = static_cast<uint32_t>(bits);
             h1 = static_cast<uint32_t>(bits >> 32);
             on = ~0u;
@@ -701,7 +707,10 @@ __device__ __forceinline__ void tile_kernel_body(const Params& p) {
     uint64_t* drain_bar = d_empty + 2;
     uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(drain_bar + 1);
     volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
-    static_assert((4 * SA + 2 * SB + 5) * 8 + 8 <= Cfg::BAR_BYTES, "barrier region");
+    // per split warp: the current unit's generator parameters, past the barriers
+    GenB* gen_slots = reinterpret_cast<GenB*>(reinterpret_cast<uint8_t*>(bars) + 512);
+    static_assert((4 * SA + 2 * SB + 5) * 8 + 8 <= 512 && 512 + 8 * sizeof(GenB) <= Cfg::BAR_BYTES,
+                  "barrier region");
     constexpr uint32_t kBFullCount = GEN_B ? NSPLIT : 1;
 
     const int warp = threadIdx.x >> 5;
@@ -957,20 +966,24 @@ __device__ __forceinline__ void tile_kernel_body(const Params& p) {
         for (int u = blockIdx.x; u < num_units; u += gridDim.x) {
             UnitDesc ud;
             get_unit<Cfg>(p, u, ud);
+            if constexpr (GEN_B) {
+                // the generator's view of the unit, kept in this warp's shared slot rather than
+                // in registers the A split needs
+                if (ud.b_gen && lane == 0)
+                    gen_slots[warp - 2] = GenB{ud.gen_seed, ud.tn * ud.bn, ud.bn, ud.n, ud.k};
+                __syncwarp();
+            }
             for (int st = ud.s0; st < ud.s1; ++st) {
                 if constexpr (GEN_B) {
                     if (ud.b_gen) {
                         // this stage's generated B, rows spread over all split threads, written
                         // while the stage's A is still in flight (its slot was freed by the MMAs
-                        // of SB stages back); the unit's fields are read again here, which keeps
-                        // them out of the A split's registers
+                        // of SB stages back)
                         if (!ptx::mbar_wait(&b_empty[bs], bph ^ 1u, abort_flag, limit)) {
                             fail(kErrSplitTimeout);
                             goto split_done;
                         }
-                        UnitDesc ug;
-                        get_unit<Cfg>(p, u, ug);
-                        gen_b_rows(b_base + bs * Cfg::B_STAGE, ug, st, sidx, Cfg::SPLIT_THREADS);
+                        gen_b_rows(b_base + bs * Cfg::B_STAGE, gen_slots[warp - 2], st, sidx, Cfg::SPLIT_THREADS);
                         ptx::fence_proxy_async_smem();
                         __syncwarp();
                         if (lane == 0) ptx::mbar_arrive(&b_full[bs]);
