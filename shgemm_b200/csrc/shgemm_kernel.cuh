@@ -634,18 +634,18 @@ __device__ __forceinline__ uint32_t sign_pair_word(uint32_t h, int i) {
     return ((h << (15 - i)) & 0x80008000u) | 0x3C003C00u;
 }
 
-// One k-step (64 k) of a generated B stage, rows j = t0, t0 + nthreads, ... < bn (columns
-// tn bn + j of the k x n block-sign operand): each row 64 binary16 values K-major in the
-// 128-byte-swizzled layout the TMA would have written (16-byte chunk q of row j at chunk
-// q ^ (j & 7)). Entries past n or past k are zero, as the TMA's out-of-range fill. Entry r of
-// the row is word r / 2 of the chunk sequence; word p = 4 q + e takes bits (p mod 16) and
-// (p mod 16) + 16 of 32-bit half p / 16 of the block's hash (block_sign_bit).
 // What the generator needs of a unit: its first B column, tile N, n, k and seed.
 struct GenB {
     uint64_t seed;
     int c0, bn, n, k;
 };
 
+// One k-step (64 k) of a generated B stage, rows j = t0, t0 + nthreads, ... < bn (columns
+// c0 + j of the k x n block-sign operand): each row 64 binary16 values K-major in the
+// 128-byte-swizzled layout the TMA would have written (16-byte chunk q of row j at chunk
+// q ^ (j & 7)). Entries past n or past k are zero, as the TMA's out-of-range fill. Entry r of
+// the row is word r / 2 of the chunk sequence; word p = 4 q + e takes bits (p mod 16) and
+// (p mod 16) + 16 of 32-bit half p / 16 of the block's hash (block_sign_bit).
 __device__ __forceinline__ void gen_b_rows(uint8_t* stage, const GenB& ud, int st, int t0, int nthreads) {
     const int c0 = ud.c0;
     const int kvalid = ud.k - st * 64;  // >= 1 on every step of the range
@@ -677,8 +677,8 @@ __device__ __forceinline__ void gen_b_rows(uint8_t* stage, const GenB& ud, int s
 
 // GEN_B (grouped binary16 launches with a K-major B): problems may ask for their B to be
 // generated (block-sign Rademacher) instead of loaded. The split warps write those B stages,
-// spread over their 192 threads, after their share of the A split; the TMA producer skips
-// them. A B stage then completes on the split warps' arrivals (one per warp) or on the
+// spread over their 192 threads, before they wait for the same k-step's A; the TMA producer
+// skips them. A B stage then completes on the split warps' arrivals (one per warp) or on the
 // producer's TMA (expect_tx plus the same number of arrivals).
 template <int TC, int BN, bool A_KMAJOR, bool B_KMAJOR, bool B_WIDE, bool GEN_B, class Params>
 __device__ __forceinline__ void tile_kernel_body(const Params& p) {
