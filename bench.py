@@ -1150,6 +1150,7 @@ def run_reference_arm(args, wl):
             "cpu_baseline": {"value": value, "unit": "TFLOP/s", "cores": oracle.num_threads(), "kind": "port",
                              "sample": desc},
             "e2e": {"value": value, "unit": "TFLOP/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "same_sample_as_cpu_baseline": served,
             "note": "reference not buildable (wmma_extension/cutf submodules absent); its algorithm is timed "
                     "through the oracle port"}
     print(json.dumps(line), flush=True)
