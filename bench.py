@@ -75,6 +75,8 @@ WORKLOADS = {
     "sketch": dict(m=4096, n=256, k=1 << 20, op_a=1, op_b=0, tc=0, alpha=1.0, beta=0.0, dist="sketch",
                    desc="left sketch Y = Omega^T A, A 2^20 x 4096 FP32 (low rank + noise), Omega 2^20 x 256 "
                         "binary16 N(0,1/256), split-K, fp16 compute", op_c=1, bound="hbm"),
+    "sketch_tf32": dict(m=4096, n=256, k=1 << 20, op_a=1, op_b=0, tc=1, alpha=1.0, beta=0.0, dist="sketch",
+                        desc="left sketch Y = Omega^T A as the binary16 sketch, tf32 compute", op_c=1, bound="hbm"),
     # the sketch at 1/8 of its length (A 2 GiB, still 16x L2), for profiler captures
     "sketch128k": dict(m=4096, n=256, k=1 << 17, op_a=1, op_b=0, tc=0, alpha=1.0, beta=0.0, dist="sketch",
                        op_c=1, desc="left sketch Y = Omega^T A, A 2^17 x 4096 FP32 (low rank + noise), "
@@ -500,6 +502,12 @@ def square_case(args, wl, ctx, traffic_key, tf32_error=False, e2e=True):
         roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                     "traffic": None, "peak_kind": f"{peak_kind} HBM copy bandwidth",
                     "work_per_launch": f"A + B + C = {bytes_min:.4e} bytes (each operand read once)"}
+        # the issued tensor work against its own peak beside the bandwidth fraction: a sketch in
+        # TF32 (half the binary16 rate) can be tensor-bound
+        t_peak, t_label = tensor_peak(ms_total >= 100.0, wl["tc"])
+        t_ach = flops_issued / (ms_step * 1e-3) / 1e12
+        roofline["tensor"] = {"achieved": t_ach, "peak": t_peak, "unit": "TFLOP/s", "frac": t_ach / t_peak,
+                              "peak_kind": t_label}
     else:
         # burst peak for a short timed region, the power-capped sustained one for a long one
         peak, label = tensor_peak(ms_total >= 100.0, wl["tc"])

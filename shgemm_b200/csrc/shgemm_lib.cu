@@ -169,6 +169,12 @@ KernelEntry kernel_table(int tc, int bn, int ak, int bk) {
     return {nullptr, 0};
 }
 
+// TF32, 128 x 256 tiles, B widened to FP32 in the workspace (K-major).
+KernelEntry tile_wide_table(bool ak) {
+    if (ak) return {reinterpret_cast<void*>(&shgemm_tile_wide_kernel<true>), TileCfg<kTF32, 256, true, true, true>::SMEM_BYTES};
+    return {reinterpret_cast<void*>(&shgemm_tile_wide_kernel<false>), TileCfg<kTF32, 256, false, true, true>::SMEM_BYTES};
+}
+
 // Tensor-memory operand kernels (binary16 compute, 128 x 256 tiles, B K-major).
 template <bool AK, int KC, int SV>
 KernelEntry tm_entry() {
@@ -599,7 +605,7 @@ Plan plan_from_tuned(const shgemm_b200_tuned_config& t, size_t m, size_t n, size
 }
 
 Plan make_plan_for(int num_sms, int fixed_level, long long split_k, size_t m, size_t n, size_t k, int tc,
-                   size_t ws_bytes) {
+                   size_t ws_bytes, int force_bn = 0) {
     Plan p{};
     p.sv = -1;
     p.pair = -1;
@@ -619,6 +625,10 @@ Plan make_plan_for(int num_sms, int fixed_level, long long split_k, size_t m, si
     p.level = level;
     p.bn = level_bn(tc, level);
     if (n <= 64 && fixed_level == SHGEMM_LEVEL_AUTO) p.bn = 64;
+    if (force_bn) {  // a kernel with one tile shape (the widened-B TF32 kernel)
+        p.level = 1;
+        p.bn = force_bn;
+    }
     p.tiles_n = static_cast<int>((n + p.bn - 1) / p.bn);
     const long long tiles = static_cast<long long>(p.tiles_m) * p.tiles_n;
     // Split-K: deterministic slices when the tiles alone leave SMs idle and k is long;
@@ -734,6 +744,8 @@ int shgemm_b200_create(shgemm_b200_handle_t* out, int device) {
             }
     for (int ak = 0; ak < 2; ++ak) {
         KernelEntry e = tm2_kernel_table(ak != 0);
+        cudaFuncSetAttribute(e.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, e.smem);
+        e = tile_wide_table(ak != 0);
         cudaFuncSetAttribute(e.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, e.smem);
     }
     h->max_pairs = query_max_pairs(tm2_kernel_table(true), sms);
@@ -985,10 +997,26 @@ static int run_tiled(shgemm_b200_handle_t h, int op_a, int op_b, size_t m, size_
         pl = plan_with(splitk_bytes - bblk_bytes);
         if (pl.bn != 256) block_b = false;
     }
-    if (!block_b) pl = plan_with(splitk_bytes);
+    // TF32 compute with a K-major binary16 B and n > 128: when the workspace also holds B widened
+    // to FP32 (ahead of the split-K partials), B is widened once per call and the 128 x 256
+    // kernel loads it as the TF32 tile layout itself (the kernel that widens B tile by tile in
+    // its split warps runs at about a third of the rate). Split-K as usual.
+    const size_t ldw = (k + 3) / 4 * 4;
+    const size_t wide_bytes = (ldw * n * sizeof(float) + 255) / 256 * 256;
+    const bool wide_b = tc == kTF32 && b_kmajor && !force && h->tile_kernel == 0 &&
+                        h->fixed_level == SHGEMM_LEVEL_AUTO && n > 128 && splitk_bytes >= wide_bytes &&
+                        k <= static_cast<size_t>(INT32_MAX);
+    if (wide_b) {
+        group_m = static_cast<int>(h->group_m);
+        pl = make_plan_for(h->num_sms, h->fixed_level, h->split_k, m, n, k, tc, splitk_bytes - wide_bytes, 256);
+    } else if (!block_b) {
+        pl = plan_with(splitk_bytes);
+    }
     if (force) group_m = force->group_m;
-    float* part_ws = block_b ? splitk_ws + bblk_bytes / sizeof(float) : splitk_ws;
+    float* part_ws = block_b ? splitk_ws + bblk_bytes / sizeof(float)
+                             : wide_b ? splitk_ws + wide_bytes / sizeof(float) : splitk_ws;
     __half* b_blk = reinterpret_cast<__half*>(splitk_ws);
+    float* b_wide = splitk_ws;
     // binary16 compute with 128 x 256 tiles and a K-major B: the tensor-memory operand kernel,
     // in CTA pairs (256 x 256 tiles, SHGEMM_CFG_PAIR_TILES) when B is not re-laid out and the
     // drain chunk and ring are the defaults
@@ -1014,10 +1042,13 @@ static int run_tiled(shgemm_b200_handle_t h, int op_a, int op_b, size_t m, size_
         ok = make_tmap(&P.tmap_a, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, a, k, m, lda * 4, 32, 128,
                        CU_TENSOR_MAP_SWIZZLE_128B);
     else
-        ok = make_tmap(&P.tmap_a, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, a, m, k, lda * 4, use_tm ? 128 : a_mmajor_box(tc),
-                       bk, CU_TENSOR_MAP_SWIZZLE_NONE);
+        ok = make_tmap(&P.tmap_a, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, a, m, k, lda * 4,
+                       use_tm ? 128 : a_mmajor_box(tc, wide_b), bk, CU_TENSOR_MAP_SWIZZLE_NONE);
     if (!ok) return SHGEMM_STATUS_NOT_SUPPORTED;
-    if (tc == kFP16) {
+    if (wide_b) {  // [256 n][32 k] FP32 rows of 128 bytes: the TF32 tile layout
+        ok = make_tmap(&P.tmap_b, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, b_wide, k, n, ldw * 4, 32, 256,
+                       CU_TENSOR_MAP_SWIZZLE_128B);
+    } else if (tc == kFP16) {
         if (block_b)  // k-blocks {64 k, n columns, kblocks}: one 64 x 256 tile step is 32 KB contiguous
             ok = make_tmap_3d(&P.tmap_b, CU_TENSOR_MAP_DATA_TYPE_FLOAT16, b_blk, 64, n, kblocks, 128, n * 128, 64,
                               pl.bn, 1, CU_TENSOR_MAP_SWIZZLE_128B);
@@ -1065,6 +1096,7 @@ static int run_tiled(shgemm_b200_handle_t h, int op_a, int op_b, size_t m, size_
 
     const KernelEntry e = use_tm2 ? tm2_kernel_table(a_kmajor)
                           : use_tm ? tm_kernel_table(a_kmajor, kc, sv)
+                          : wide_b ? tile_wide_table(a_kmajor)
                                    : kernel_table(tc, pl.bn, a_kmajor, b_kmajor);
     const int threads = use_tm ? TmCfg<true, 1, 0>::NUM_THREADS : 512;
     if (!e.fn) return SHGEMM_STATUS_NOT_SUPPORTED;
@@ -1076,7 +1108,16 @@ static int run_tiled(shgemm_b200_handle_t h, int op_a, int op_b, size_t m, size_
                     "k_slices = %d, chunk_k = %d, grid = %d%s\n",
                     m, n, k, op_a == kOpN ? "N" : "T", op_b == kOpN ? "N" : "T", tc == kTF32 ? "TF32" : "FP16",
                     pl.level, pl.bn, pl.slices, use_tm ? 64 * kc : bk, grid,
-                    use_tm2 ? ", operands in TMEM, CTA pairs" : use_tm ? ", operands in TMEM" : "");
+                    use_tm2 ? ", operands in TMEM, CTA pairs" : use_tm ? ", operands in TMEM"
+                                                              : wide_b ? ", B widened to FP32" : "");
+    }
+    if (wide_b) {
+        const size_t total = k * n;
+        const int blocks = static_cast<int>(std::min<size_t>((total + 255) / 256, size_t(h->num_sms) * 16));
+        widen_b_kernel<<<blocks, 256, 0, h->stream>>>(static_cast<const __half*>(b), ldb, b_wide, ldw,
+                                                      static_cast<int>(k), static_cast<int>(n));
+        h->launches++;
+        if (launch_status() != SHGEMM_STATUS_OK) return SHGEMM_STATUS_LAUNCH_FAILED;
     }
     if (block_b) {
         const size_t total = kblocks * n * 8;
@@ -2295,10 +2336,11 @@ int noalloc_setup(int dev, NoAllocDevice*& out) {
                     }
                 }
         for (int ak = 0; ak < 2; ++ak) {
-            KernelEntry e = tm2_kernel_table(ak != 0);
-            if (cudaFuncSetAttribute(e.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, e.smem) != cudaSuccess) {
-                cudaGetLastError();
-                return SHGEMM_STATUS_NOT_SUPPORTED;
+            for (KernelEntry e : {tm2_kernel_table(ak != 0), tile_wide_table(ak != 0)}) {
+                if (cudaFuncSetAttribute(e.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, e.smem) != cudaSuccess) {
+                    cudaGetLastError();
+                    return SHGEMM_STATUS_NOT_SUPPORTED;
+                }
             }
         }
         d.num_sms = sms;
