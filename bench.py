@@ -379,8 +379,9 @@ def square_case(args, wl, ctx, traffic_key, tf32_error=False, e2e=True):
     h.set_config(sg.CFG_TM_STAGES, args.stages)
     h.set_config(sg.CFG_PAIR_TILES, args.pair)
     if (wl["tc"] == 1 or tf32_error) and wl["op_b"] == 0:
-        # room for the widened FP32 copy of B (the TF32 route that loads B unconverted)
-        h.set_workspace_size(max(64 << 20, n * ((k + 3) // 4 * 4) * 4 + (1 << 20)))
+        # room for the widened FP32 copy of B (the TF32 kernels that load B unconverted) and for
+        # split-K partials beside it
+        h.set_workspace_size(n * ((k + 3) // 4 * 4) * 4 + (64 << 20))
     if wl.get("lda_pad"):
         # room for the staged copy of A (aligned leading dimension) in one k-slab
         cols = k if wl["op_a"] == 0 else m

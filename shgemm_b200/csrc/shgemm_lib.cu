@@ -1003,12 +1003,29 @@ static int run_tiled(shgemm_b200_handle_t h, int op_a, int op_b, size_t m, size_
     // its split warps runs at about a third of the rate). Split-K as usual.
     const size_t ldw = (k + 3) / 4 * 4;
     const size_t wide_bytes = (ldw * n * sizeof(float) + 255) / 256 * 256;
-    const bool wide_b = tc == kTF32 && b_kmajor && !force && h->tile_kernel == 0 &&
+    bool wide_b = tc == kTF32 && b_kmajor && !force && h->tile_kernel == 0 &&
                         h->fixed_level == SHGEMM_LEVEL_AUTO && n > 128 && splitk_bytes >= wide_bytes &&
                         k <= static_cast<size_t>(INT32_MAX);
     if (wide_b) {
-        group_m = static_cast<int>(h->group_m);
-        pl = make_plan_for(h->num_sms, h->fixed_level, h->split_k, m, n, k, tc, splitk_bytes - wide_bytes, 256);
+        // taken when it keeps enough SMs busy: the widened-B kernel does a unit's work ~3x as fast,
+        // but the widened B leaves less room for split-K partials
+        const Plan pw = make_plan_for(h->num_sms, h->fixed_level, h->split_k, m, n, k, tc, splitk_bytes - wide_bytes,
+                                      256);
+        int gm_n = 8;
+        const Plan pn = make_plan(h, op_a, op_b, m, n, k, tc, splitk_bytes, &gm_n);
+        auto busy = [&](const Plan& q) {
+            const long long units = static_cast<long long>(q.tiles_m) * q.tiles_n * q.slices;
+            return units >= h->num_sms ? wave_efficiency(units, h->num_sms)
+                                       : static_cast<double>(units) / h->num_sms;
+        };
+        wide_b = 2.0 * busy(pw) >= busy(pn);
+        if (wide_b) {
+            group_m = static_cast<int>(h->group_m);
+            pl = pw;
+        } else {
+            group_m = gm_n;
+            pl = pn;
+        }
     } else if (!block_b) {
         pl = plan_with(splitk_bytes);
     }
