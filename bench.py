@@ -77,6 +77,8 @@ WORKLOADS = {
                         "binary16 N(0,1/256), split-K, fp16 compute", op_c=1, bound="hbm"),
     "sketch_tf32": dict(m=4096, n=256, k=1 << 20, op_a=1, op_b=0, tc=1, alpha=1.0, beta=0.0, dist="sketch",
                         desc="left sketch Y = Omega^T A as the binary16 sketch, tf32 compute", op_c=1, bound="hbm"),
+    "sketch128k_tf32": dict(m=4096, n=256, k=1 << 17, op_a=1, op_b=0, tc=1, alpha=1.0, beta=0.0, dist="sketch",
+                            op_c=1, desc="left sketch Y = Omega^T A at 2^17, tf32 compute", bound="hbm"),
     # the sketch at 1/8 of its length (A 2 GiB, still 16x L2), for profiler captures
     "sketch128k": dict(m=4096, n=256, k=1 << 17, op_a=1, op_b=0, tc=0, alpha=1.0, beta=0.0, dist="sketch",
                        op_c=1, desc="left sketch Y = Omega^T A, A 2^17 x 4096 FP32 (low rank + noise), "
