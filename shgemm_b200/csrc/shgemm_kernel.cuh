@@ -81,8 +81,9 @@ struct alignas(64) TileGemmParams {
     // Tensor-memory kernel: every FP32 tile is read by one unit only (a single tile column),
     // so its loads carry an evict-first L2 hint and leave L2 to the shared binary16 tiles.
     int a_read_once;
-    // Tensor-memory kernel: tmap_b is a 3-D view {64 k, n, k / 64} of the binary16 operand
-    // re-laid out as contiguous k-blocks; a step loads box (0, 256 tn, step).
+    // tmap_b is a 3-D view {BK, n, k / BK} of B re-laid out as contiguous k-blocks (the
+    // binary16 operand for the tensor-memory kernel, BK = 64; the widened FP32 operand for
+    // the widened-B TF32 kernel, BK = 32); a step loads box (0, bn tn, step).
     int b_blocked;
 };
 
@@ -270,6 +271,8 @@ __device__ __forceinline__ void get_unit(const GroupedParams& p, int u, UnitDesc
 __device__ __forceinline__ int unit_count(const TileGemmParams& p) { return p.num_units; }
 __device__ __forceinline__ int unit_count(const GroupedParams& p) { return *p.num_units; }
 __device__ __forceinline__ int output_op(const TileGemmParams& p) { return p.op_c; }
+__device__ __forceinline__ bool b_blocked(const TileGemmParams& p) { return p.b_blocked != 0; }
+__device__ __forceinline__ bool b_blocked(const GroupedParams&) { return false; }
 __device__ __forceinline__ int output_op(const GroupedParams& p) { return p.op_c; }
 __device__ __forceinline__ void prefetch_params_maps(const TileGemmParams& p) {
     ptx::tma_prefetch_desc(&p.tmap_a);
@@ -818,7 +821,10 @@ __device__ __forceinline__ void tile_kernel_body(const Params& p) {
                         ptx::mbar_arrive_expect_tx(&b_full[bs], ud.bn * Cfg::BK * (B_WIDE ? 4 : 2));
                         if constexpr (GEN_B) ptx::mbar_arrive_n(&b_full[bs], kBFullCount - 1);
                         if constexpr (B_KMAJOR) {
-                            ptx::tma_load_2d(b_dst, ud.tmap_b, &b_full[bs], kc, tn * ud.bn);
+                            if (b_blocked(p))  // k-blocks: {k within the block, column, block}
+                                ptx::tma_load_3d(b_dst, ud.tmap_b, &b_full[bs], 0, tn * ud.bn, st);
+                            else
+                                ptx::tma_load_2d(b_dst, ud.tmap_b, &b_full[bs], kc, tn * ud.bn);
                         } else if constexpr (!kTf32) {
 #pragma unroll
                             for (int sub = 0; sub < BN / 64; ++sub)

@@ -296,6 +296,24 @@ __global__ void widen_b_kernel(const __half* __restrict__ src, uint64_t ldb, flo
     }
 }
 
+// Widens a k x n binary16 K-contiguous operand to FP32 laid out as k-blocks of 32:
+// dst[(kb * n + col) * 32 + j] = src[col * ldb + 32 kb + j], zero where 32 kb + j >= k. One
+// 32-deep TF32 step of a 256-column tile is then one contiguous 32 KB run (FP32 columns 4 MB
+// apart would put each of the tile's columns on a page of its own, as with block_b_kernel).
+__global__ void widen_b_blocked_kernel(const __half* __restrict__ src, uint64_t ldb, float* __restrict__ dst, int k,
+                                       int n, int kblocks) {
+    const size_t total = static_cast<size_t>(n) * kblocks * 32;
+    for (size_t idx = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; idx < total;
+         idx += static_cast<size_t>(gridDim.x) * blockDim.x) {
+        const int j = static_cast<int>(idx & 31);
+        const size_t rest = idx >> 5;
+        const int col = static_cast<int>(rest % n);
+        const size_t kb = rest / n;
+        const size_t r = kb * 32 + j;
+        dst[idx] = r < static_cast<size_t>(k) ? __half2float(src[static_cast<size_t>(col) * ldb + r]) : 0.0f;
+    }
+}
+
 // Re-lays a k x n binary16 K-contiguous operand (leading dimension ldb, 16-byte aligned
 // columns) out as k-blocks: dst[(kb * n + col) * 64 + j] = src[col * ldb + 64 kb + j], zero
 // where 64 kb + j >= k. One 64-deep step of a 256-column tile is then one contiguous 32 KB
@@ -1001,11 +1019,11 @@ static int run_tiled(shgemm_b200_handle_t h, int op_a, int op_b, size_t m, size_
     // to FP32 (ahead of the split-K partials), B is widened once per call and the 128 x 256
     // kernel loads it as the TF32 tile layout itself (the kernel that widens B tile by tile in
     // its split warps runs at about a third of the rate). Split-K as usual.
-    const size_t ldw = (k + 3) / 4 * 4;
-    const size_t wide_bytes = (ldw * n * sizeof(float) + 255) / 256 * 256;
+    const size_t wkb = (k + 31) / 32;  // k-blocks of the widened B
+    const size_t wide_bytes = (wkb * 32 * n * sizeof(float) + 255) / 256 * 256;
     bool wide_b = tc == kTF32 && b_kmajor && !force && h->tile_kernel == 0 &&
                         h->fixed_level == SHGEMM_LEVEL_AUTO && n > 128 && splitk_bytes >= wide_bytes &&
-                        k <= static_cast<size_t>(INT32_MAX);
+                        k <= static_cast<size_t>(INT32_MAX) && wkb * n < (size_t(1) << 31);
     if (wide_b) {
         // taken when it keeps enough SMs busy: the widened-B kernel does a unit's work ~3x as fast,
         // but the widened B leaves less room for split-K partials
@@ -1062,9 +1080,9 @@ static int run_tiled(shgemm_b200_handle_t h, int op_a, int op_b, size_t m, size_
         ok = make_tmap(&P.tmap_a, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, a, m, k, lda * 4,
                        use_tm ? 128 : a_mmajor_box(tc, wide_b), bk, CU_TENSOR_MAP_SWIZZLE_NONE);
     if (!ok) return SHGEMM_STATUS_NOT_SUPPORTED;
-    if (wide_b) {  // [256 n][32 k] FP32 rows of 128 bytes: the TF32 tile layout
-        ok = make_tmap(&P.tmap_b, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, b_wide, k, n, ldw * 4, 32, 256,
-                       CU_TENSOR_MAP_SWIZZLE_128B);
+    if (wide_b) {  // k-blocks {32 k, n columns, kblocks}: a [256 n][32 k] box is the TF32 tile layout
+        ok = make_tmap_3d(&P.tmap_b, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, b_wide, 32, n, wkb, 128, n * 128, 32, 256, 1,
+                          CU_TENSOR_MAP_SWIZZLE_128B);
     } else if (tc == kFP16) {
         if (block_b)  // k-blocks {64 k, n columns, kblocks}: one 64 x 256 tile step is 32 KB contiguous
             ok = make_tmap_3d(&P.tmap_b, CU_TENSOR_MAP_DATA_TYPE_FLOAT16, b_blk, 64, n, kblocks, 128, n * 128, 64,
@@ -1105,7 +1123,7 @@ static int run_tiled(shgemm_b200_handle_t h, int op_a, int op_b, size_t m, size_
     P.num_units = pl.tiles_m * pl.tiles_n * pl.slices;
     P.group_m = group_m;
     P.a_read_once = use_tm && !use_tm2 && pl.tiles_n == 1;
-    P.b_blocked = block_b ? 1 : 0;
+    P.b_blocked = (block_b || wide_b) ? 1 : 0;
     if (use_tm2) {  // pair tiles of 256 rows
         P.tiles_m = static_cast<int>((m + 255) / 256);
         P.num_units = P.tiles_m * pl.tiles_n * pl.slices;
@@ -1129,10 +1147,11 @@ static int run_tiled(shgemm_b200_handle_t h, int op_a, int op_b, size_t m, size_
                                                               : wide_b ? ", B widened to FP32" : "");
     }
     if (wide_b) {
-        const size_t total = k * n;
+        const size_t total = wkb * 32 * n;
         const int blocks = static_cast<int>(std::min<size_t>((total + 255) / 256, size_t(h->num_sms) * 16));
-        widen_b_kernel<<<blocks, 256, 0, h->stream>>>(static_cast<const __half*>(b), ldb, b_wide, ldw,
-                                                      static_cast<int>(k), static_cast<int>(n));
+        widen_b_blocked_kernel<<<blocks, 256, 0, h->stream>>>(static_cast<const __half*>(b), ldb, b_wide,
+                                                              static_cast<int>(k), static_cast<int>(n),
+                                                              static_cast<int>(wkb));
         h->launches++;
         if (launch_status() != SHGEMM_STATUS_OK) return SHGEMM_STATUS_LAUNCH_FAILED;
     }
