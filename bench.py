@@ -1200,6 +1200,9 @@ def served_line(args, wl, ctx, s, cpu):
         "speedup_vs_per_call_per_request": s["value"] / pc["per_request"]["value"],
         "saturation_speedup_vs_per_call": s["saturation"]["value"] / pc["per_draw"]["value"],
         "saturation_speedup_vs_per_call_per_request": s["saturation"]["value"] / pc["per_request"]["value"],
+        "speedup_note": ("the stream is arrival-bound (served = offered load while the server keeps up), and the "
+                         "per-call loops run the same requests back to back: the stream ratios set an arrival "
+                         "rate against a capacity; the saturation ratios compare capacities"),
         "issued_tflops": 2 * s["value"],
         "gpu_launches": s["gpu_launches"],
         "roofline": s["roofline"],
