@@ -184,6 +184,9 @@ struct alignas(64) GroupedParams {
     // alpha and beta), read once by each epilogue warp when the kernel starts.
     const float* alpha_dev;
     const float* beta_dev;
+    // The next unit to hand out after each CTA's first (blockIdx.x): a counter in device
+    // memory, zeroed by the table copy that precedes every launch (and every graph replay).
+    int* next_unit;
 };
 
 // What one work unit (a 128 x bn tile of one problem over a range of k-steps) needs.
@@ -270,6 +273,20 @@ __device__ __forceinline__ void get_unit(const GroupedParams& p, int u, UnitDesc
 
 __device__ __forceinline__ int unit_count(const TileGemmParams& p) { return p.num_units; }
 __device__ __forceinline__ int unit_count(const GroupedParams& p) { return *p.num_units; }
+
+// The k-th unit (k = 0, 1, ...) a CTA works on, or -1 when none is left. A single problem's
+// units are uniform: CTA b takes b, b + gridDim.x, ... Grouped units are uneven (their k and
+// tile N differ): after its first unit a CTA takes the next one from a device counter when
+// its producer is ready for it, so the units balance by their actual time rather than by an
+// estimate (the list is still longest first).
+__device__ __forceinline__ int claim_unit(const TileGemmParams& p, int k) {
+    const long long u = blockIdx.x + static_cast<long long>(k) * gridDim.x;
+    return u < p.num_units ? static_cast<int>(u) : -1;
+}
+__device__ __forceinline__ int claim_unit(const GroupedParams& p, int k) {
+    const int u = k == 0 ? static_cast<int>(blockIdx.x) : static_cast<int>(gridDim.x) + atomicAdd(p.next_unit, 1);
+    return u < *p.num_units ? u : -1;
+}
 __device__ __forceinline__ int output_op(const TileGemmParams& p) { return p.op_c; }
 __device__ __forceinline__ bool b_blocked(const TileGemmParams& p) { return p.b_blocked != 0; }
 __device__ __forceinline__ bool b_blocked(const GroupedParams&) { return false; }
@@ -712,7 +729,13 @@ __device__ __forceinline__ void tile_kernel_body(const Params& p) {
     volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
     // per split warp: the current unit's generator parameters, past the barriers
     GenB* gen_slots = reinterpret_cast<GenB*>(reinterpret_cast<uint8_t*>(bars) + 512);
-    static_assert((4 * SA + 2 * SB + 5) * 8 + 8 <= 512 && 512 + 8 * sizeof(GenB) <= Cfg::BAR_BYTES,
+    // the producer claims each unit and hands it to the other roles through a 4-slot ring
+    int* unit_ring = reinterpret_cast<int*>(reinterpret_cast<uint8_t*>(bars) + 768);
+    uint64_t* unit_full = reinterpret_cast<uint64_t*>(reinterpret_cast<uint8_t*>(bars) + 800);
+    uint64_t* unit_empty = unit_full + 4;
+    constexpr uint32_t kUnitReaders = 1 + NSPLIT + 8;  // MMA issuer, split warps, epilogue warps
+    static_assert((4 * SA + 2 * SB + 5) * 8 + 8 <= 512 && 512 + 8 * sizeof(GenB) <= 768 &&
+                      800 + 8 * 8 <= Cfg::BAR_BYTES,
                   "barrier region");
     constexpr uint32_t kBFullCount = GEN_B ? NSPLIT : 1;
 
@@ -735,6 +758,10 @@ __device__ __forceinline__ void tile_kernel_body(const Params& p) {
             ptx::mbar_init(&d_empty[b], 8);
         }
         ptx::mbar_init(drain_bar, 1);
+        for (int r = 0; r < 4; ++r) {
+            ptx::mbar_init(&unit_full[r], 1);
+            ptx::mbar_init(&unit_empty[r], kUnitReaders);
+        }
         *abort_flag = 0;
         ptx::fence_mbarrier_init();
     }
@@ -747,12 +774,18 @@ __device__ __forceinline__ void tile_kernel_body(const Params& p) {
     ptx::tc_fence_after();
     const uint32_t tmem_base = *tmem_slot;
 
-    const int num_units = unit_count(p);
     const uint64_t limit = p.wait_limit_ns;
 
     auto fail = [&](int code) {
         *abort_flag = 1;
         atomicCAS(p.error_flag, 0, code);
+    };
+    // the k-th unit from the producer's ring (false: the wait ran out); the caller then
+    // releases the slot (one arrival per reading warp)
+    auto take_unit = [&](int k, int& u) -> bool {
+        if (!ptx::mbar_wait(&unit_full[k & 3], (k >> 2) & 1, abort_flag, limit)) return false;
+        u = unit_ring[k & 3];
+        return true;
     };
 
     // Warpgroups 0-1 (producer, MMA, split) give registers to warpgroups 2-3 (epilogue).
@@ -764,7 +797,16 @@ __device__ __forceinline__ void tile_kernel_body(const Params& p) {
             int as = 0, bs = 0;
             uint32_t aph = 0, bph = 0;
             uint32_t a_issued = 0, a_par = 0, b_issued = 0, b_par = 0;  // per stage: load in flight, its parity
-            for (int u = blockIdx.x; u < num_units; u += gridDim.x) {
+            for (int uk = 0;; ++uk) {
+                // claim the next unit and hand it to the other roles
+                if (!ptx::mbar_wait(&unit_empty[uk & 3], ((uk >> 2) & 1) ^ 1u, abort_flag, limit)) {
+                    fail(kErrProducerTimeout);
+                    goto producer_done;
+                }
+                const int u = claim_unit(p, uk);
+                unit_ring[uk & 3] = u;
+                ptx::mbar_arrive(&unit_full[uk & 3]);
+                if (u < 0) break;
                 UnitDesc ud;
                 get_unit<Cfg>(p, u, ud);
                 const int tm = ud.tm, tn = ud.tn, s0 = ud.s0, s1 = ud.s1;
@@ -867,7 +909,14 @@ __device__ __forceinline__ void tile_kernel_body(const Params& p) {
             int as = 0, bs = 0;
             uint32_t aph = 0, bph = 0, gc = 0;
             bool issued_any = false;
-            for (int u = blockIdx.x; u < num_units; u += gridDim.x) {
+            for (int uk = 0;; ++uk) {
+                int u;
+                if (!take_unit(uk, u)) {
+                    fail(kErrMmaTimeout);
+                    goto mma_done;
+                }
+                ptx::mbar_arrive(&unit_empty[uk & 3]);
+                if (u < 0) break;
                 UnitDesc ud;
                 get_unit<Cfg>(p, u, ud);
                 const int nsteps = ud.s1 - ud.s0;
@@ -969,7 +1018,15 @@ __device__ __forceinline__ void tile_kernel_body(const Params& p) {
         // binary16: global item g of this CTA's item sequence goes to split warp g % SPLIT_WARPS;
         // `first` is this warp's first item of the current stage.
         int first = warp - 2;
-        for (int u = blockIdx.x; u < num_units; u += gridDim.x) {
+        for (int uk = 0;; ++uk) {
+            int u;
+            if (!take_unit(uk, u)) {
+                fail(kErrSplitTimeout);
+                goto split_done;
+            }
+            __syncwarp();
+            if (lane == 0) ptx::mbar_arrive(&unit_empty[uk & 3]);
+            if (u < 0) break;
             UnitDesc ud;
             get_unit<Cfg>(p, u, ud);
             if constexpr (GEN_B) {
@@ -1047,7 +1104,15 @@ __device__ __forceinline__ void tile_kernel_body(const Params& p) {
         const int row_in_tile = q * 32 + lane;
         const uint32_t lane_addr = static_cast<uint32_t>(q * 32) << 16;
         uint32_t gc = 0;
-        for (int u = blockIdx.x; u < num_units; u += gridDim.x) {
+        for (int uk = 0;; ++uk) {
+            int u;
+            if (!take_unit(uk, u)) {
+                fail(kErrEpilogueTimeout);
+                goto epi_done;
+            }
+            __syncwarp();
+            if (lane == 0) ptx::mbar_arrive(&unit_empty[uk & 3]);
+            if (u < 0) break;
             int nsteps, hn;
             {
                 UnitDesc ud;

@@ -2107,6 +2107,7 @@ int grouped_stage(shgemm_b200_handle_t h, GroupedTable& t, bool b_wide, int op_a
     std::stable_sort(list.begin(), list.end(), [](const Cost& x, const Cost& y) { return x.cost > y.cost; });
     for (size_t u = 0; u < list.size(); ++u) units[u] = list[u].unit;
     *reinterpret_cast<int*>(host + t.count_off) = static_cast<int>(list.size());
+    *reinterpret_cast<int*>(host + t.count_off + sizeof(int)) = 0;  // the launch's unit counter
     t.tc = tc;
     t.b32 = b_wide ? 1 : 0;
     t.op_a = op_a;
@@ -2122,12 +2123,13 @@ static int grouped_run(shgemm_b200_handle_t h, GroupedTable& t, bool b_wide, int
                        const shgemm_b200_problem* probs, int count, DevScalars dev) {
     const int st = grouped_stage(h, t, b_wide, op_a, op_b, tc, op_c, probs, count);
     if (st != SHGEMM_STATUS_OK) return st;
-    // problems, units and count in two copies from the pinned staging (the tables are
-    // fixed-offset so a captured graph replays with whatever the staging holds)
+    // problems, units, count and a zeroed unit counter in two copies from the pinned staging
+    // (the tables are fixed-offset so a captured graph replays with whatever the staging holds,
+    // and each replay starts its counter from zero)
     if (cudaMemcpyAsync(t.dev, t.host, sizeof(GroupedProblem) * static_cast<size_t>(count), cudaMemcpyHostToDevice,
                         h->stream) != cudaSuccess ||
         cudaMemcpyAsync(static_cast<uint8_t*>(t.dev) + t.units_off, static_cast<uint8_t*>(t.host) + t.units_off,
-                        t.count_off + sizeof(int) - t.units_off, cudaMemcpyHostToDevice, h->stream) != cudaSuccess)
+                        t.count_off + 2 * sizeof(int) - t.units_off, cudaMemcpyHostToDevice, h->stream) != cudaSuccess)
         return SHGEMM_STATUS_CUDA_ERROR;
     t.copied_count = count;
     cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
@@ -2138,6 +2140,7 @@ static int grouped_run(shgemm_b200_handle_t h, GroupedTable& t, bool b_wide, int
     P.problems = static_cast<const GroupedProblem*>(t.dev);
     P.units = reinterpret_cast<const int2*>(static_cast<uint8_t*>(t.dev) + t.units_off);
     P.num_units = reinterpret_cast<const int*>(static_cast<uint8_t*>(t.dev) + t.count_off);
+    P.next_unit = reinterpret_cast<int*>(static_cast<uint8_t*>(t.dev) + t.count_off + sizeof(int));
     P.error_flag = h->error_word;
     P.wait_limit_ns = static_cast<uint64_t>(h->wait_limit_ms) * 1000000ull;
     P.op_c = op_c;
