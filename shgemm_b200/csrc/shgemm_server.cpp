@@ -93,7 +93,6 @@ class Arena {
 
 struct Request {
     unsigned long long ticket = 0;
-    int units = 0;  // output tiles of the grouped launch
     shgemm_b200_sketch_request r{};
     int state = SHGEMM_REQ_QUEUED;
     Clock::time_point t_submit, t_done;
@@ -101,6 +100,19 @@ struct Request {
     size_t om_off = Arena::kNone, y_off = Arena::kNone;
     size_t ldb = 0;  // Omega leading dimension (elements)
     bool y_held = false;
+    // Large requests run as row chunks in successive launches, one chunk in flight at a time,
+    // so that requests arriving behind them share the next launch instead of waiting for all
+    // of them (Omega is generated with the first chunk; later chunks launch after it completed).
+    size_t row_next = 0;   // rows handed to launches
+    size_t rows_done = 0;  // rows whose launches completed
+    bool in_flight = false;
+    bool omega_made = false;
+};
+
+// One launch's share of a request: rows [row0, row0 + rows) of its Y.
+struct Piece {
+    std::shared_ptr<Request> q;
+    size_t row0 = 0, rows = 0;
 };
 
 struct Slot {
@@ -109,7 +121,7 @@ struct Slot {
     // batch start, Omega generated (grouped launch starts), batch done: timing events
     cudaEvent_t start = nullptr, mid = nullptr, done = nullptr;
     bool busy = false;
-    std::vector<std::shared_ptr<Request>> reqs;
+    std::vector<Piece> pieces;
 };
 
 }  // namespace
@@ -168,14 +180,28 @@ void fill_sizes(const shgemm_b200_server& s, Request& q) {
     q.a_bytes = q.r.lda * q.r.k * sizeof(float);
     q.om_bytes = std::max<size_t>(1, q.ldb * cols * e);
     q.y_bytes = std::max<size_t>(1, q.r.m * cols * sizeof(float));
-    // tiles the grouped launch makes of it (tile N: power of two in [32, 256])
-    size_t bn = 32;
-    while (bn < 256 && bn < cols) bn *= 2;
-    const size_t units = ((q.r.m + 127) / 128) * ((cols + bn - 1) / bn);
-    q.units = static_cast<int>(std::min<size_t>(units, size_t(1) << 30));
 }
 
 constexpr int kMaxUnitsPerLaunch = 1 << 16;
+// Work of one chunk of a large request, 2 m n k: ~1.6 ms on a B200 in TF32.
+constexpr double kChunkFlops = 4e11;
+
+// Rows of the next chunk of q: all that is left, or a multiple of 128 near kChunkFlops.
+size_t chunk_rows(const Request& q) {
+    const size_t left = q.r.m - q.row_next;
+    const double per_row = 2.0 * static_cast<double>(q.r.n) * q.r.draws * static_cast<double>(q.r.k);
+    size_t rows = static_cast<size_t>(kChunkFlops / per_row) / 128 * 128;
+    rows = std::max<size_t>(rows, 128);
+    return rows >= left ? left : rows;
+}
+
+// Tiles a launch makes of `rows` rows of q (tile N: power of two in [32, 256]).
+int piece_units(const Request& q, size_t rows) {
+    const size_t cols = q.r.n * static_cast<size_t>(q.r.draws);
+    size_t bn = 32;
+    while (bn < 256 && bn < cols) bn *= 2;
+    return static_cast<int>(std::min<size_t>(((rows + 127) / 128) * ((cols + bn - 1) / bn), size_t(1) << 30));
+}
 
 }  // namespace
 
@@ -209,42 +235,55 @@ bool shgemm_b200_server::launch_locked(Slot& s) {
     const int tc = cfg.compute_type;
     const int fp32 = tc == SHGEMM_TC_TF32 ? 1 : 0;
     std::vector<shgemm_b200_problem> probs;
-    s.reqs.clear();
-    int units = 0;
-    while (!ready.empty() && static_cast<int>(s.reqs.size()) < cfg.max_batch &&
-           units + ready.front()->units <= kMaxUnitsPerLaunch) {
-        units += ready.front()->units;
-        s.reqs.push_back(ready.front());
-        ready.pop_front();
-    }
-    if (s.reqs.empty()) return false;
-    bool ok = cudaEventRecord(s.start, s.stream) == cudaSuccess;
     std::vector<shgemm_b200_omega_job> jobs;
-    for (auto& qp : s.reqs) {
-        Request& q = *qp;
+    s.pieces.clear();
+    int units = 0;
+    // first come first served, one chunk per request (requests with a chunk in flight wait)
+    for (auto it = ready.begin(); it != ready.end() && static_cast<int>(s.pieces.size()) < cfg.max_batch;) {
+        Request& q = **it;
+        if (q.in_flight) {
+            ++it;
+            continue;
+        }
+        const size_t rows = chunk_rows(q);
+        const int pu = piece_units(q, rows);
+        if (!s.pieces.empty() && units + pu > kMaxUnitsPerLaunch) break;
+        units += pu;
+        s.pieces.push_back({*it, q.row_next, rows});
+        q.in_flight = true;
         q.state = SHGEMM_REQ_RUNNING;
         const size_t cols = q.r.n * static_cast<size_t>(q.r.draws);
-        // draw j of Omega from (seed, j): column block j of the k x (draws n) operand
-        for (int j = 0; j < q.r.draws; ++j) {
-            uint8_t* dst = arena.ptr(q.om_off) + static_cast<size_t>(j) * q.r.n * q.ldb * omega_elem(*this);
-            jobs.push_back({dst, q.ldb, q.r.k, q.r.n,
-                            q.r.omega_seed * 0x100000001B3ull + static_cast<unsigned long long>(j), q.r.omega_scale,
-                            q.r.omega_dist});
+        if (!q.omega_made) {
+            // draw j of Omega from (seed, j): column block j of the k x (draws n) operand
+            for (int j = 0; j < q.r.draws; ++j) {
+                uint8_t* dst = arena.ptr(q.om_off) + static_cast<size_t>(j) * q.r.n * q.ldb * omega_elem(*this);
+                jobs.push_back({dst, q.ldb, q.r.k, q.r.n,
+                                q.r.omega_seed * 0x100000001B3ull + static_cast<unsigned long long>(j),
+                                q.r.omega_scale, q.r.omega_dist});
+            }
+            q.omega_made = true;
         }
         shgemm_b200_problem p{};
-        p.m = q.r.m;
+        p.m = rows;
         p.n = cols;
         p.k = q.r.k;
-        p.a = q.r.a;
+        p.a = q.r.a + q.row_next;  // rows row_next .. of the column-major A (128-row aligned)
         p.lda = q.r.lda;
         p.b = arena.ptr(q.om_off);
         p.ldb = q.ldb;
-        p.c = reinterpret_cast<float*>(arena.ptr(q.y_off));
+        p.c = reinterpret_cast<float*>(arena.ptr(q.y_off)) + q.row_next;
         p.ldc = std::max<size_t>(1, q.r.m);
         p.alpha = 1.0f;
         p.beta = 0.0f;
         probs.push_back(p);
+        q.row_next += rows;
+        if (q.row_next >= q.r.m)
+            it = ready.erase(it);  // every row handed out
+        else
+            ++it;
     }
+    if (s.pieces.empty()) return false;
+    bool ok = cudaEventRecord(s.start, s.stream) == cudaSuccess;
     // every draw of the batch in one launch (per 64 draws)
     ok = ok && shgemm_b200_generate_omega_batch(s.stream, jobs.data(), static_cast<int>(jobs.size()), fp32) ==
                    SHGEMM_STATUS_OK;
@@ -276,8 +315,16 @@ bool shgemm_b200_server::complete_locked(Slot& s, bool ok) {
             cudaGetLastError();
         }
     }
-    for (auto& qp : s.reqs) {
-        Request& q = *qp;
+    for (auto& pc : s.pieces) {
+        Request& q = *pc.q;
+        q.in_flight = false;
+        if (q.state != SHGEMM_REQ_RUNNING) continue;  // an earlier chunk failed it
+        q.rows_done += pc.rows;
+        if (ok && q.rows_done < q.r.m) continue;  // more chunks to come
+        if (!ok && q.row_next < q.r.m) {           // drop its remaining chunks
+            auto it = std::find(ready.begin(), ready.end(), pc.q);
+            if (it != ready.end()) ready.erase(it);
+        }
         arena.release(q.om_off, q.om_bytes);
         resident -= q.a_bytes + round_up(q.om_bytes);
         q.t_done = now;
@@ -294,7 +341,7 @@ bool shgemm_b200_server::complete_locked(Slot& s, bool ok) {
         if (cfg.auto_release || !ok) release_y_locked(q);  // else Y stays resident until released
         --n_unfinished;
     }
-    s.reqs.clear();
+    s.pieces.clear();
     s.busy = false;
     cv_done.notify_all();
     return true;
@@ -437,7 +484,7 @@ int shgemm_b200_server_submit(shgemm_b200_server_t s, const shgemm_b200_sketch_r
     auto q = std::make_shared<Request>();
     q->r = *r;
     fill_sizes(*s, *q);
-    if (q->units > kMaxUnitsPerLaunch) return SHGEMM_STATUS_NOT_SUPPORTED;
+    if (piece_units(*q, chunk_rows(*q)) > kMaxUnitsPerLaunch) return SHGEMM_STATUS_NOT_SUPPORTED;
     const size_t need = q->a_bytes + round_up(q->om_bytes) + round_up(q->y_bytes);
     if (need > s->cfg.hbm_budget_bytes || round_up(q->om_bytes) + round_up(q->y_bytes) > s->arena.size())
         return SHGEMM_STATUS_NOT_SUPPORTED;

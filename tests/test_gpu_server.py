@@ -241,3 +241,44 @@ def test_server_poisson_stream(cuda_device):
     assert st["completed"] == 120 and st["failed"] == 0
     assert st["batches"] >= 2
     assert st["p99_ms"] >= st["p50_ms"] > 0
+
+
+def test_large_request_runs_in_chunks_and_small_ones_pass_it(cuda_device):
+    """A request of ~2.2e12 flops runs as row chunks in successive launches (one in flight):
+    a small request submitted right behind it completes first, and the large one's rows on
+    both sides of every chunk boundary match the restated reference algorithm."""
+    import torch
+
+    from shgemm_b200 import server as srv
+
+    m, n, k, draws, seed = 65536, 256, 16384, 4, 77
+    g = torch.Generator(device="cuda")
+    g.manual_seed(5)
+    A_dev = torch.randn(k * m, generator=g, device="cuda")  # column-major m x k, lda = m
+    small_m, small_k = 1024, 1024
+    S_dev = torch.randn(small_k * small_m, generator=g, device="cuda")
+    with srv.SketchServer(0, hbm_budget_bytes=16 << 30, compute_type=oracle.TF32) as s:
+        tb = s.submit(m, n, k, A_dev, m, draws=draws, seed=seed)
+        ts = s.submit(small_m, 64, small_k, S_dev, small_m, draws=draws, seed=seed + 1)
+        assert s.wait(ts) == srv.DONE and s.wait(tb) == srv.DONE
+        _, _, _, lat_small = s.poll(ts)
+        st, y, ldy, lat_big = s.poll(tb)
+        assert st == srv.DONE and ldy == m
+        assert lat_small < lat_big  # the small request did not wait for all of the large one
+        cols = n * draws
+        chunk = int(4e11 / (2.0 * cols * k)) // 128 * 128
+        rows = sorted({0, 1, m - 1} | {b + d for b in range(chunk, m, chunk) for d in (-1, 0)})
+        Y = _view(y, m * cols).view(cols, m)[:, rows].T.contiguous().cpu().numpy()  # len(rows) x cols
+        s.release(tb)
+        s.release(ts)
+    r = len(rows)
+    A_rows = A_dev.view(k, m)[:, rows].contiguous().cpu().numpy().reshape(-1)  # r x k column-major, ld = r
+    del A_dev, S_dev
+    for j in range(draws):
+        om16, _ = _omega_host(k, n, srv.draw_seed(seed, j), True, n ** -0.5)
+        inp = dict(A=A_rows, B=om16.reshape(-1), C=np.zeros(r * n, np.float32), lda=r, ldb=k, ldc=r)
+        gpu = Y[:, j * n:(j + 1) * n].T.reshape(-1).copy()  # r x n column-major
+        orc = K.run_oracle(oracle.TF32, 0, 0, r, n, k, 1.0, inp, 0.0, 0, chunk=0)
+        ref = K.fp64(0, 0, r, n, k, 1.0, inp, 0.0, 0)
+        sgc = K.sgemm(0, 0, r, n, k, 1.0, inp, 0.0, 0)
+        K.assert_parity(K.parity_report(gpu, orc, ref, sgc, r, n, r, 0))
