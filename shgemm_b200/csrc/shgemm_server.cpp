@@ -100,13 +100,17 @@ struct Request {
     size_t om_off = Arena::kNone, y_off = Arena::kNone;
     size_t ldb = 0;  // Omega leading dimension (elements)
     bool y_held = false;
-    // Large requests run as row chunks in successive launches, one chunk in flight at a time,
-    // so that requests arriving behind them share the next launch instead of waiting for all
-    // of them (Omega is generated with the first chunk; later chunks launch after it completed).
+    // Large requests run as row chunks, one per launch, so that requests arriving behind them
+    // share the next launch instead of waiting for all of them. Omega is generated with the
+    // first chunk; a later chunk launched on another stream while that batch runs waits for
+    // it on the device (cudaStreamWaitEvent), so several chunks may be in flight.
     size_t row_next = 0;   // rows handed to launches
     size_t rows_done = 0;  // rows whose launches completed
-    bool in_flight = false;
+    int chunks_in_flight = 0;
     bool omega_made = false;
+    int omega_slot = -1;        // slot whose batch generates Omega
+    bool omega_ready = false;   // that batch completed
+    bool failed = false;
 };
 
 // One launch's share of a request: rows [row0, row0 + rows) of its Y.
@@ -238,22 +242,22 @@ bool shgemm_b200_server::launch_locked(Slot& s) {
     std::vector<shgemm_b200_omega_job> jobs;
     s.pieces.clear();
     int units = 0;
-    // first come first served, one chunk per request (requests with a chunk in flight wait)
+    const int me = static_cast<int>(&s - slots.data());
+    std::vector<char> wait_on(slots.size(), 0);  // other slots whose Omega batch this one needs
+    // first come first served, one chunk per request and launch
     for (auto it = ready.begin(); it != ready.end() && static_cast<int>(s.pieces.size()) < cfg.max_batch;) {
         Request& q = **it;
-        if (q.in_flight) {
-            ++it;
-            continue;
-        }
         const size_t rows = chunk_rows(q);
         const int pu = piece_units(q, rows);
         if (!s.pieces.empty() && units + pu > kMaxUnitsPerLaunch) break;
         units += pu;
         s.pieces.push_back({*it, q.row_next, rows});
-        q.in_flight = true;
+        ++q.chunks_in_flight;
         q.state = SHGEMM_REQ_RUNNING;
         const size_t cols = q.r.n * static_cast<size_t>(q.r.draws);
+        if (q.omega_made && !q.omega_ready && q.omega_slot != me) wait_on[q.omega_slot] = 1;
         if (!q.omega_made) {
+            q.omega_slot = me;
             // draw j of Omega from (seed, j): column block j of the k x (draws n) operand
             for (int j = 0; j < q.r.draws; ++j) {
                 uint8_t* dst = arena.ptr(q.om_off) + static_cast<size_t>(j) * q.r.n * q.ldb * omega_elem(*this);
@@ -283,7 +287,10 @@ bool shgemm_b200_server::launch_locked(Slot& s) {
             ++it;
     }
     if (s.pieces.empty()) return false;
-    bool ok = cudaEventRecord(s.start, s.stream) == cudaSuccess;
+    bool ok = true;
+    for (size_t o = 0; o < slots.size() && ok; ++o)
+        if (wait_on[o]) ok = cudaStreamWaitEvent(s.stream, slots[o].done, 0) == cudaSuccess;
+    ok = ok && cudaEventRecord(s.start, s.stream) == cudaSuccess;
     // every draw of the batch in one launch (per 64 draws)
     ok = ok && shgemm_b200_generate_omega_batch(s.stream, jobs.data(), static_cast<int>(jobs.size()), fp32) ==
                    SHGEMM_STATUS_OK;
@@ -315,20 +322,25 @@ bool shgemm_b200_server::complete_locked(Slot& s, bool ok) {
             cudaGetLastError();
         }
     }
+    const int me = static_cast<int>(&s - slots.data());
     for (auto& pc : s.pieces) {
         Request& q = *pc.q;
-        q.in_flight = false;
-        if (q.state != SHGEMM_REQ_RUNNING) continue;  // an earlier chunk failed it
-        q.rows_done += pc.rows;
-        if (ok && q.rows_done < q.r.m) continue;  // more chunks to come
-        if (!ok && q.row_next < q.r.m) {           // drop its remaining chunks
+        --q.chunks_in_flight;
+        if (q.omega_slot == me) q.omega_ready = true;
+        if (ok) q.rows_done += pc.rows;
+        if (!ok && !q.failed) {  // drop its remaining chunks
+            q.failed = true;
             auto it = std::find(ready.begin(), ready.end(), pc.q);
             if (it != ready.end()) ready.erase(it);
         }
+        // finished: every row done, or failed with no chunk left reading its Omega
+        if (q.failed ? q.chunks_in_flight > 0 : q.rows_done < q.r.m) continue;
+        if (q.state != SHGEMM_REQ_RUNNING) continue;
+        const bool good = !q.failed;
         arena.release(q.om_off, q.om_bytes);
         resident -= q.a_bytes + round_up(q.om_bytes);
         q.t_done = now;
-        if (ok) {
+        if (good) {
             q.state = SHGEMM_REQ_DONE;
             ++n_completed;
             latencies_ms.push_back(std::chrono::duration<double, std::milli>(now - q.t_submit).count());
@@ -338,7 +350,7 @@ bool shgemm_b200_server::complete_locked(Slot& s, bool ok) {
             q.state = SHGEMM_REQ_FAILED;
             ++n_failed;
         }
-        if (cfg.auto_release || !ok) release_y_locked(q);  // else Y stays resident until released
+        if (cfg.auto_release || !good) release_y_locked(q);  // else Y stays resident until released
         --n_unfinished;
     }
     s.pieces.clear();
