@@ -71,6 +71,8 @@ WORKLOADS = {
     # the small square SHGEMM (1024^3)
     "square1k": dict(m=1024, n=1024, k=1024, op_a=0, op_b=0, tc=0, alpha=1.0, beta=0.0, dist="uniform",
                      desc="plain SHGEMM 1024^3 NN, fp16 compute, A U[-1,1], B U[-1,1]"),
+    "square1k_tf32": dict(m=1024, n=1024, k=1024, op_a=0, op_b=0, tc=1, alpha=1.0, beta=0.0, dist="uniform",
+                          desc="plain SHGEMM 1024^3 NN, tf32 compute, A U[-1,1], B U[-1,1]"),
     # Y = Omega^T A as hsgemm(op_t, op_n) -> internal shgemm(op_t, op_n, 4096, 256, 2^20, op_c = t)
     "sketch": dict(m=4096, n=256, k=1 << 20, op_a=1, op_b=0, tc=0, alpha=1.0, beta=0.0, dist="sketch",
                    desc="left sketch Y = Omega^T A, A 2^20 x 4096 FP32 (low rank + noise), Omega 2^20 x 256 "
