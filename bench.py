@@ -851,7 +851,8 @@ def served_case(args, wl, ctx):
     pools = make_sketch_pools(wl, dev, seed=ctx.rank)
     reqs = sketch_requests(wl, pools, seed=ctx.rank, count=int(rate * duration * 1.5) + 64)
 
-    server = srv.SketchServer(ctx.local, hbm_budget_bytes=wl["budget"], compute_type=tc, streams=2, auto_release=True)
+    server = srv.SketchServer(ctx.local, hbm_budget_bytes=wl["budget"], compute_type=tc, streams=args.server_streams,
+                              auto_release=True)
     # warm-up: a few short bursts through the same server (kernels, arena, streams)
     warm = sketch_requests(wl, pools, seed=10_000 + ctx.rank, count=8 * args.warmup)
     for (m, n, k, a, lda, sd) in warm:
@@ -1268,6 +1269,7 @@ def main():
                     help="tensor-memory kernel in CTA pairs (SHGEMM_CFG_PAIR_TILES, with --no-autotune)")
     ap.add_argument("--rate", type=float, default=None, help="served: arrivals per second")
     ap.add_argument("--duration", type=float, default=None, help="served: seconds of arrivals")
+    ap.add_argument("--server-streams", type=int, default=2, help="served: the sketch server's streams (slots)")
     args = ap.parse_args()
     wl = dict(WORKLOADS[args.workload])
     if args.tc:
