@@ -1269,7 +1269,7 @@ def main():
                     help="tensor-memory kernel in CTA pairs (SHGEMM_CFG_PAIR_TILES, with --no-autotune)")
     ap.add_argument("--rate", type=float, default=None, help="served: arrivals per second")
     ap.add_argument("--duration", type=float, default=None, help="served: seconds of arrivals")
-    ap.add_argument("--server-streams", type=int, default=2, help="served: the sketch server's streams (slots)")
+    ap.add_argument("--server-streams", type=int, default=3, help="served: the sketch server's streams (slots)")
     args = ap.parse_args()
     wl = dict(WORKLOADS[args.workload])
     if args.tc:

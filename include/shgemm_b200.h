@@ -389,7 +389,7 @@ typedef struct {
     size_t hbm_budget_bytes; /* admission budget: A + Omega + Y of every admitted request */
     int compute_type;        /* SHGEMM_TC_FP16 or SHGEMM_TC_TF32 */
     int max_batch;           /* requests per grouped launch (<= 8192; 0: 512) */
-    int streams;             /* grouped launches in flight at once (1..8; 0: 2) */
+    int streams;             /* grouped launches in flight at once (1..8; 0: 3) */
     int auto_release;        /* 1: a completed request's Y is freed at once (throughput runs) */
 } shgemm_b200_server_config;
 

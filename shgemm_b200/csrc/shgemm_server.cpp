@@ -401,7 +401,7 @@ int shgemm_b200_server_create(shgemm_b200_server_t* out, int device, const shgem
     *out = nullptr;
     shgemm_b200_server_config c = *config;
     if (c.max_batch == 0) c.max_batch = 512;
-    if (c.streams == 0) c.streams = 2;
+    if (c.streams == 0) c.streams = 3;
     if ((c.compute_type != SHGEMM_TC_FP16 && c.compute_type != SHGEMM_TC_TF32) || c.max_batch < 1 ||
         c.max_batch > 8192 || c.streams < 1 || c.streams > 8 || c.hbm_budget_bytes == 0)
         return SHGEMM_STATUS_INVALID_VALUE;

@@ -109,7 +109,7 @@ class SketchServer:
     """
 
     def __init__(self, device: int = 0, hbm_budget_bytes: int = 40 << 30, compute_type: int = 1,
-                 max_batch: int = 512, streams: int = 2, auto_release: bool = False):
+                 max_batch: int = 512, streams: int = 3, auto_release: bool = False):
         L = _declare()
         self._s = ctypes.c_void_p()
         cfg = ServerConfig(hbm_budget_bytes, compute_type, max_batch, streams, int(auto_release))
