@@ -302,6 +302,9 @@ bool shgemm_b200_server::launch_locked(Slot& s) {
     ok = ok && cudaEventRecord(s.done, s.stream) == cudaSuccess;
     if (!ok) {
         cudaGetLastError();
+        // whatever was enqueued before the failure finishes before its memory is reused
+        cudaStreamSynchronize(s.stream);
+        cudaGetLastError();
         complete_locked(s, false);
         return true;
     }
