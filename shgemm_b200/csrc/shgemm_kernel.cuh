@@ -1198,11 +1198,12 @@ __global__ void __launch_bounds__(512, 1) shgemm_tile_kernel(const __grid_consta
     tile_kernel_body<TC, BN, A_KMAJOR, B_KMAJOR, false, false>(p);
 }
 
-// Single TF32 problem whose binary16 B was widened to FP32 beforehand (128 x 256 tiles, B
-// K-major): loaded straight into the TF32 tile layout, split-K as the other tile kernels.
-template <bool A_KMAJOR>
+// Single TF32 problem whose binary16 B was widened to FP32 beforehand (128 x BN tiles, BN 256
+// or 128, B K-major): loaded straight into the TF32 tile layout, split-K as the other tile
+// kernels.
+template <int BN, bool A_KMAJOR>
 __global__ void __launch_bounds__(512, 1) shgemm_tile_wide_kernel(const __grid_constant__ TileGemmParams p) {
-    tile_kernel_body<kTF32, 256, A_KMAJOR, true, true, false>(p);
+    tile_kernel_body<kTF32, BN, A_KMAJOR, true, true, false>(p);
 }
 
 // Many problems in one launch: per-problem descriptors and a unit list in device memory.

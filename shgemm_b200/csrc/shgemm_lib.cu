@@ -170,9 +170,13 @@ KernelEntry kernel_table(int tc, int bn, int ak, int bk) {
 }
 
 // TF32, 128 x 256 tiles, B widened to FP32 in the workspace (K-major).
-KernelEntry tile_wide_table(bool ak) {
-    if (ak) return {reinterpret_cast<void*>(&shgemm_tile_wide_kernel<true>), TileCfg<kTF32, 256, true, true, true>::SMEM_BYTES};
-    return {reinterpret_cast<void*>(&shgemm_tile_wide_kernel<false>), TileCfg<kTF32, 256, false, true, true>::SMEM_BYTES};
+template <int BN, bool AK>
+KernelEntry tile_wide_entry() {
+    return {reinterpret_cast<void*>(&shgemm_tile_wide_kernel<BN, AK>), TileCfg<kTF32, BN, AK, true, true>::SMEM_BYTES};
+}
+KernelEntry tile_wide_table(bool ak, int bn) {
+    if (bn == 256) return ak ? tile_wide_entry<256, true>() : tile_wide_entry<256, false>();
+    return ak ? tile_wide_entry<128, true>() : tile_wide_entry<128, false>();
 }
 
 // Tensor-memory operand kernels (binary16 compute, 128 x 256 tiles, B K-major).
@@ -763,8 +767,10 @@ int shgemm_b200_create(shgemm_b200_handle_t* out, int device) {
     for (int ak = 0; ak < 2; ++ak) {
         KernelEntry e = tm2_kernel_table(ak != 0);
         cudaFuncSetAttribute(e.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, e.smem);
-        e = tile_wide_table(ak != 0);
-        cudaFuncSetAttribute(e.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, e.smem);
+        for (int bn : {128, 256}) {
+            e = tile_wide_table(ak != 0, bn);
+            cudaFuncSetAttribute(e.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, e.smem);
+        }
     }
     h->max_pairs = query_max_pairs(tm2_kernel_table(true), sms);
     for (int tc = 0; tc < 2; ++tc)
@@ -1015,20 +1021,22 @@ static int run_tiled(shgemm_b200_handle_t h, int op_a, int op_b, size_t m, size_
         pl = plan_with(splitk_bytes - bblk_bytes);
         if (pl.bn != 256) block_b = false;
     }
-    // TF32 compute with a K-major binary16 B and n > 128: when the workspace also holds B widened
-    // to FP32 (ahead of the split-K partials), B is widened once per call and the 128 x 256
-    // kernel loads it as the TF32 tile layout itself (the kernel that widens B tile by tile in
-    // its split warps runs at about a third of the rate). Split-K as usual.
+    // TF32 compute with a K-major binary16 B and n > 64: when the workspace also holds B widened
+    // to FP32 (ahead of the split-K partials), B is widened once per call and a 128 x 256 (or,
+    // for n <= 128, 128 x 128) kernel loads it as the TF32 tile layout itself (the kernel that
+    // widens B tile by tile in its split warps runs at about a third of the rate). Split-K as
+    // usual.
+    const int wide_bn = n > 128 ? 256 : 128;
     const size_t wkb = (k + 31) / 32;  // k-blocks of the widened B
     const size_t wide_bytes = (wkb * 32 * n * sizeof(float) + 255) / 256 * 256;
     bool wide_b = tc == kTF32 && b_kmajor && !force && h->tile_kernel == 0 &&
-                        h->fixed_level == SHGEMM_LEVEL_AUTO && n > 128 && splitk_bytes >= wide_bytes &&
+                        h->fixed_level == SHGEMM_LEVEL_AUTO && n > 64 && splitk_bytes >= wide_bytes &&
                         k <= static_cast<size_t>(INT32_MAX) && wkb * n < (size_t(1) << 31);
     if (wide_b) {
         // taken when it keeps enough SMs busy: the widened-B kernel does a unit's work ~3x as fast,
         // but the widened B leaves less room for split-K partials
         const Plan pw = make_plan_for(h->num_sms, h->fixed_level, h->split_k, m, n, k, tc, splitk_bytes - wide_bytes,
-                                      256);
+                                      wide_bn);
         int gm_n = 8;
         const Plan pn = make_plan(h, op_a, op_b, m, n, k, tc, splitk_bytes, &gm_n);
         auto busy = [&](const Plan& q) {
@@ -1080,9 +1088,9 @@ static int run_tiled(shgemm_b200_handle_t h, int op_a, int op_b, size_t m, size_
         ok = make_tmap(&P.tmap_a, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, a, m, k, lda * 4,
                        use_tm ? 128 : a_mmajor_box(tc, wide_b), bk, CU_TENSOR_MAP_SWIZZLE_NONE);
     if (!ok) return SHGEMM_STATUS_NOT_SUPPORTED;
-    if (wide_b) {  // k-blocks {32 k, n columns, kblocks}: a [256 n][32 k] box is the TF32 tile layout
-        ok = make_tmap_3d(&P.tmap_b, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, b_wide, 32, n, wkb, 128, n * 128, 32, 256, 1,
-                          CU_TENSOR_MAP_SWIZZLE_128B);
+    if (wide_b) {  // k-blocks {32 k, n columns, kblocks}: a [bn n][32 k] box is the TF32 tile layout
+        ok = make_tmap_3d(&P.tmap_b, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, b_wide, 32, n, wkb, 128, n * 128, 32, wide_bn,
+                          1, CU_TENSOR_MAP_SWIZZLE_128B);
     } else if (tc == kFP16) {
         if (block_b)  // k-blocks {64 k, n columns, kblocks}: one 64 x 256 tile step is 32 KB contiguous
             ok = make_tmap_3d(&P.tmap_b, CU_TENSOR_MAP_DATA_TYPE_FLOAT16, b_blk, 64, n, kblocks, 128, n * 128, 64,
@@ -1131,7 +1139,7 @@ static int run_tiled(shgemm_b200_handle_t h, int op_a, int op_b, size_t m, size_
 
     const KernelEntry e = use_tm2 ? tm2_kernel_table(a_kmajor)
                           : use_tm ? tm_kernel_table(a_kmajor, kc, sv)
-                          : wide_b ? tile_wide_table(a_kmajor)
+                          : wide_b ? tile_wide_table(a_kmajor, wide_bn)
                                    : kernel_table(tc, pl.bn, a_kmajor, b_kmajor);
     const int threads = use_tm ? TmCfg<true, 1, 0>::NUM_THREADS : 512;
     if (!e.fn) return SHGEMM_STATUS_NOT_SUPPORTED;
@@ -2378,7 +2386,7 @@ int noalloc_setup(int dev, NoAllocDevice*& out) {
                     }
                 }
         for (int ak = 0; ak < 2; ++ak) {
-            for (KernelEntry e : {tm2_kernel_table(ak != 0), tile_wide_table(ak != 0)}) {
+            for (KernelEntry e : {tm2_kernel_table(ak != 0), tile_wide_table(ak != 0, 128), tile_wide_table(ak != 0, 256)}) {
                 if (cudaFuncSetAttribute(e.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, e.smem) != cudaSuccess) {
                     cudaGetLastError();
                     return SHGEMM_STATUS_NOT_SUPPORTED;

@@ -1,6 +1,6 @@
-"""TF32 calls with a K-contiguous binary16 B and n > 128 whose workspace holds B widened to FP32
-(the sketch shapes: few tiles, long k): B is widened once per call and the 128 x 256 TF32
-kernel that loads FP32 B directly runs with split-K. Parity with the restated reference
+"""TF32 calls with a K-contiguous binary16 B and n > 64 whose workspace holds B widened to FP32
+(the sketch shapes: few tiles, long k): B is widened once per call and the 128 x 256 (n > 128)
+or 128 x 128 TF32 kernel that loads FP32 B directly runs with split-K. Parity with the restated reference
 algorithm, and the debug line shows that this path ran. Shapes keep the operands
 TMA-addressable (16-byte leading dimensions) and ragged against the 128 x 256 x 32 tiles."""
 import ctypes
@@ -25,7 +25,8 @@ def h(cuda_device):
 
 
 @pytest.mark.parametrize("op_a,op_c", [(1, 1), (0, 0), (1, 0)])
-@pytest.mark.parametrize("mnk", [(512, 256, 32768), (300, 200, 20008), (132, 257, 4104), (1024, 384, 8192)])
+@pytest.mark.parametrize("mnk", [(512, 256, 32768), (300, 200, 20008), (132, 257, 4104), (1024, 384, 8192),
+                                 (700, 100, 16384), (256, 128, 8200)])
 def test_tf32_widened_b_split_k(h, capfd, op_a, op_c, mnk):
     import shgemm_b200 as sg
 
