@@ -264,6 +264,15 @@ int shgemm_b200_set_workspace_size(shgemm_b200_handle_t handle, size_t bytes);
  * shgemm_b200_destroy; calls on the handle overwrite its contents. */
 int shgemm_b200_get_workspace(shgemm_b200_handle_t handle, void** ptr, size_t* bytes);
 
+/* The heuristic plan of a call, without a device: the kernel level (0: the smaller tile N,
+ * 1: the larger; the reference's choice, src/shgemm.cu:643-656: the large tile when it fills
+ * the machine or when split-K will), the tile N, and the deterministic split-K slice count
+ * (split when the tiles leave SMs idle, k >= 4096 and the workspace holds >= 2 partials of
+ * m x n FP32; the count maximises the busy fraction of num_sms over the waves). Autotuned
+ * entries, the widened-B TF32 path and level fixing can override it on a handle. */
+int shgemm_b200_plan_preview(int num_sms, size_t m, size_t n, size_t k, int compute_type, size_t workspace_bytes,
+                             int* level, int* tile_n, int* slices);
+
 /* Synchronises the handle's stream and reports (then clears) the device-side
  * error word: SHGEMM_STATUS_TIMEOUT when a kernel gave up a bounded wait
  * (*device_code = which role), SHGEMM_STATUS_CUDA_ERROR on a CUDA error.

@@ -95,6 +95,7 @@ def lib() -> ctypes.CDLL:
         "shgemm_b200_get_config": [vp, i, ctypes.POINTER(ctypes.c_longlong)],
         "shgemm_b200_set_workspace_size": [vp, sz],
         "shgemm_b200_get_workspace": [vp, ctypes.POINTER(vp), ctypes.POINTER(sz)],
+        "shgemm_b200_plan_preview": [i, sz, sz, sz, i, sz, pi, pi, pi],
         "shgemm_b200_check_error": [vp, pi],
         "shgemm_b200_get_launch_count": [vp, ctypes.POINTER(ctypes.c_longlong)],
         "shgemm_b200_selftest_wait_timeout": [vp, ctypes.c_uint, pi],
@@ -264,6 +265,15 @@ class Handle:
 
 
 # ---------------------------------------------------------------- reference-shaped API
+def plan_preview(num_sms: int, m: int, n: int, k: int, compute_type: int, workspace_bytes: int) -> dict:
+    """The heuristic plan of a call (kernel level, tile N, split-K slices), computed on the host
+    without a device: the planner behind shgemm before autotuned entries or level fixing."""
+    level, tile_n, slices = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+    _check(lib().shgemm_b200_plan_preview(num_sms, m, n, k, compute_type, workspace_bytes, ctypes.byref(level),
+                                          ctypes.byref(tile_n), ctypes.byref(slices)), "plan_preview")
+    return {"level": level.value, "tile_n": tile_n.value, "slices": slices.value}
+
+
 def create(device: int = 0) -> Handle:
     """mtk::shgemm::create (include/shgemm/shgemm.hpp:94)."""
     return Handle(device)

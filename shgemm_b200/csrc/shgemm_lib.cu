@@ -907,6 +907,19 @@ int shgemm_b200_set_workspace_size(shgemm_b200_handle_t h, size_t bytes) {
     return SHGEMM_STATUS_OK;
 }
 
+int shgemm_b200_plan_preview(int num_sms, size_t m, size_t n, size_t k, int compute_type, size_t workspace_bytes,
+                             int* level, int* tile_n, int* slices) {
+    if (num_sms < 1 || (compute_type != SHGEMM_TC_FP16 && compute_type != SHGEMM_TC_TF32) || !level || !tile_n ||
+        !slices || m == 0 || n == 0 || k == 0)
+        return SHGEMM_STATUS_INVALID_VALUE;
+    const Plan p = make_plan_for(num_sms, SHGEMM_LEVEL_AUTO, 0, m, n, k,
+                                 compute_type == SHGEMM_TC_TF32 ? kTF32 : kFP16, workspace_bytes);
+    *level = p.level;
+    *tile_n = p.bn;
+    *slices = p.slices;
+    return SHGEMM_STATUS_OK;
+}
+
 int shgemm_b200_get_workspace(shgemm_b200_handle_t h, void** ptr, size_t* bytes) {
     if (!h || !ptr || !bytes) return SHGEMM_STATUS_INVALID_VALUE;
     *ptr = h->workspace;
