@@ -42,3 +42,18 @@ def test_reference_arm_prints_the_contract_line():
     assert line["cpu_baseline"]["kind"] == "port" and line["cpu_baseline"]["cores"] >= 1
     assert line["e2e"]["h2d_bytes_per_step"] == 0 and line["e2e"]["d2h_bytes_per_step"] == 0
     assert line["metric"] == bench.METRIC
+
+
+def test_cmake_project_configures(tmp_path):
+    """The CMake project (target `shgemm`, as the reference's) configures; building it is the
+    same nvcc compile as build.py."""
+    import shutil
+
+    cmake = shutil.which("cmake")
+    if cmake is None:
+        pytest.skip("cmake not installed")
+    r = subprocess.run([cmake, "-S", ROOT, "-B", str(tmp_path)], capture_output=True, text=True, timeout=240)
+    assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
+    r = subprocess.run([cmake, "--build", str(tmp_path), "--target", "help"], capture_output=True, text=True,
+                       timeout=120)
+    assert r.returncode == 0 and "shgemm" in r.stdout
