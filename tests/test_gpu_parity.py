@@ -324,7 +324,7 @@ def test_wide_pitch_b_k_blocks(h, op_a, k):
 def test_k_chunk_128(h, dist, op_a):
     """SHGEMM_CFG_K_CHUNK = 128 (one FP32 drain per 128 k in the tensor-memory kernel, an odd
     step count included): same non-finite mask as the restated reference and relative error
-    within 2x plain FP32 SGEMM's; the 64-k default meets the tighter
+    within 2x plain FP32 SGEMM's (the library's accuracy target); the 64-k default meets the tighter
     2x-the-restated-algorithm bar as well."""
     import shgemm_b200 as sg
 
