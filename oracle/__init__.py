@@ -7,7 +7,8 @@ product library (``shgemm_b200``) never imports it.
 Parity status: "parity unpinned" against the reference's own outputs -- the
 reference's numerics live in an un-vendored submodule (wmma_extension/tcec)
 and its tests store no golden values. The element conversions are pinned
-bit-for-bit against independent implementations (tests/golden/).
+bit-for-bit against independent implementations (tests/golden/), and both GEMM
+modes against a restatement in exact rational arithmetic (tests/test_oracle_exact.py).
 
 The C restatement lives in ``shgemm_oracle.c`` (each function cites the
 reference file:line it follows) and is built by ``oracle/Makefile`` into

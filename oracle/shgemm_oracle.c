@@ -12,7 +12,9 @@
  * its tests hold no golden values (the test/ programs only print errors). What IS pinned:
  * the element conversions below are checked bit-for-bit against independent
  * implementations (numpy's IEEE binary16 cast and exact rational rounding) by
- * tests/test_oracle.py with the fixtures in tests/golden/.
+ * tests/test_oracle.py with the fixtures in tests/golden/, and both GEMM modes are
+ * checked bit-for-bit against a restatement in exact rational arithmetic
+ * (tests/test_oracle_exact.py) on inputs whose fragment sums FP64 holds exactly.
  *
  * Algorithm restated (reference file:line):
  *  - split of the FP32 operand, src/wmmae_shgemm.hpp:30-31:
@@ -25,8 +27,10 @@
  *    sum with a round-to-nearest FP32 add; the lo product is accumulated over
  *    the whole k range.  `chunk` is the k-fragment length (16 for fp16 and 8
  *    for tf32 in the reference; the B200 kernel's k-chunk when modelling it).
- *    Products of split values are exact in FP64; a fragment sum is modelled as
- *    the exact sum rounded once to FP32.
+ *    Products of split values are exact in FP64; a fragment sum is formed in
+ *    FP64 and rounded once to FP32. The FP64 sum is exact while the products'
+ *    bits span at most ~49 bits (a 2^27 spread of magnitudes); beyond that it
+ *    carries a 2^-53 relative error, far below the FP32 rounding it feeds.
  *    That is oracle_shgemm, the idealised form. oracle_shgemm_tcmodel models
  *    the tensor core's accumulation as the reference meets it instead: each
  *    hi fragment sum truncated (rounded toward zero) to FP32 before its
