@@ -68,12 +68,42 @@ def test_create_without_gpu_fails_cleanly():
         shgemm_b200.Handle(0)
 
 
-def test_library_is_sm100a_only():
+def test_library_is_built_for_sm100a_only():
+    """Both build recipes compile device code for sm_100a alone (machine code, no PTX for
+    other architectures to JIT from)."""
+    from shgemm_b200 import build
+
+    assert build.ARCH == ["-gencode", "arch=compute_100a,code=sm_100a"]
+    cmake = open(os.path.join(ROOT, "CMakeLists.txt")).read()
+    assert re.search(r"CMAKE_CUDA_ARCHITECTURES\s+100a-real\)", cmake)
+
+
+def test_c_header_is_plain_c_and_links(tmp_path):
+    """include/shgemm_b200.h is strict C99 (what cgo, JNI and ctypes bindings include) and a
+    C program links against the library with it."""
     import shgemm_b200
 
-    out = subprocess.run(["cuobjdump", "--list-elf", shgemm_b200.library_path()], capture_output=True,
-                         text=True).stdout
-    assert "sm_100a" in out
+    src = tmp_path / "c_user.c"
+    src.write_text('#include "shgemm_b200.h"\n'
+                   "int main(void) { return shgemm_b200_noalloc_scratch_bytes() > 0 ? 0 : 1; }\n")
+    libdir = os.path.dirname(shgemm_b200.library_path())
+    env = dict(os.environ)
+    env.pop("CC", None)
+    subprocess.run(["gcc", "-std=c99", "-Wall", "-Wextra", "-pedantic", "-Werror", "-I",
+                    os.path.join(ROOT, "include"), str(src), "-L", libdir, "-lshgemm_b200", "-o",
+                    str(tmp_path / "c_user")], check=True, env=env)
+
+
+def test_cpp_header_compiles_as_host_cpp(tmp_path):
+    """include/shgemm/shgemm.hpp builds with the host C++ compiler alone (callers need not
+    compile with nvcc to use the C++ API)."""
+    src = tmp_path / "cpp_user.cpp"
+    src.write_text("#include <shgemm/shgemm.hpp>\nint main() { return 0; }\n")
+    cuda_inc = os.path.join(os.environ.get("CUDA_HOME", "/usr/local/cuda"), "include")
+    env = dict(os.environ)
+    env.pop("CXX", None)
+    subprocess.run(["g++", "-std=c++17", "-Wall", "-Wextra", "-Werror", "-I", os.path.join(ROOT, "include"), "-I",
+                    cuda_inc, "-c", str(src), "-o", str(tmp_path / "cpp_user.o")], check=True, env=env)
 
 
 def test_host_entry_points_validate_without_gpu():
