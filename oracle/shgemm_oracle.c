@@ -120,6 +120,7 @@ static inline float round_tc(int tc, float v) {
 
 /* Split of one FP32 value (src/wmmae_shgemm.hpp:30-31), scale 2^11. */
 void oracle_split(int tc, const float* v, size_t n, float* hi, float* lo) {
+#pragma omp parallel for schedule(static)
     for (size_t i = 0; i < n; i++) {
         const float h = round_tc(tc, v[i]);
         hi[i] = h;
@@ -139,16 +140,40 @@ static inline size_t c_index(int op, size_t i, size_t j, size_t ld) {
     return op == OP_N ? i + j * ld : j + i * ld;
 }
 
-/* Packs op(A) as [m][k] rows and op(B) as [n][k] rows (k contiguous). */
-static void pack_a(int op, size_t m, size_t k, const float* A, size_t lda, float* out) {
+/*
+ * The GEMM loops below work on register blocks of RB rows of op(A) by CB columns of
+ * op(B). Every element of C still takes its products in k order through the same
+ * operations as a loop over one element (no reassociation; no contraction, the file is
+ * compiled with -ffp-contract=off), so the blocking changes speed only: the RB rows of a
+ * block sit in vector lanes. op(A) is packed in row blocks, element (i, kk) at
+ * ((i / RB) * k + kk) * RB + i % RB, rows past m zero; op(B) as [n][k] rows (k
+ * contiguous), columns past n zero. The block kernels are compiled for AVX-512, AVX2 and
+ * baseline x86-64 and the loader picks one for the host (IEEE operations: the same
+ * results on each). They are called from the OpenMP loops, not inlined into them, so that
+ * each clone holds the whole k loop.
+ */
+#define RB 4
+#define CB 4
+#define HOT __attribute__((noinline, target_clones("arch=x86-64-v4", "arch=x86-64-v3", "default")))
+
+static size_t round_up_sz(size_t x, size_t q) { return (x + q - 1) / q * q; }
+
+static void pack_a_blocked(int op, size_t m, size_t k, const float* A, size_t lda, float* out) {
+    const size_t mb = round_up_sz(m, RB) / RB;
 #pragma omp parallel for schedule(static)
-    for (size_t i = 0; i < m; i++)
-        for (size_t kk = 0; kk < k; kk++) out[i * k + kk] = A[a_index(op, i, kk, lda)];
+    for (size_t ib = 0; ib < mb; ib++)
+        for (size_t kk = 0; kk < k; kk++)
+            for (size_t r = 0; r < RB; r++) {
+                const size_t i = ib * RB + r;
+                out[(ib * k + kk) * RB + r] = i < m ? A[a_index(op, i, kk, lda)] : 0.0f;
+            }
 }
-static void pack_b_f16(int op, size_t k, size_t n, const uint16_t* B, size_t ldb, float* out) {
+
+static void pack_b_f16(int op, size_t k, size_t n, size_t n_pad, const uint16_t* B, size_t ldb, float* out) {
 #pragma omp parallel for schedule(static)
-    for (size_t j = 0; j < n; j++)
-        for (size_t kk = 0; kk < k; kk++) out[j * k + kk] = oracle_f16_bits_to_f32(B[b_index(op, kk, j, ldb)]);
+    for (size_t j = 0; j < n_pad; j++)
+        for (size_t kk = 0; kk < k; kk++)
+            out[j * k + kk] = j < n ? oracle_f16_bits_to_f32(B[b_index(op, kk, j, ldb)]) : 0.0f;
 }
 
 static inline float epilogue(float acc, float alpha, float beta, const float* c) {
@@ -156,55 +181,176 @@ static inline float epilogue(float acc, float alpha, float beta, const float* c)
     return fmaf(acc, alpha, beta * (*c));
 }
 
+/* Operands of one GEMM in the blocked layouts (hi/lo only for the split forms). */
+typedef struct {
+    float *a, *ahi, *alo, *b;
+    size_t mb, nb;
+} packed_t;
+
+static void packed_free(packed_t* p) {
+    free(p->a);
+    free(p->ahi);
+    free(p->alo);
+    free(p->b);
+}
+
+/* Packs op(A) and op(B); with tc >= 0 also splits op(A). Returns 0 on success. */
+static int packed_make(packed_t* p, int tc, int op_a, int op_b, size_t m, size_t n, size_t k, const float* A,
+                       size_t lda, const uint16_t* B, size_t ldb) {
+    const size_t mp = round_up_sz(m, RB), np = round_up_sz(n, CB);
+    memset(p, 0, sizeof(*p));
+    p->mb = mp / RB;
+    p->nb = np / CB;
+    p->a = (float*)malloc(sizeof(float) * (mp * k + 1));
+    p->b = (float*)malloc(sizeof(float) * (np * k + 1));
+    if (tc >= 0) {
+        p->ahi = (float*)malloc(sizeof(float) * (mp * k + 1));
+        p->alo = (float*)malloc(sizeof(float) * (mp * k + 1));
+    }
+    if (!p->a || !p->b || (tc >= 0 && (!p->ahi || !p->alo))) {
+        packed_free(p);
+        return 1;
+    }
+    pack_a_blocked(op_a, m, k, A, lda, p->a);
+    if (tc >= 0) oracle_split(tc, p->a, mp * k, p->ahi, p->alo);
+    pack_b_f16(op_b, k, n, np, B, ldb, p->b);
+    return 0;
+}
+
+/* One vector per block column: RB lanes of FP32 or FP64 (GCC vector extensions; on a
+ * host without wide registers the compiler splits them). Lane arithmetic is the scalar
+ * IEEE operation, conversions round to nearest like a (float) cast. */
+typedef float vf_t __attribute__((vector_size(RB * sizeof(float))));
+typedef double vd_t __attribute__((vector_size(RB * sizeof(double))));
+typedef int32_t vi_t __attribute__((vector_size(RB * sizeof(int32_t))));
+
+static inline __attribute__((always_inline)) vf_t load_vf(const float* p) {
+    vf_t v;
+    memcpy(&v, p, sizeof(v));
+    return v;
+}
+
+/* Each lane of a double vector rounded toward zero to FP32 (the tensor core's truncating
+ * accumulation is modelled as exact products and sums rounded this way): round to
+ * nearest, and where that moved away from zero to a finite value, step one unit back
+ * toward zero (the bit pattern minus one, for either sign). NaN lanes compare false and
+ * stay; a lane that rounds to infinity stays infinite. */
+static inline __attribute__((always_inline)) vf_t rz_vf(vd_t d) {
+    const vf_t f = __builtin_convertvector(d, vf_t);
+    const vd_t back = __builtin_convertvector(f, vd_t);
+    const vd_t inf = (vd_t){0} + (double)INFINITY;
+    const __typeof__(back > d) away = ((back > d) & (d >= 0)) | ((back < d) & (d < 0));
+    const __typeof__(back > d) finite = (back < inf) & (back > -inf);
+    const vi_t step = __builtin_convertvector(away & finite, vi_t); /* -1 where it moves */
+    vi_t bits;
+    memcpy(&bits, &f, sizeof(bits));
+    bits += step;
+    vf_t out;
+    memcpy(&out, &bits, sizeof(out));
+    return out;
+}
+
+/* Idealised accumulation of one block (oracle_shgemm): per k-fragment the hi sum in FP64,
+ * rounded once and added with a round-to-nearest FP32 add; lo summed in FP64 over all k. */
+HOT static void block_ideal(const float* restrict ah, const float* restrict al, const float* restrict b, size_t k,
+                            size_t chunk, float out[CB][RB]) {
+    vf_t acc[CB];
+    vd_t lo[CB];
+    for (int c = 0; c < CB; c++) {
+        acc[c] = (vf_t){0};
+        lo[c] = (vd_t){0};
+    }
+    for (size_t k0 = 0; k0 < k; k0 += chunk) {
+        const size_t k1 = (k0 + chunk < k) ? k0 + chunk : k;
+        vd_t s[CB];
+        for (int c = 0; c < CB; c++) s[c] = (vd_t){0};
+        for (size_t kk = k0; kk < k1; kk++) {
+            const vd_t h = __builtin_convertvector(load_vf(ah + kk * RB), vd_t);
+            const vd_t l = __builtin_convertvector(load_vf(al + kk * RB), vd_t);
+            for (int c = 0; c < CB; c++) {
+                const double bv = (double)b[c * k + kk];
+                s[c] += h * bv;
+                lo[c] += l * bv;
+            }
+        }
+        for (int c = 0; c < CB; c++) acc[c] = acc[c] + __builtin_convertvector(s[c], vf_t);
+    }
+    for (int c = 0; c < CB; c++) {
+        const vf_t r = acc[c] + __builtin_convertvector(lo[c], vf_t) * (1.0f / 2048.0f);
+        memcpy(out[c], &r, sizeof(r));
+    }
+}
+
+/* Tensor-core model of one block (oracle_shgemm_tcmodel): per k-fragment the hi sum
+ * truncated to FP32 and added with a round-to-nearest FP32 add; the fragment's lo sum
+ * added to an FP32 lo accumulator with truncation. */
+HOT static void block_tcmodel(const float* restrict ah, const float* restrict al, const float* restrict b, size_t k,
+                              size_t chunk, float out[CB][RB]) {
+    vf_t acc[CB], lo[CB];
+    for (int c = 0; c < CB; c++) acc[c] = lo[c] = (vf_t){0};
+    for (size_t k0 = 0; k0 < k; k0 += chunk) {
+        const size_t k1 = (k0 + chunk < k) ? k0 + chunk : k;
+        vd_t s[CB], t[CB];
+        for (int c = 0; c < CB; c++) s[c] = t[c] = (vd_t){0};
+        for (size_t kk = k0; kk < k1; kk++) {
+            const vd_t h = __builtin_convertvector(load_vf(ah + kk * RB), vd_t);
+            const vd_t l = __builtin_convertvector(load_vf(al + kk * RB), vd_t);
+            for (int c = 0; c < CB; c++) {
+                const double bv = (double)b[c * k + kk];
+                s[c] += h * bv;
+                t[c] += l * bv;
+            }
+        }
+        for (int c = 0; c < CB; c++) {
+            acc[c] = acc[c] + rz_vf(s[c]);
+            lo[c] = rz_vf(__builtin_convertvector(lo[c], vd_t) + t[c]);
+        }
+    }
+    for (int c = 0; c < CB; c++) {
+        const vf_t r = acc[c] + lo[c] * (1.0f / 2048.0f);
+        memcpy(out[c], &r, sizeof(r));
+    }
+}
+
+static int shgemm_blocked(int tcmodel, int tc, int op_a, int op_b, size_t m, size_t n, size_t k, float alpha,
+                          const float* A, size_t lda, const uint16_t* B, size_t ldb, float beta, float* C,
+                          size_t ldc, int op_c, size_t chunk) {
+    if (chunk == 0) chunk = (tc == TC_FP16) ? 16 : 8;
+    packed_t p;
+    if (packed_make(&p, tc, op_a, op_b, m, n, k, A, lda, B, ldb)) return 1;
+    /* TF32 compute: the binary16 operand is exact in TF32 (src/utils.hpp:15-17). */
+#pragma omp parallel for collapse(2) schedule(static)
+    for (size_t jb = 0; jb < p.nb; jb++) {
+        for (size_t ib = 0; ib < p.mb; ib++) {
+            float out[CB][RB];
+            const float* ah = p.ahi + ib * k * RB;
+            const float* al = p.alo + ib * k * RB;
+            const float* bj = p.b + jb * CB * k;
+            if (tcmodel)
+                block_tcmodel(ah, al, bj, k, chunk, out);
+            else
+                block_ideal(ah, al, bj, k, chunk, out);
+            for (size_t c = 0; c < CB && jb * CB + c < n; c++)
+                for (size_t r = 0; r < RB && ib * RB + r < m; r++) {
+                    float* cp = C + c_index(op_c, ib * RB + r, jb * CB + c, ldc);
+                    *cp = epilogue(out[c][r], alpha, beta, cp);
+                }
+        }
+    }
+    packed_free(&p);
+    return 0;
+}
+
 /*
  * Restated reference SHGEMM: C = alpha * op(A) * op(B) + beta * C with A FP32
  * and B binary16 (bits). chunk = hi-fragment length. Returns 0 on success.
+ * Per element: for each k-fragment, s = sum of hi * b in FP64, acc = acc + (float)s;
+ * lo = sum over all k of lo * b in FP64; c = acc + (float)lo * 2^-11; then the epilogue.
  */
 int oracle_shgemm(int tc, int op_a, int op_b, size_t m, size_t n, size_t k, float alpha,
                   const float* A, size_t lda, const uint16_t* B, size_t ldb, float beta,
                   float* C, size_t ldc, int op_c, size_t chunk) {
-    if (chunk == 0) chunk = (tc == TC_FP16) ? 16 : 8;
-    float* a = (float*)malloc(sizeof(float) * (m * k + 1));
-    float* ahi = (float*)malloc(sizeof(float) * (m * k + 1));
-    float* alo = (float*)malloc(sizeof(float) * (m * k + 1));
-    float* b = (float*)malloc(sizeof(float) * (n * k + 1));
-    if (!a || !ahi || !alo || !b) { free(a); free(ahi); free(alo); free(b); return 1; }
-    pack_a(op_a, m, k, A, lda, a);
-    oracle_split(tc, a, m * k, ahi, alo);
-    pack_b_f16(op_b, k, n, B, ldb, b);
-    /* TF32 compute: the binary16 operand is exact in TF32 (src/utils.hpp:15-17). */
-#pragma omp parallel for collapse(2) schedule(static)
-    for (size_t j = 0; j < n; j++) {
-        for (size_t i = 0; i < m; i++) {
-            const float* ah = ahi + i * k;
-            const float* al = alo + i * k;
-            const float* bj = b + j * k;
-            float acc = 0.0f;
-            double lo = 0.0;
-            for (size_t k0 = 0; k0 < k; k0 += chunk) {
-                const size_t k1 = (k0 + chunk < k) ? k0 + chunk : k;
-                double s = 0.0;
-                for (size_t kk = k0; kk < k1; kk++) {
-                    s += (double)ah[kk] * (double)bj[kk];
-                    lo += (double)al[kk] * (double)bj[kk];
-                }
-                acc = acc + (float)s;
-            }
-            const float c = acc + (float)lo * (1.0f / 2048.0f);
-            float* cp = C + c_index(op_c, i, j, ldc);
-            *cp = epilogue(c, alpha, beta, cp);
-        }
-    }
-    free(a); free(ahi); free(alo); free(b);
-    return 0;
-}
-
-/* FP32 value of a double rounded toward zero (the tensor core's truncating
- * accumulation is modelled as exact products and sums rounded this way). */
-static inline float rz_f32(double d) {
-    float f = (float)d; /* round to nearest */
-    if (isfinite(f) && fabs((double)f) > fabs(d)) f = nextafterf(f, 0.0f);
-    return f;
+    return shgemm_blocked(0, tc, op_a, op_b, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, op_c, chunk);
 }
 
 /*
@@ -224,39 +370,31 @@ static inline float rz_f32(double d) {
 int oracle_shgemm_tcmodel(int tc, int op_a, int op_b, size_t m, size_t n, size_t k, float alpha,
                           const float* A, size_t lda, const uint16_t* B, size_t ldb, float beta,
                           float* C, size_t ldc, int op_c, size_t chunk) {
-    if (chunk == 0) chunk = (tc == TC_FP16) ? 16 : 8;
-    float* a = (float*)malloc(sizeof(float) * (m * k + 1));
-    float* ahi = (float*)malloc(sizeof(float) * (m * k + 1));
-    float* alo = (float*)malloc(sizeof(float) * (m * k + 1));
-    float* b = (float*)malloc(sizeof(float) * (n * k + 1));
-    if (!a || !ahi || !alo || !b) { free(a); free(ahi); free(alo); free(b); return 1; }
-    pack_a(op_a, m, k, A, lda, a);
-    oracle_split(tc, a, m * k, ahi, alo);
-    pack_b_f16(op_b, k, n, B, ldb, b);
-#pragma omp parallel for collapse(2) schedule(static)
-    for (size_t j = 0; j < n; j++) {
-        for (size_t i = 0; i < m; i++) {
-            const float* ah = ahi + i * k;
-            const float* al = alo + i * k;
-            const float* bj = b + j * k;
-            float acc = 0.0f, lo = 0.0f;
-            for (size_t k0 = 0; k0 < k; k0 += chunk) {
-                const size_t k1 = (k0 + chunk < k) ? k0 + chunk : k;
-                double s = 0.0, t = 0.0;
-                for (size_t kk = k0; kk < k1; kk++) {
-                    s += (double)ah[kk] * (double)bj[kk];
-                    t += (double)al[kk] * (double)bj[kk];
-                }
-                acc = acc + rz_f32(s);
-                lo = rz_f32((double)lo + t);
+    return shgemm_blocked(1, tc, op_a, op_b, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, op_c, chunk);
+}
+
+/* FP64 dot products of one block, each element over four interleaved partial sums
+ * (k = 0, 4, 8, .. / 1, 5, .. / ..; the tail into the first), combined as
+ * (s0 + s1) + (s2 + s3). Two of the block's columns per pass. */
+HOT static void block_dgemm(const float* restrict a, const float* restrict b, size_t k, double out[CB][RB]) {
+    for (int c0 = 0; c0 < CB; c0 += 2) {
+        vd_t s[4][2];
+        for (int q = 0; q < 4; q++) s[q][0] = s[q][1] = (vd_t){0};
+        size_t kk = 0;
+        for (; kk + 4 <= k; kk += 4)
+            for (int q = 0; q < 4; q++) {
+                const vd_t av = __builtin_convertvector(load_vf(a + (kk + q) * RB), vd_t);
+                for (int c = 0; c < 2; c++) s[q][c] += av * (double)b[(c0 + c) * k + kk + q];
             }
-            const float c = acc + lo * (1.0f / 2048.0f);
-            float* cp = C + c_index(op_c, i, j, ldc);
-            *cp = epilogue(c, alpha, beta, cp);
+        for (; kk < k; kk++) {
+            const vd_t av = __builtin_convertvector(load_vf(a + kk * RB), vd_t);
+            for (int c = 0; c < 2; c++) s[0][c] += av * (double)b[(c0 + c) * k + kk];
+        }
+        for (int c = 0; c < 2; c++) {
+            const vd_t r = (s[0][c] + s[1][c]) + (s[2][c] + s[3][c]);
+            memcpy(out[c0 + c], &r, sizeof(r));
         }
     }
-    free(a); free(ahi); free(alo); free(b);
-    return 0;
 }
 
 /*
@@ -267,32 +405,38 @@ int oracle_shgemm_tcmodel(int tc, int op_a, int op_b, size_t m, size_t n, size_t
 int oracle_dgemm_ref(int op_a, int op_b, size_t m, size_t n, size_t k, double alpha,
                      const float* A, size_t lda, const uint16_t* B, size_t ldb, double beta,
                      const float* Cin, size_t ldc, int op_c, double* C64) {
-    float* a = (float*)malloc(sizeof(float) * (m * k + 1));
-    float* b = (float*)malloc(sizeof(float) * (n * k + 1));
-    if (!a || !b) { free(a); free(b); return 1; }
-    pack_a(op_a, m, k, A, lda, a);
-    pack_b_f16(op_b, k, n, B, ldb, b);
+    packed_t p;
+    if (packed_make(&p, -1, op_a, op_b, m, n, k, A, lda, B, ldb)) return 1;
 #pragma omp parallel for collapse(2) schedule(static)
-    for (size_t j = 0; j < n; j++) {
-        for (size_t i = 0; i < m; i++) {
-            const float* ai = a + i * k;
-            const float* bj = b + j * k;
-            double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
-            size_t kk = 0;
-            for (; kk + 4 <= k; kk += 4) {
-                s0 += (double)ai[kk] * bj[kk];
-                s1 += (double)ai[kk + 1] * bj[kk + 1];
-                s2 += (double)ai[kk + 2] * bj[kk + 2];
-                s3 += (double)ai[kk + 3] * bj[kk + 3];
-            }
-            for (; kk < k; kk++) s0 += (double)ai[kk] * bj[kk];
-            double s = alpha * ((s0 + s1) + (s2 + s3));
-            if (beta != 0.0) s += beta * (double)Cin[c_index(op_c, i, j, ldc)];
-            C64[i + j * m] = s;
+    for (size_t jb = 0; jb < p.nb; jb++) {
+        for (size_t ib = 0; ib < p.mb; ib++) {
+            double out[CB][RB];
+            block_dgemm(p.a + ib * k * RB, p.b + jb * CB * k, k, out);
+            for (size_t c = 0; c < CB && jb * CB + c < n; c++)
+                for (size_t r = 0; r < RB && ib * RB + r < m; r++) {
+                    const size_t i = ib * RB + r, j = jb * CB + c;
+                    double s = alpha * out[c][r];
+                    if (beta != 0.0) s += beta * (double)Cin[c_index(op_c, i, j, ldc)];
+                    C64[i + j * m] = s;
+                }
         }
     }
-    free(a); free(b);
+    packed_free(&p);
     return 0;
+}
+
+/* Sequential FP32 fused multiply-adds over k for one block. */
+HOT static void block_sgemm(const float* restrict a, const float* restrict b, size_t k, float out[CB][RB]) {
+    float acc[CB][RB];
+    for (int c = 0; c < CB; c++)
+        for (int r = 0; r < RB; r++) acc[c][r] = 0.0f;
+    for (size_t kk = 0; kk < k; kk++)
+        for (int c = 0; c < CB; c++) {
+            const float bv = b[c * k + kk];
+            for (int r = 0; r < RB; r++) acc[c][r] = fmaf(a[kk * RB + r], bv, acc[c][r]);
+        }
+    for (int c = 0; c < CB; c++)
+        for (int r = 0; r < RB; r++) out[c][r] = acc[c][r];
 }
 
 /*
@@ -302,56 +446,52 @@ int oracle_dgemm_ref(int op_a, int op_b, size_t m, size_t n, size_t k, double al
 int oracle_sgemm(int op_a, int op_b, size_t m, size_t n, size_t k, float alpha,
                  const float* A, size_t lda, const uint16_t* B, size_t ldb, float beta,
                  float* C, size_t ldc, int op_c) {
-    float* a = (float*)malloc(sizeof(float) * (m * k + 1));
-    float* b = (float*)malloc(sizeof(float) * (n * k + 1));
-    if (!a || !b) { free(a); free(b); return 1; }
-    pack_a(op_a, m, k, A, lda, a);
-    pack_b_f16(op_b, k, n, B, ldb, b);
+    packed_t p;
+    if (packed_make(&p, -1, op_a, op_b, m, n, k, A, lda, B, ldb)) return 1;
 #pragma omp parallel for collapse(2) schedule(static)
-    for (size_t j = 0; j < n; j++) {
-        for (size_t i = 0; i < m; i++) {
-            const float* ai = a + i * k;
-            const float* bj = b + j * k;
-            float acc = 0.0f;
-            for (size_t kk = 0; kk < k; kk++) acc = fmaf(ai[kk], bj[kk], acc);
-            float* cp = C + c_index(op_c, i, j, ldc);
-            *cp = epilogue(acc, alpha, beta, cp);
+    for (size_t jb = 0; jb < p.nb; jb++) {
+        for (size_t ib = 0; ib < p.mb; ib++) {
+            float out[CB][RB];
+            block_sgemm(p.a + ib * k * RB, p.b + jb * CB * k, k, out);
+            for (size_t c = 0; c < CB && jb * CB + c < n; c++)
+                for (size_t r = 0; r < RB && ib * RB + r < m; r++) {
+                    float* cp = C + c_index(op_c, ib * RB + r, jb * CB + c, ldc);
+                    *cp = epilogue(out[c][r], alpha, beta, cp);
+                }
         }
     }
-    free(a); free(b);
+    packed_free(&p);
     return 0;
 }
 
 /*
  * Plain OpenMP GEMMs in FP32 and FP64 for the timed CPU baseline (not checkers):
  * C = A B, column-major, A m x k (lda), B k x n (ldb), C m x n (ldc), C overwritten.
- * Threads split the columns of C; each walks k in blocks of 256 so the block of A
- * stays in cache, with the innermost loop down a column (contiguous, vectorisable).
+ * Threads split the columns of C; a column is a sum of columns of A scaled by B's
+ * entries, the innermost loop down a column of A (contiguous, vectorised).
  */
-#define CPU_GEMM_KB 256
-#define CPU_GEMM_BODY(T)                                                           \
-    _Pragma("omp parallel for schedule(dynamic, 4)")                               \
-    for (size_t j = 0; j < n; j++) {                                               \
-        T* cj = C + j * ldc;                                                       \
-        for (size_t i = 0; i < m; i++) cj[i] = (T)0;                               \
-        for (size_t k0 = 0; k0 < k; k0 += CPU_GEMM_KB) {                           \
-            const size_t k1 = (k0 + CPU_GEMM_KB < k) ? k0 + CPU_GEMM_KB : k;       \
-            for (size_t kk = k0; kk < k1; kk++) {                                  \
-                const T b = B[kk + j * ldb];                                       \
-                const T* ak = A + kk * lda;                                        \
-                for (size_t i = 0; i < m; i++) cj[i] += ak[i] * b;                 \
-            }                                                                      \
-        }                                                                          \
+#define CPU_GEMM_COLUMN(T, NAME)                                                        \
+    HOT static void NAME(size_t m, size_t k, const T* A, size_t lda, const T* bj, T* cj) { \
+        for (size_t i = 0; i < m; i++) cj[i] = (T)0;                                    \
+        for (size_t kk = 0; kk < k; kk++) {                                             \
+            const T b = bj[kk];                                                         \
+            const T* ak = A + kk * lda;                                                 \
+            for (size_t i = 0; i < m; i++) cj[i] += ak[i] * b;                          \
+        }                                                                               \
     }
+CPU_GEMM_COLUMN(float, cpu_column_f32)
+CPU_GEMM_COLUMN(double, cpu_column_f64)
 
 void oracle_cpu_sgemm(size_t m, size_t n, size_t k, const float* A, size_t lda, const float* B, size_t ldb,
                       float* C, size_t ldc) {
-    CPU_GEMM_BODY(float)
+#pragma omp parallel for schedule(dynamic, 4)
+    for (size_t j = 0; j < n; j++) cpu_column_f32(m, k, A, lda, B + j * ldb, C + j * ldc);
 }
 
 void oracle_cpu_dgemm(size_t m, size_t n, size_t k, const double* A, size_t lda, const double* B, size_t ldb,
                       double* C, size_t ldc) {
-    CPU_GEMM_BODY(double)
+#pragma omp parallel for schedule(dynamic, 4)
+    for (size_t j = 0; j < n; j++) cpu_column_f64(m, k, A, lda, B + j * ldb, C + j * ldc);
 }
 
 /* Number of OpenMP threads the oracle runs with (for the CPU-baseline report). */
