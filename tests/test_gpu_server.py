@@ -244,9 +244,10 @@ def test_server_poisson_stream(cuda_device):
 
 
 def test_large_request_runs_in_chunks_and_small_ones_pass_it(cuda_device):
-    """A request of ~2.2e12 flops runs as row chunks in successive launches (one in flight):
-    a small request submitted right behind it completes first, and the large one's rows on
-    both sides of every chunk boundary match the restated reference algorithm."""
+    """A request of ~2.2e12 flops runs as row chunks in successive launches (up to one per
+    server stream in flight): a small request submitted right behind it completes first, and
+    the large one's rows on both sides of every chunk boundary match the restated reference
+    algorithm."""
     import torch
 
     from shgemm_b200 import server as srv
