@@ -118,3 +118,18 @@ def test_host_entry_points_validate_without_gpu():
                 ctypes.byref(lvl))
         assert st == 1  # SHGEMM_STATUS_INVALID_VALUE
     assert L.shgemm_b200_release_host_staging(None) == 1
+
+
+def test_cpp_api_sample_builds_without_gpu(tmp_path):
+    """The reference README's usage (tests/cpp/api_sample.cu) compiles with nvcc for sm_100a
+    and links against the library here; the GPU test suite runs it."""
+    import shgemm_b200
+    from shgemm_b200 import build
+
+    libdir = os.path.dirname(shgemm_b200.library_path())
+    env = dict(os.environ)
+    env.pop("CC", None)
+    subprocess.run([build.nvcc(), "-std=c++17", "-O2", *build.ARCH, "-I", os.path.join(ROOT, "include"),
+                    os.path.join(ROOT, "tests", "cpp", "api_sample.cu"), "-L", libdir, "-lshgemm_b200",
+                    "-o", str(tmp_path / "api_sample")], check=True, env=env)
+    assert (tmp_path / "api_sample").exists()
