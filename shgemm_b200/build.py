@@ -13,7 +13,7 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libshgemm_b200.so")
 SOURCES = ["shgemm_lib.cu", "shgemm_api.cpp", "shgemm_server.cpp"]
-HEADERS = ["ptx.cuh", "shgemm_kernel.cuh", "shgemm_kernel_tm.cuh", "shgemm_kernel_tm2.cuh"]
+HEADERS = ["ptx.cuh", "shgemm_kernel.cuh", "shgemm_kernel_tm.cuh", "shgemm_kernel_tm2.cuh", "server_host.hpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

@@ -12,6 +12,7 @@
 // Completions are found by polling each stream's event; a request's latency is the
 // host time from submit to the poll that saw its batch finish.
 #include "shgemm_b200.h"
+#include "server_host.hpp"
 
 #include <cuda_runtime.h>
 
@@ -33,10 +34,10 @@ namespace {
 
 using Clock = std::chrono::steady_clock;
 
-constexpr size_t kAlign = 256;
-size_t round_up(size_t x) { return (x + kAlign - 1) / kAlign * kAlign; }
+using shgemm_b200_server_host::OffsetAllocator;
+using shgemm_b200_server_host::round_up;
 
-// First-fit sub-allocator over one device allocation; neighbouring free blocks merge.
+// The server's device memory: one allocation, carved by the first-fit offset allocator.
 class Arena {
    public:
     bool init(size_t bytes) {
@@ -46,49 +47,22 @@ class Arena {
             base_ = nullptr;
             return false;
         }
-        size_ = bytes;
-        free_[0] = bytes;
+        offs_.reset(bytes);
         return true;
     }
     void destroy() {
         if (base_) cudaFree(base_);
         base_ = nullptr;
     }
-    static constexpr size_t kNone = SIZE_MAX;
-    size_t alloc(size_t bytes) {
-        bytes = round_up(std::max<size_t>(bytes, 1));
-        for (auto it = free_.begin(); it != free_.end(); ++it) {
-            if (it->second < bytes) continue;
-            const size_t off = it->first, rest = it->second - bytes;
-            free_.erase(it);
-            if (rest) free_[off + bytes] = rest;
-            return off;
-        }
-        return kNone;
-    }
-    void release(size_t off, size_t bytes) {
-        bytes = round_up(std::max<size_t>(bytes, 1));
-        auto it = free_.emplace(off, bytes).first;
-        auto nx = std::next(it);
-        if (nx != free_.end() && it->first + it->second == nx->first) {
-            it->second += nx->second;
-            free_.erase(nx);
-        }
-        if (it != free_.begin()) {
-            auto pv = std::prev(it);
-            if (pv->first + pv->second == it->first) {
-                pv->second += it->second;
-                free_.erase(it);
-            }
-        }
-    }
+    static constexpr size_t kNone = OffsetAllocator::kNone;
+    size_t alloc(size_t bytes) { return offs_.alloc(bytes); }
+    void release(size_t off, size_t bytes) { offs_.release(off, bytes); }
     uint8_t* ptr(size_t off) const { return base_ + off; }
-    size_t size() const { return size_; }
+    size_t size() const { return offs_.size(); }
 
    private:
     uint8_t* base_ = nullptr;
-    size_t size_ = 0;
-    std::map<size_t, size_t> free_;  // offset -> bytes
+    OffsetAllocator offs_;
 };
 
 struct Request {
@@ -186,25 +160,16 @@ void fill_sizes(const shgemm_b200_server& s, Request& q) {
     q.y_bytes = std::max<size_t>(1, q.r.m * cols * sizeof(float));
 }
 
-constexpr int kMaxUnitsPerLaunch = 1 << 16;
-// Work of one chunk of a large request, 2 m n k: ~1.6 ms on a B200 in TF32.
-constexpr double kChunkFlops = 4e11;
+using shgemm_b200_server_host::kMaxUnitsPerLaunch;
 
-// Rows of the next chunk of q: all that is left, or a multiple of 128 near kChunkFlops.
+// Rows of the next chunk of q (server_host.hpp).
 size_t chunk_rows(const Request& q) {
-    const size_t left = q.r.m - q.row_next;
-    const double per_row = 2.0 * static_cast<double>(q.r.n) * q.r.draws * static_cast<double>(q.r.k);
-    size_t rows = static_cast<size_t>(kChunkFlops / per_row) / 128 * 128;
-    rows = std::max<size_t>(rows, 128);
-    return rows >= left ? left : rows;
+    return shgemm_b200_server_host::chunk_rows(q.r.m, q.row_next, q.r.n, q.r.draws, q.r.k);
 }
 
-// Tiles a launch makes of `rows` rows of q (tile N: power of two in [32, 256]).
+// Tiles a launch makes of `rows` rows of q.
 int piece_units(const Request& q, size_t rows) {
-    const size_t cols = q.r.n * static_cast<size_t>(q.r.draws);
-    size_t bn = 32;
-    while (bn < 256 && bn < cols) bn *= 2;
-    return static_cast<int>(std::min<size_t>(((rows + 127) / 128) * ((cols + bn - 1) / bn), size_t(1) << 30));
+    return shgemm_b200_server_host::piece_units(rows, q.r.n * static_cast<size_t>(q.r.draws));
 }
 
 }  // namespace
