@@ -2120,8 +2120,8 @@ int grouped_stage(shgemm_b200_handle_t h, GroupedTable& t, bool b_wide, int op_a
                 list.push_back({static_cast<long long>(g.steps + 1) * (1024 + bn), make_int2(i, tm | (tn << 16))});
     }
     if (list.size() > static_cast<size_t>(kGroupedMaxUnits)) return SHGEMM_STATUS_NOT_SUPPORTED;
-    // Longest units first: the persistent CTAs take them round-robin, which balances
-    // uneven k (greedy longest-processing-time order). A unit's time is its k-steps times a
+    // Longest units first: the persistent CTAs claim them in this order as they free up,
+    // which balances uneven k (greedy longest-processing-time order). A unit's time is its k-steps times a
     // step's time, which the A tile's stream sets for every tile N (measured per step on
     // single-class batches: 0.93 us at N = 32 and 64, 0.99 at 128, 1.1 at 256), hence
     // 1024 + bn per step.
