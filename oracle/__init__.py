@@ -61,6 +61,8 @@ def lib() -> ctypes.CDLL:
         L.oracle_shgemm.argtypes = [i, i, i, sz, sz, sz, f, p, sz, p, sz, f, p, sz, i, sz]
         L.oracle_shgemm_tcmodel.restype = i
         L.oracle_shgemm_tcmodel.argtypes = [i, i, i, sz, sz, sz, f, p, sz, p, sz, f, p, sz, i, sz]
+        L.oracle_shgemm_b200model.restype = i
+        L.oracle_shgemm_b200model.argtypes = [i, i, i, sz, sz, sz, f, p, sz, p, sz, f, p, sz, i, sz]
         L.oracle_dgemm_ref.restype = i
         L.oracle_dgemm_ref.argtypes = [i, i, sz, sz, sz, d, p, sz, p, sz, d, p, sz, i, p]
         L.oracle_sgemm.restype = i
@@ -110,7 +112,7 @@ def split(tc: int, x) -> tuple[np.ndarray, np.ndarray]:
     return hi, lo
 
 
-IDEAL, TCMODEL = "ideal", "tcmodel"
+IDEAL, TCMODEL, B200MODEL = "ideal", "tcmodel", "b200model"
 
 
 def shgemm(tc, op_a, op_b, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, op_c=OP_N, chunk=0, model=IDEAL):
@@ -120,15 +122,21 @@ def shgemm(tc, op_a, op_b, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, op_c=OP
     each hi fragment exactly and accumulates lo exactly (oracle_shgemm); TCMODEL models
     the reference's tensor-core accumulation -- hi fragments truncated to FP32 before
     their round-to-nearest add, lo in a truncating FP32 accumulator over all k
-    (oracle_shgemm_tcmodel, src/wmmae_shgemm.hpp:86-124).
+    (oracle_shgemm_tcmodel, src/wmmae_shgemm.hpp:86-124); B200MODEL models this library's
+    kernels instead -- per drain of ``chunk`` k (64 binary16 / 32 TF32 by default) lo then
+    hi fragments in one truncating accumulator, folded by the 2^-11 input scale, added to
+    the running sum with round to nearest (oracle_shgemm_b200model).
     """
     A = _f32(A)
     B = _u16(B)
     assert C.dtype == np.float32 and C.flags.c_contiguous
-    fn = lib().oracle_shgemm if model == IDEAL else lib().oracle_shgemm_tcmodel
-    if model not in (IDEAL, TCMODEL):
+    fns = {IDEAL: "oracle_shgemm", TCMODEL: "oracle_shgemm_tcmodel", B200MODEL: "oracle_shgemm_b200model"}
+    if model not in fns:
         raise ValueError(model)
-    rc = fn(tc, op_a, op_b, m, n, k, alpha, _ptr(A), lda, _ptr(B), ldb, beta, _ptr(C), ldc, op_c, chunk)
+    rc = getattr(lib(), fns[model])(tc, op_a, op_b, m, n, k, alpha, _ptr(A), lda, _ptr(B), ldb, beta, _ptr(C), ldc,
+                                   op_c, chunk)
+    if rc == 2:
+        raise ValueError("chunk must be a multiple of the MMA fragment (16 k binary16, 8 k TF32)")
     if rc != 0:
         raise MemoryError("oracle_shgemm: allocation failed")
     return C

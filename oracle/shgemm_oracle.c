@@ -35,7 +35,10 @@
  *    the tensor core's accumulation as the reference meets it instead: each
  *    hi fragment sum truncated (rounded toward zero) to FP32 before its
  *    round-to-nearest add, and lo kept in an FP32 accumulator across all k
- *    that takes each fragment's sum with truncation.
+ *    that takes each fragment's sum with truncation. oracle_shgemm_b200model
+ *    models this library's kernels the same way (not the reference): per
+ *    drain one truncating accumulator takes the lo fragments, then the hi
+ *    fragments with the 2^-11 input scale, and is added with round to nearest.
  *  - fold, tcec store_matrix_sync at src/shgemm.cu:87-99: c = hi + lo * 2^-11.
  *  - epilogue, src/dmem_accessor.hpp:267-271 (beta != 0) and 199-214
  *    (beta == 0, C is not read): alpha * c + beta * C.
@@ -312,10 +315,49 @@ HOT static void block_tcmodel(const float* restrict ah, const float* restrict al
     }
 }
 
+/* The B200 kernels' accumulation as modelled for one block (oracle_shgemm_b200model): per
+ * drain of nfrag fragments of `frag` k, one FP32 accumulator D starts at zero, takes the
+ * drain's lo fragments one by one (D = RZ(D + fragment sum)), then the first hi fragment with
+ * D scaled by 2^-11 (the MMA's scale-input-d: D = RZ(D 2^-11 + fragment sum)) and the other hi
+ * fragments (D = RZ(D + fragment sum)); the drain adds D to the FP32 running sum with a
+ * round-to-nearest add. Fragment sums are FP64 as in the other modes; D 2^-11 + s is formed
+ * in FP64 before its truncation. */
+HOT static void block_b200model(const float* restrict ah, const float* restrict al, const float* restrict b,
+                                size_t k, size_t frag, size_t nfrag, float out[CB][RB]) {
+    vf_t acc[CB];
+    for (int c = 0; c < CB; c++) acc[c] = (vf_t){0};
+    for (size_t k0 = 0; k0 < k; k0 += frag * nfrag) {
+        vf_t d[CB];
+        for (int c = 0; c < CB; c++) d[c] = (vf_t){0};
+        for (int part = 0; part < 2; part++) { /* 0: lo fragments, 1: hi fragments */
+            const float* src = part == 0 ? al : ah;
+            for (size_t f = 0; f < nfrag; f++) {
+                const size_t kb = k0 + f * frag;
+                if (kb >= k) break;
+                const size_t ke = (kb + frag < k) ? kb + frag : k;
+                vd_t s[CB];
+                for (int c = 0; c < CB; c++) s[c] = (vd_t){0};
+                for (size_t kk = kb; kk < ke; kk++) {
+                    const vd_t v = __builtin_convertvector(load_vf(src + kk * RB), vd_t);
+                    for (int c = 0; c < CB; c++) s[c] += v * (double)b[c * k + kk];
+                }
+                for (int c = 0; c < CB; c++) {
+                    vd_t dd = __builtin_convertvector(d[c], vd_t);
+                    if (part == 1 && f == 0) dd *= 1.0 / 2048.0;
+                    d[c] = rz_vf(dd + s[c]);
+                }
+            }
+        }
+        for (int c = 0; c < CB; c++) acc[c] = acc[c] + d[c];
+    }
+    for (int c = 0; c < CB; c++) memcpy(out[c], &acc[c], sizeof(acc[c]));
+}
+
 static int shgemm_blocked(int tcmodel, int tc, int op_a, int op_b, size_t m, size_t n, size_t k, float alpha,
                           const float* A, size_t lda, const uint16_t* B, size_t ldb, float beta, float* C,
                           size_t ldc, int op_c, size_t chunk) {
-    if (chunk == 0) chunk = (tc == TC_FP16) ? 16 : 8;
+    if (chunk == 0) chunk = (tc == TC_FP16) ? (tcmodel == 2 ? 64 : 16) : (tcmodel == 2 ? 32 : 8);
+    if (tcmodel == 2 && (chunk % ((tc == TC_FP16) ? 16 : 8)) != 0) return 2;
     packed_t p;
     if (packed_make(&p, tc, op_a, op_b, m, n, k, A, lda, B, ldb)) return 1;
     /* TF32 compute: the binary16 operand is exact in TF32 (src/utils.hpp:15-17). */
@@ -326,7 +368,9 @@ static int shgemm_blocked(int tcmodel, int tc, int op_a, int op_b, size_t m, siz
             const float* ah = p.ahi + ib * k * RB;
             const float* al = p.alo + ib * k * RB;
             const float* bj = p.b + jb * CB * k;
-            if (tcmodel)
+            if (tcmodel == 2)
+                block_b200model(ah, al, bj, k, (tc == TC_FP16) ? 16 : 8, chunk / ((tc == TC_FP16) ? 16 : 8), out);
+            else if (tcmodel)
                 block_tcmodel(ah, al, bj, k, chunk, out);
             else
                 block_ideal(ah, al, bj, k, chunk, out);
@@ -371,6 +415,21 @@ int oracle_shgemm_tcmodel(int tc, int op_a, int op_b, size_t m, size_t n, size_t
                           const float* A, size_t lda, const uint16_t* B, size_t ldb, float beta,
                           float* C, size_t ldc, int op_c, size_t chunk) {
     return shgemm_blocked(1, tc, op_a, op_b, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, op_c, chunk);
+}
+
+/*
+ * SHGEMM with the accumulation of this library's B200 kernels modelled (not the reference's):
+ * per drain of `chunk` k (0: 64 for binary16, 32 for TF32; a multiple of the 16- or 8-k
+ * MMA fragment), the lo fragments and then the hi fragments go into one truncating FP32
+ * accumulator, the first hi fragment scaling it by 2^-11, and the drain is added to the
+ * running sum with a round-to-nearest add; then the epilogue. For comparing the method's
+ * modelled error with the reference's (oracle_shgemm_tcmodel) on the CPU. Returns 2 when
+ * chunk is not a multiple of the fragment.
+ */
+int oracle_shgemm_b200model(int tc, int op_a, int op_b, size_t m, size_t n, size_t k, float alpha,
+                            const float* A, size_t lda, const uint16_t* B, size_t ldb, float beta,
+                            float* C, size_t ldc, int op_c, size_t chunk) {
+    return shgemm_blocked(2, tc, op_a, op_b, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, op_c, chunk);
 }
 
 /* FP64 dot products of one block, each element over four interleaved partial sums

@@ -200,3 +200,35 @@ def test_tcmodel_error_close_to_idealised(tc):
     e_s = oracle.rel_fro(oracle.logical_c(S, m, n, m), ref)
     assert 0.9 * e[oracle.IDEAL] <= e[oracle.TCMODEL] <= 1.5 * e[oracle.IDEAL]
     assert e[oracle.TCMODEL] < 0.5 * e_s
+
+
+@pytest.mark.parametrize("tc", [oracle.FP16, oracle.TF32])
+def test_b200_accumulation_model_against_the_reference_model(tc):
+    """The B200 kernels' accumulation (B200MODEL: one round-to-nearest add to the running sum
+    per 64 k in binary16 / 32 k in TF32, truncation only inside a drain, lo folded in by the
+    2^-11 input scale) against the reference's (TCMODEL: one add per 16 / 8 k, lo truncated
+    over all k), both on the CPU: the modelled error against FP64 is no larger at k = 1024 and
+    about half at k = 16384 (fewer roundings of the large running sum)."""
+    rng = np.random.default_rng(3)
+    m = n = 64
+    for k, lo_bound, hi_bound in ((1024, 0.6, 1.1), (16384, 0.4, 0.65)):
+        signs = np.where(rng.random(m * k) < 0.5, -1.0, 1.0)
+        A = (signs * 2.0 ** rng.uniform(-15, 14, m * k)).astype(np.float32)  # binary16-safe range
+        B = rng.standard_normal(k * n).astype(np.float16)
+        ref = oracle.dgemm_ref(0, 0, m, n, k, 1.0, A, m, B, k)
+        err = {}
+        for model in (oracle.TCMODEL, oracle.B200MODEL):
+            C = np.zeros(m * n, np.float32)
+            oracle.shgemm(tc, 0, 0, m, n, k, 1.0, A, m, B, k, 0.0, C, m, 0, 0, model)
+            err[model] = oracle.rel_fro(oracle.logical_c(C, m, n, m), ref)
+        ratio = err[oracle.B200MODEL] / err[oracle.TCMODEL]
+        print(f"tc={tc} k={k}: B200 model / reference model error = {ratio:.2f}")
+        assert lo_bound <= ratio <= hi_bound, (k, ratio)
+
+
+def test_b200_model_rejects_a_partial_fragment_chunk():
+    A = np.ones(16 * 16, np.float32)
+    B = np.ones(16 * 16, np.float16)
+    with pytest.raises(ValueError):
+        oracle.shgemm(oracle.FP16, 0, 0, 16, 16, 16, 1.0, A, 16, B, 16, 0.0, np.zeros(256, np.float32), 16, 0, 24,
+                      oracle.B200MODEL)

@@ -2,10 +2,11 @@
 arithmetic, with every IEEE rounding done on the rationals (no FP32 or FP64 sums at all).
 
 Pins what the element-conversion fixtures do not: the operand indexing of every op
-combination, the k-fragment walk with a ragged last fragment, both accumulation models (the
-idealised one and the tensor-core model of src/wmmae_shgemm.hpp:86-124), the fold
-hi + lo * 2^-11 (tcec store, src/shgemm.cu:87-99) and the alpha/beta epilogue
-(src/dmem_accessor.hpp:199-214, 267-271), bit for bit.
+combination, the k-fragment walk with a ragged last fragment, the three accumulation models
+(the idealised one, the reference's tensor-core model of src/wmmae_shgemm.hpp:86-124, and
+the model of this library's kernels: a truncating accumulator per drain with lo folded in by
+the 2^-11 input scale), the fold hi + lo * 2^-11 (tcec store, src/shgemm.cu:87-99) and the
+alpha/beta epilogue (src/dmem_accessor.hpp:199-214, 267-271), bit for bit.
 
 The oracle forms each fragment sum in FP64, which is exact while the products' bits fit in
 53 bits; the inputs here keep every |value| within [2^-3, 2^3) (A) and [2^-2, 2^2) (B), so
@@ -74,7 +75,29 @@ def _split(tc, v):
     return Fraction(float(hi)), Fraction(float(lo))
 
 
+def _b200_element(h, l, bv, k, frag, nfrag):
+    """One element as the B200 kernels accumulate it (the oracle's B200MODEL): per drain of
+    nfrag fragments, D from zero takes the lo fragment sums with truncation, then the first hi
+    fragment sum with D scaled by 2^-11, then the other hi fragment sums, all truncated; the
+    drain is added to the running sum with round to nearest."""
+    acc = Fraction(0)
+    for k0 in range(0, k, frag * nfrag):
+        d = Fraction(0)
+        for part, src in ((0, l), (1, h)):
+            for f in range(nfrag):
+                kb = k0 + f * frag
+                if kb >= k:
+                    break
+                s = sum((src[kk] * bv[kk] for kk in range(kb, min(kb + frag, k))), Fraction(0))
+                d = rz((d / 2048 if part == 1 and f == 0 else d) + s)
+        acc = rn(acc + d)
+    return acc
+
+
 def _exact_shgemm(tc, op_a, op_b, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, op_c, chunk, model):
+    if model == oracle.B200MODEL:
+        frag = 16 if tc == oracle.FP16 else 8
+        chunk = chunk or (64 if tc == oracle.FP16 else 32)
     chunk = chunk or (16 if tc == oracle.FP16 else 8)
     a = lambda i, kk: A[i + kk * lda] if op_a == oracle.OP_N else A[kk + i * lda]  # noqa: E731
     b = lambda kk, j: B[kk + j * ldb] if op_b == oracle.OP_N else B[j + kk * ldb]  # noqa: E731
@@ -83,6 +106,18 @@ def _exact_shgemm(tc, op_a, op_b, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, 
     al, be = Fraction(float(np.float32(alpha))), Fraction(float(np.float32(beta)))
     for j in range(n):
         for i in range(m):
+            if model == oracle.B200MODEL:
+                for kk in range(k):
+                    if (i, kk) not in split:
+                        split[(i, kk)] = _split(tc, a(i, kk))
+                h = [split[(i, kk)][0] for kk in range(k)]
+                l = [split[(i, kk)][1] for kk in range(k)]
+                bv = [Fraction(float(np.float16(b(kk, j)))) for kk in range(k)]
+                c = _b200_element(h, l, bv, k, frag, chunk // frag)
+                idx = i + j * ldc if op_c == oracle.OP_N else j + i * ldc
+                res = rn(c * al) if beta == 0 else rn(c * al + rn(be * Fraction(float(out[idx]))))
+                out[idx] = _f32(res)
+                continue
             acc, lo_acc, lo_exact = Fraction(0), Fraction(0), Fraction(0)
             for k0 in range(0, k, chunk):
                 s = t = Fraction(0)
@@ -129,7 +164,7 @@ CASES = [(0, 0, 0), (1, 0, 0), (0, 1, 1), (1, 1, 1)]
 
 
 @pytest.mark.parametrize("tc", [oracle.FP16, oracle.TF32])
-@pytest.mark.parametrize("model", [oracle.IDEAL, oracle.TCMODEL])
+@pytest.mark.parametrize("model", [oracle.IDEAL, oracle.TCMODEL, oracle.B200MODEL])
 @pytest.mark.parametrize("ops", CASES)
 @pytest.mark.parametrize("chunk,k", [(0, 37), (64, 150)])
 def test_oracle_matches_exact_restatement(tc, model, ops, chunk, k):
