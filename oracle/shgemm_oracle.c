@@ -315,17 +315,63 @@ HOT static void block_tcmodel(const float* restrict ah, const float* restrict al
     }
 }
 
+typedef int64_t vl_t __attribute__((vector_size(RB * sizeof(int64_t))));
+
+static inline __attribute__((always_inline)) vl_t bits_vd(vd_t x) {
+    vl_t b;
+    memcpy(&b, &x, sizeof(b));
+    return b;
+}
+static inline __attribute__((always_inline)) vd_t vd_bits(vl_t b) {
+    vd_t x;
+    memcpy(&x, &b, sizeof(x));
+    return x;
+}
+
+/* One MMA instruction of the model with alignment (align_bits = p > 0): the accumulator c and
+ * the fragment's products (exact in FP64) are aligned to the largest magnitude among them and
+ * each is truncated toward zero to the multiple of 2^(E - p + 1), E that magnitude's exponent,
+ * i.e. p bits from its leading bit; the truncated terms are summed exactly (fewer than 2^5
+ * terms of at most p + 1 bits each fit FP64's 53) and the sum is truncated to FP32. With
+ * p = 0 the exact sum is truncated instead. Zero lanes stay zero. */
+static inline __attribute__((always_inline)) vf_t mma_model(vd_t c, const vd_t* prod, size_t np, int p) {
+    if (p <= 0) {
+        vd_t s = c;
+        for (size_t i = 0; i < np; i++) s += prod[i];
+        return rz_vf(s);
+    }
+    const vl_t abs_mask = (vl_t){0} + 0x7fffffffffffffffLL;
+    vl_t mx = bits_vd(c) & abs_mask; /* magnitudes compare as integers */
+    for (size_t i = 0; i < np; i++) {
+        const vl_t a = bits_vd(prod[i]) & abs_mask;
+        const vl_t gt = a > mx;
+        mx = (a & gt) | (mx & ~gt);
+    }
+    vl_t eq = ((mx >> 52) & 0x7ff) - (p - 1); /* biased exponent of the quantum */
+    const vl_t low = eq < 1;
+    eq = (eq & ~low) | (((vl_t){0} + 1) & low);
+    const vd_t q = vd_bits(eq << 52);
+    vd_t s = __builtin_convertvector(__builtin_convertvector(c / q, vl_t), vd_t) * q;
+    vd_t plain = c;
+    for (size_t i = 0; i < np; i++) {
+        s += __builtin_convertvector(__builtin_convertvector(prod[i] / q, vl_t), vd_t) * q;
+        plain += prod[i];
+    }
+    /* lanes with an infinite or NaN term take the IEEE sum (the integer path would not) */
+    const vl_t nonfinite = (bits_vd(plain) & abs_mask) >= ((vl_t){0} + 0x7ff0000000000000LL);
+    return rz_vf(vd_bits((bits_vd(plain) & nonfinite) | (bits_vd(s) & ~nonfinite)));
+}
+
 /* The B200 kernels' accumulation as modelled for one block (oracle_shgemm_b200model): per
  * drain of nfrag fragments of `frag` k, one FP32 accumulator D starts at zero, takes the
- * drain's lo fragments one by one (D = RZ(D + fragment sum)), then the first hi fragment with
- * D scaled by 2^-11 (the MMA's scale-input-d: D = RZ(D 2^-11 + fragment sum)) and the other hi
- * fragments (D = RZ(D + fragment sum)); the drain adds D to the FP32 running sum with a
- * round-to-nearest add. Fragment sums are FP64 as in the other modes; D 2^-11 + s is formed
- * in FP64 before its truncation. */
+ * drain's lo fragments one MMA each (D = mma(D, fragment)), then the first hi fragment with
+ * D scaled by 2^-11 (the MMA's scale-input-d) and the other hi fragments; the drain adds D to
+ * the FP32 running sum with a round-to-nearest add. Each MMA is mma_model. */
 HOT static void block_b200model(const float* restrict ah, const float* restrict al, const float* restrict b,
-                                size_t k, size_t frag, size_t nfrag, float out[CB][RB]) {
+                                size_t k, size_t frag, size_t nfrag, int align_bits, float out[CB][RB]) {
     vf_t acc[CB];
     for (int c = 0; c < CB; c++) acc[c] = (vf_t){0};
+    vd_t prod[CB][16];
     for (size_t k0 = 0; k0 < k; k0 += frag * nfrag) {
         vf_t d[CB];
         for (int c = 0; c < CB; c++) d[c] = (vf_t){0};
@@ -335,16 +381,14 @@ HOT static void block_b200model(const float* restrict ah, const float* restrict 
                 const size_t kb = k0 + f * frag;
                 if (kb >= k) break;
                 const size_t ke = (kb + frag < k) ? kb + frag : k;
-                vd_t s[CB];
-                for (int c = 0; c < CB; c++) s[c] = (vd_t){0};
                 for (size_t kk = kb; kk < ke; kk++) {
                     const vd_t v = __builtin_convertvector(load_vf(src + kk * RB), vd_t);
-                    for (int c = 0; c < CB; c++) s[c] += v * (double)b[c * k + kk];
+                    for (int c = 0; c < CB; c++) prod[c][kk - kb] = v * (double)b[c * k + kk];
                 }
                 for (int c = 0; c < CB; c++) {
                     vd_t dd = __builtin_convertvector(d[c], vd_t);
                     if (part == 1 && f == 0) dd *= 1.0 / 2048.0;
-                    d[c] = rz_vf(dd + s[c]);
+                    d[c] = mma_model(dd, prod[c], ke - kb, align_bits);
                 }
             }
         }
@@ -355,9 +399,9 @@ HOT static void block_b200model(const float* restrict ah, const float* restrict 
 
 static int shgemm_blocked(int tcmodel, int tc, int op_a, int op_b, size_t m, size_t n, size_t k, float alpha,
                           const float* A, size_t lda, const uint16_t* B, size_t ldb, float beta, float* C,
-                          size_t ldc, int op_c, size_t chunk) {
+                          size_t ldc, int op_c, size_t chunk, int align_bits) {
     if (chunk == 0) chunk = (tc == TC_FP16) ? (tcmodel == 2 ? 64 : 16) : (tcmodel == 2 ? 32 : 8);
-    if (tcmodel == 2 && (chunk % ((tc == TC_FP16) ? 16 : 8)) != 0) return 2;
+    if (tcmodel == 2 && ((chunk % ((tc == TC_FP16) ? 16 : 8)) != 0 || align_bits < 0 || align_bits > 40)) return 2;
     packed_t p;
     if (packed_make(&p, tc, op_a, op_b, m, n, k, A, lda, B, ldb)) return 1;
     /* TF32 compute: the binary16 operand is exact in TF32 (src/utils.hpp:15-17). */
@@ -369,7 +413,8 @@ static int shgemm_blocked(int tcmodel, int tc, int op_a, int op_b, size_t m, siz
             const float* al = p.alo + ib * k * RB;
             const float* bj = p.b + jb * CB * k;
             if (tcmodel == 2)
-                block_b200model(ah, al, bj, k, (tc == TC_FP16) ? 16 : 8, chunk / ((tc == TC_FP16) ? 16 : 8), out);
+                block_b200model(ah, al, bj, k, (tc == TC_FP16) ? 16 : 8, chunk / ((tc == TC_FP16) ? 16 : 8),
+                                align_bits, out);
             else if (tcmodel)
                 block_tcmodel(ah, al, bj, k, chunk, out);
             else
@@ -394,7 +439,7 @@ static int shgemm_blocked(int tcmodel, int tc, int op_a, int op_b, size_t m, siz
 int oracle_shgemm(int tc, int op_a, int op_b, size_t m, size_t n, size_t k, float alpha,
                   const float* A, size_t lda, const uint16_t* B, size_t ldb, float beta,
                   float* C, size_t ldc, int op_c, size_t chunk) {
-    return shgemm_blocked(0, tc, op_a, op_b, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, op_c, chunk);
+    return shgemm_blocked(0, tc, op_a, op_b, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, op_c, chunk, 0);
 }
 
 /*
@@ -414,22 +459,24 @@ int oracle_shgemm(int tc, int op_a, int op_b, size_t m, size_t n, size_t k, floa
 int oracle_shgemm_tcmodel(int tc, int op_a, int op_b, size_t m, size_t n, size_t k, float alpha,
                           const float* A, size_t lda, const uint16_t* B, size_t ldb, float beta,
                           float* C, size_t ldc, int op_c, size_t chunk) {
-    return shgemm_blocked(1, tc, op_a, op_b, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, op_c, chunk);
+    return shgemm_blocked(1, tc, op_a, op_b, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, op_c, chunk, 0);
 }
 
 /*
  * SHGEMM with the accumulation of this library's B200 kernels modelled (not the reference's):
  * per drain of `chunk` k (0: 64 for binary16, 32 for TF32; a multiple of the 16- or 8-k
- * MMA fragment), the lo fragments and then the hi fragments go into one truncating FP32
- * accumulator, the first hi fragment scaling it by 2^-11, and the drain is added to the
- * running sum with a round-to-nearest add; then the epilogue. For comparing the method's
- * modelled error with the reference's (oracle_shgemm_tcmodel) on the CPU. Returns 2 when
- * chunk is not a multiple of the fragment.
+ * MMA fragment), the lo fragments and then the hi fragments go through one FP32 accumulator,
+ * one modelled MMA instruction per fragment (mma_model: alignment to the largest term with
+ * `align_bits` bits kept and truncation, or with align_bits = 0 truncation of the exact sum),
+ * the first hi fragment scaling the accumulator by 2^-11, and the drain is added to the
+ * running sum with a round-to-nearest add; then the epilogue. Returns 2 when chunk is not a
+ * multiple of the fragment or align_bits is outside 0..40.
  */
 int oracle_shgemm_b200model(int tc, int op_a, int op_b, size_t m, size_t n, size_t k, float alpha,
                             const float* A, size_t lda, const uint16_t* B, size_t ldb, float beta,
-                            float* C, size_t ldc, int op_c, size_t chunk) {
-    return shgemm_blocked(2, tc, op_a, op_b, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, op_c, chunk);
+                            float* C, size_t ldc, int op_c, size_t chunk, int align_bits) {
+    return shgemm_blocked(2, tc, op_a, op_b, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, op_c, chunk,
+                          align_bits);
 }
 
 /* FP64 dot products of one block, each element over four interleaved partial sums
