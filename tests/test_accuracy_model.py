@@ -93,3 +93,22 @@ def test_model_reproduces_measured_b200_errors(op_a, dist):
         assert abs(model / measured - 1) < 0.01, (dist, chunk, model, measured)
     if dist == "positive":
         assert err(128, 0) < 0.5 * MEASURED_B200[(op_a, dist)][1]  # the exact-sum model cannot explain it
+
+
+def test_smoke_model_agreement_line():
+    """The diagnostic line smoke() prints: a result equal to the model reads 100 % identical
+    and 0 ulp; the idealised oracle's result (a different accumulation) reads otherwise."""
+    import __graft_entry__ as entry
+
+    m, n, k = 64, 48, 512
+    rng = np.random.default_rng(0)
+    A = rng.uniform(-1, 1, m * k).astype(np.float32)
+    B = rng.uniform(-1, 1, k * n).astype(np.float16)
+    for tc in (oracle.FP16, oracle.TF32):
+        same = np.zeros(m * n, np.float32)
+        oracle.shgemm(tc, 0, 0, m, n, k, 1.0, A, m, B, k, 0.0, same, m, 0, 0, oracle.B200MODEL)
+        line = entry.model_agreement(tc, m, n, k, A, B, same)
+        assert "100.00 % of entries bit-identical" in line and "max 0 ulp" in line, line
+        other = np.zeros(m * n, np.float32)
+        oracle.shgemm(tc, 0, 0, m, n, k, 1.0, A, m, B, k, 0.0, other, m, 0, 0)
+        assert "100.00 % of entries bit-identical" not in entry.model_agreement(tc, m, n, k, A, B, other)
