@@ -7,8 +7,11 @@ product library (``shgemm_b200``) never imports it.
 Parity status: "parity unpinned" against the reference's own outputs -- the
 reference's numerics live in an un-vendored submodule (wmma_extension/tcec)
 and its tests store no golden values. The element conversions are pinned
-bit-for-bit against independent implementations (tests/golden/), and both GEMM
+bit-for-bit against independent implementations (tests/golden/), and the GEMM
 modes against a restatement in exact rational arithmetic (tests/test_oracle_exact.py).
+Three accumulation modes: IDEAL (the reference's algorithm with exact fragment sums),
+TCMODEL (the reference's tensor-core accumulation) and B200MODEL (this library's own
+kernels, down to the MMA instruction, calibrated on the B200's measured errors).
 
 The C restatement lives in ``shgemm_oracle.c`` (each function cites the
 reference file:line it follows) and is built by ``oracle/Makefile`` into
