@@ -113,3 +113,24 @@ def test_smoke_model_agreement_line():
         other = np.zeros(m * n, np.float32)
         oracle.shgemm(tc, 0, 0, m, n, k, 1.0, A, m, B, k, 0.0, other, m, 0, 0)
         assert "100.00 % of entries bit-identical" not in entry.model_agreement(tc, m, n, k, A, B, other)
+
+
+# FP64 relative errors of the smoke call (256 x 192 x 1024, A and B uniform(-1, 1) from
+# numpy seed 0, beta = 0), as a B200 printed them in an earlier build's round-end smoke run:
+# binary16 (tensor-memory kernel, 64-k drain) and TF32 (tile kernel, 32-k drain).
+SMOKE_B200 = {oracle.FP16: 1.380e-07, oracle.TF32: 1.531e-07}
+
+
+@pytest.mark.parametrize("tc", sorted(SMOKE_B200))
+def test_model_reproduces_recorded_smoke_errors(tc):
+    """Out-of-sample check of the MMA model, TF32 included (the width was chosen on binary16
+    data): the smoke call's two recorded errors to their printed four digits."""
+    m, n, k = 256, 192, 1024
+    rng = np.random.default_rng(0)
+    A = rng.uniform(-1, 1, m * k).astype(np.float32)
+    B = rng.uniform(-1, 1, k * n).astype(np.float16)
+    ref = oracle.dgemm_ref(0, 0, m, n, k, 1.0, A, m, B, k)
+    C = np.zeros(m * n, np.float32)
+    oracle.shgemm(tc, 0, 0, m, n, k, 1.0, A, m, B, k, 0.0, C, m, 0, 0, oracle.B200MODEL)
+    e = oracle.rel_fro(oracle.logical_c(C, m, n, m), ref)
+    assert abs(e / SMOKE_B200[tc] - 1) < 5e-4, (tc, e)
